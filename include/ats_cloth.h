@@ -1,0 +1,192 @@
+/*
+ * ats_cloth.h -- C ABI of the B200 cloth solver (libats_b200.so).
+ *
+ * The solver is the hot path of libAtsSim's cloth simulation: Vertex Block Descent
+ * (inertial prediction, per-colour sweeps that gather mass-spring stretch and
+ * quadratic bending gradients and 3x3 Hessians and solve a 3x3 block system, then
+ * the velocity update) and XPBD per-colour constraint projection. Each entry point
+ * below replaces one task of the reference's CPU/Metal implementation; the
+ * function ids are those of src/heterogeneous/launcher.h (namespace Launcher).
+ *
+ * Conventions
+ *   - Every call returns an int status: ATS_OK (0) or an ATS_ERR_* code; the
+ *     message of the last failure on the calling thread is ats_last_error().
+ *   - Handles own their device memory; one handle is used from one host thread.
+ *   - `stream` is a cudaStream_t passed as a plain pointer (NULL = legacy default
+ *     stream). Step entry points only enqueue work and return, like the Metal
+ *     encode path of the reference (examples/example3_hybrid_cpu_gpu.cpp:1210-1377).
+ *   - Host arrays are plain pointers; vertex arrays are in the caller's original
+ *     vertex order, instances concatenated (instance 0 first).
+ *   - There is no CPU fallback: without a usable CUDA device every compute call
+ *     fails with ATS_ERR_CUDA.
+ */
+#ifndef ATS_CLOTH_H
+#define ATS_CLOTH_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    ATS_OK = 0,
+    ATS_ERR_INVALID = 1,   /* bad argument (null pointer, out-of-range index, bad mesh) */
+    ATS_ERR_CUDA = 2,      /* CUDA runtime error or no device */
+    ATS_ERR_NOMEM = 3,     /* host or device allocation failed */
+    ATS_ERR_TIMEOUT = 4,   /* a bounded device wait expired */
+    ATS_ERR_STATE = 5      /* call not valid in the handle's current state */
+};
+
+enum { ATS_SOLVER_VBD = 0, ATS_SOLVER_XPBD = 1 };
+
+/* Grid triangulation patterns for ats_grid_mesh. */
+enum {
+    ATS_GRID_UNIFORM = 0,    /* every quad split along (r,c)-(r+1,c+1) */
+    ATS_GRID_ALTERNATING = 1 /* split alternates with (r+c) parity, the square40K.obj layout */
+};
+
+/* Which colouring / topology array to read back. */
+enum {
+    ATS_COLORING_VERTEX = 0,  /* VBD vertex colours (example2_async_iter.cpp:572-646) */
+    ATS_COLORING_STRETCH = 1, /* XPBD edge colours (example2_async_iter.cpp:458-533) */
+    ATS_COLORING_BENDING = 2  /* XPBD bending-edge colours (same function, nv = 4) */
+};
+
+typedef struct ats_topology ats_topology;
+typedef struct ats_cloth ats_cloth;
+typedef void* ats_stream;
+
+/* One cloth instance. positions are the rest (and initial) state. */
+typedef struct ats_instance_desc {
+    int num_verts;
+    const float* positions;      /* 3 * num_verts */
+    int num_faces;
+    const int* faces;            /* 3 * num_faces, 0-based, triangles */
+    const float* mass;           /* num_verts, kg (SceneParams default_mass rules live in ats_mass_*) */
+    const unsigned char* fixed;  /* num_verts, nonzero = pinned (sa_is_fixed) */
+    float k_stretch;             /* stiffness_stretch_spring, N/m */
+    float k_bend;                /* effective quadratic bending stiffness
+                                    (SceneParams::get_stiffness_quadratic_bending()) */
+} ats_instance_desc;
+
+/* Solver parameters shared by all instances of a handle. */
+typedef struct ats_solver_params {
+    float implicit_dt;      /* frame step; the substep dt is implicit_dt / num_substep */
+    int num_substep;        /* substeps per frame */
+    int iterations;         /* constraint_iter_count */
+    float damping;          /* damping_cloth: v *= exp(-damping * dt) */
+    float gravity[3];       /* external acceleration, m/s^2 */
+    int threads_per_vertex; /* VBD sweep lanes per vertex: 1, 2, 4 or 8; 0 = default (4) */
+    int block_size;         /* VBD sweep threads per block (multiple of 32, <= 1024); 0 = default (128) */
+} ats_solver_params;
+
+typedef struct ats_cloth_info {
+    int num_instances;
+    int num_verts;          /* total over instances */
+    int num_edges;
+    int num_bending_edges;
+    int num_vertex_colors;  /* max over instances */
+    int num_stretch_colors;
+    int num_bending_colors;
+    int threads_per_vertex;
+    int block_size;
+    int stencil_slots;      /* stencil entries stored (incl. padding) */
+    long long device_bytes; /* device memory held by the handle */
+} ats_cloth_info;
+
+/* ---------------------------------------------------------------- host-only mesh helpers */
+
+/* Regular n x n grid on y = 0 spanning [-0.5, 0.5]^2: vertex (r, c) -> r*n + c at
+ * (-0.5 + c/(n-1), 0, -0.5 + r/(n-1)). positions: 3*n*n floats; faces: 6*(n-1)^2 ints. */
+int ats_grid_mesh(int n, int pattern, float* positions, int* faces);
+
+/* Pins of examples/example2_async_iter.cpp:195-209: AABB-normalised z < 0.01 and
+ * (x > 0.99 or x < 0.01). */
+int ats_reference_pins(const float* positions, int num_verts, unsigned char* fixed);
+
+/* Area-lumped mass: each triangle gives a third of its area to each corner, scaled
+ * so that the masses sum to total_mass. */
+int ats_mass_area_weighted(const float* positions, int num_verts, const int* faces, int num_faces,
+                           float total_mass, float* mass);
+
+/* Reads the vertices and triangles of a Wavefront OBJ file (0-based faces,
+ * degenerate triangles dropped as src/Utils/mesh_reader.cpp:170-177). Call with
+ * null arrays first to get the counts. */
+int ats_obj_read(const char* path, int* num_verts, float* positions, int* num_faces, int* faces);
+
+/* ---------------------------------------------------------------- topology (host only)
+ * Replaces SimMesh::extract_edges_from_surface (src/Utils/mesh_reader.h:206-298), the
+ * adjacency set-up and greedy colourings of examples/example2_async_iter.cpp:229-304,
+ * 442-697, and the rest state of :309-375. Integer results are bit-identical to the
+ * reference algorithms. */
+int ats_topology_build(const ats_instance_desc* mesh, ats_topology** out);
+int ats_topology_destroy(ats_topology* topo);
+/* counts[0..4] = edges, bending edges, vertex colours, stretch colours, bending colours */
+int ats_topology_counts(const ats_topology* topo, int* counts);
+int ats_topology_edges(const ats_topology* topo, int* edges /* 2E */, int* bending /* 4B */);
+int ats_topology_rest(const ats_topology* topo, float* rest_length /* E */, float* q /* 16B, column-major */);
+int ats_topology_coloring(const ats_topology* topo, int which, int* prefix /* C+1 */, int* items);
+
+/* ---------------------------------------------------------------- solver handle */
+
+/* Builds the topology of every instance, the colour-major device layout and uploads
+ * it. Replaces CpuSolver::init_xpbd_system (example2_async_iter.cpp:442-697) for a
+ * CUDA device. */
+int ats_cloth_create(const ats_instance_desc* instances, int num_instances, const ats_solver_params* params,
+                     ats_cloth** out);
+int ats_cloth_destroy(ats_cloth* cloth);
+int ats_cloth_query(const ats_cloth* cloth, ats_cloth_info* info);
+
+/* Frame-end state (x, v), 3 floats per vertex, original order, instances concatenated.
+ * Replaces SolverInterface::restart_system / load_saved_state and the frame_end read
+ * (example2_async_iter.cpp:1575-1614). Both calls synchronise `stream`. v may be null. */
+int ats_set_state(ats_cloth* cloth, const float* x, const float* v, ats_stream stream);
+int ats_get_state(ats_cloth* cloth, float* x, float* v, ats_stream stream);
+/* Current iterate x (mid-frame), same layout. Synchronises `stream`. */
+int ats_get_positions(ats_cloth* cloth, float* x, ats_stream stream);
+
+/* Per-instance external acceleration (gravity plus wind force / instance mass),
+ * 3 floats per instance, read by the device at every predict / sweep; enqueued on
+ * `stream` so that it takes effect for work queued after it. */
+int ats_set_accel(ats_cloth* cloth, const float* accel, ats_stream stream);
+
+/* --- step entry points (one per launcher task) --- */
+/* id_xpbd_predict_position (launcher.h:92): x = x0 + h (v + h a), pinned: x = x0. */
+int ats_predict_position(ats_cloth* cloth, ats_stream stream);
+/* id_vbd_all_in_one (launcher.h:80) with cluster_idx = color: inertia + stretch +
+ * bending gather and guarded 3x3 solve for every vertex of the colour. */
+int ats_vbd_color_sweep(ats_cloth* cloth, int color, ats_stream stream);
+/* id_xpbd_update_velocity (launcher.h:96): v = (x - x0)/h * exp(-damping h), x0 = x. */
+int ats_update_velocity(ats_cloth* cloth, ats_stream stream);
+/* id_xpbd_reset_constrains (launcher.h:93): lambda = 0. */
+int ats_xpbd_reset_constraints(ats_cloth* cloth, ats_stream stream);
+/* id_xpbd_constraint_stretch_mass_spring (launcher.h:21) for one colour. */
+int ats_xpbd_stretch_color(ats_cloth* cloth, int color, ats_stream stream);
+/* id_xpbd_constraint_bending (launcher.h:23) for one colour (quadratic bending). */
+int ats_xpbd_bending_color(ats_cloth* cloth, int color, ats_stream stream);
+
+/* One whole frame (substeps x (predict, iterations x colours, update)), as
+ * CpuSolver::physics_step_vbd / physics_step_xpbd (example2_async_iter.cpp:1017-1143). */
+int ats_frame(ats_cloth* cloth, int solver, ats_stream stream);
+/* The same frame replayed from a CUDA graph captured on first use (per solver). */
+int ats_frame_graph(ats_cloth* cloth, int solver, ats_stream stream);
+
+/* FP64 incremental-potential energy of the current iterate against the current
+ * frame start (Energy::compute_energy_* of xpbd_constraints.h:2079-2214):
+ * out[0] = inertia, out[1] = stretch, out[2] = bending. Synchronises `stream`. */
+int ats_energy(ats_cloth* cloth, double* out3, ats_stream stream);
+/* FP64 norm of the incremental-potential gradient over free vertices, one value per
+ * instance, of the current iterate (grad = m/h^2 (x - y) - f_stretch - f_bending,
+ * y = x0 + h v + h^2 a). Synchronises `stream`. */
+int ats_residual(ats_cloth* cloth, double* out_per_instance, ats_stream stream);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* ats_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ATS_CLOTH_H */

@@ -1,0 +1,329 @@
+"""libatssim_b200 -- B200-native cloth solver (VBD and XPBD) behind a C ABI.
+
+Python access to ``libats_b200.so`` (include/ats_cloth.h) through ctypes. The
+compute path is the CUDA library; this module only marshals arrays and status
+codes. Loading fails loudly when the library is missing: there is no CPU path.
+
+Names follow libAtsSim: a *cloth* holds one or more instances (meshes), each with
+its own stiffness; a *frame* is predict -> iterations x colours -> update
+(examples/example2_async_iter.cpp:1082-1143).
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "lib", "libats_b200.so")
+
+ATS_OK, ATS_ERR_INVALID, ATS_ERR_CUDA, ATS_ERR_NOMEM, ATS_ERR_TIMEOUT, ATS_ERR_STATE = range(6)
+SOLVER_VBD, SOLVER_XPBD = 0, 1
+GRID_UNIFORM, GRID_ALTERNATING = 0, 1
+COLORING = {"vertex": 0, "stretch": 1, "bending": 2}
+
+
+class AtsError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"ats status {status}: {msg}")
+        self.status = status
+
+
+class InstanceDesc(ctypes.Structure):
+    _fields_ = [
+        ("num_verts", ctypes.c_int),
+        ("positions", ctypes.POINTER(ctypes.c_float)),
+        ("num_faces", ctypes.c_int),
+        ("faces", ctypes.POINTER(ctypes.c_int)),
+        ("mass", ctypes.POINTER(ctypes.c_float)),
+        ("fixed", ctypes.POINTER(ctypes.c_ubyte)),
+        ("k_stretch", ctypes.c_float),
+        ("k_bend", ctypes.c_float),
+    ]
+
+
+class SolverParams(ctypes.Structure):
+    _fields_ = [
+        ("implicit_dt", ctypes.c_float),
+        ("num_substep", ctypes.c_int),
+        ("iterations", ctypes.c_int),
+        ("damping", ctypes.c_float),
+        ("gravity", ctypes.c_float * 3),
+        ("threads_per_vertex", ctypes.c_int),
+        ("block_size", ctypes.c_int),
+    ]
+
+
+class ClothInfo(ctypes.Structure):
+    _fields_ = [
+        ("num_instances", ctypes.c_int),
+        ("num_verts", ctypes.c_int),
+        ("num_edges", ctypes.c_int),
+        ("num_bending_edges", ctypes.c_int),
+        ("num_vertex_colors", ctypes.c_int),
+        ("num_stretch_colors", ctypes.c_int),
+        ("num_bending_colors", ctypes.c_int),
+        ("threads_per_vertex", ctypes.c_int),
+        ("block_size", ctypes.c_int),
+        ("stencil_slots", ctypes.c_int),
+        ("device_bytes", ctypes.c_longlong),
+    ]
+
+
+_lib = None
+_fp = ctypes.POINTER(ctypes.c_float)
+_ip = ctypes.POINTER(ctypes.c_int)
+_dp = ctypes.POINTER(ctypes.c_double)
+_u8p = ctypes.POINTER(ctypes.c_ubyte)
+_vp = ctypes.c_void_p
+
+# (name, argtypes) of every exported C entry point; all return int unless noted.
+_SIGNATURES = {
+    "ats_grid_mesh": [ctypes.c_int, ctypes.c_int, _fp, _ip],
+    "ats_reference_pins": [_fp, ctypes.c_int, _u8p],
+    "ats_mass_area_weighted": [_fp, ctypes.c_int, _ip, ctypes.c_int, ctypes.c_float, _fp],
+    "ats_obj_read": [ctypes.c_char_p, _ip, _fp, _ip, _ip],
+    "ats_topology_build": [ctypes.POINTER(InstanceDesc), ctypes.POINTER(_vp)],
+    "ats_topology_destroy": [_vp],
+    "ats_topology_counts": [_vp, _ip],
+    "ats_topology_edges": [_vp, _ip, _ip],
+    "ats_topology_rest": [_vp, _fp, _fp],
+    "ats_topology_coloring": [_vp, ctypes.c_int, _ip, _ip],
+    "ats_cloth_create": [ctypes.POINTER(InstanceDesc), ctypes.c_int, ctypes.POINTER(SolverParams), ctypes.POINTER(_vp)],
+    "ats_cloth_destroy": [_vp],
+    "ats_cloth_query": [_vp, ctypes.POINTER(ClothInfo)],
+    "ats_set_state": [_vp, _fp, _fp, _vp],
+    "ats_get_state": [_vp, _fp, _fp, _vp],
+    "ats_get_positions": [_vp, _fp, _vp],
+    "ats_set_accel": [_vp, _fp, _vp],
+    "ats_predict_position": [_vp, _vp],
+    "ats_vbd_color_sweep": [_vp, ctypes.c_int, _vp],
+    "ats_update_velocity": [_vp, _vp],
+    "ats_xpbd_reset_constraints": [_vp, _vp],
+    "ats_xpbd_stretch_color": [_vp, ctypes.c_int, _vp],
+    "ats_xpbd_bending_color": [_vp, ctypes.c_int, _vp],
+    "ats_frame": [_vp, ctypes.c_int, _vp],
+    "ats_frame_graph": [_vp, ctypes.c_int, _vp],
+    "ats_energy": [_vp, _dp, _vp],
+    "ats_residual": [_vp, _dp, _vp],
+}
+
+
+def lib():
+    """Loads libats_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run `python -m libatssim_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, args in _SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = ctypes.c_int
+        L.ats_last_error.restype = ctypes.c_char_p
+        L.ats_last_error.argtypes = []
+        _lib = L
+    return _lib
+
+
+def _check(status):
+    if status != ATS_OK:
+        raise AtsError(status, lib().ats_last_error().decode())
+
+
+def _p(a, t):
+    return a.ctypes.data_as(ctypes.POINTER(t))
+
+
+def _stream(stream):
+    """Accepts None, an int handle or a torch.cuda.Stream."""
+    if stream is None:
+        return None
+    if hasattr(stream, "cuda_stream"):
+        return ctypes.c_void_p(stream.cuda_stream)
+    return ctypes.c_void_p(int(stream))
+
+
+# ---------------------------------------------------------------- mesh helpers
+def grid_mesh(n, pattern=GRID_UNIFORM):
+    """n x n grid on y = 0 over [-0.5, 0.5]^2 -> (positions (n*n, 3), faces (2(n-1)^2, 3))."""
+    pos = np.zeros((n * n, 3), dtype=np.float32)
+    faces = np.zeros((2 * (n - 1) * (n - 1), 3), dtype=np.int32)
+    _check(lib().ats_grid_mesh(n, pattern, _p(pos, ctypes.c_float), _p(faces, ctypes.c_int)))
+    return pos, faces
+
+
+def reference_pins(positions):
+    pos = np.ascontiguousarray(positions, dtype=np.float32)
+    out = np.zeros(pos.shape[0], dtype=np.uint8)
+    _check(lib().ats_reference_pins(_p(pos, ctypes.c_float), pos.shape[0], _p(out, ctypes.c_ubyte)))
+    return out
+
+
+def mass_area_weighted(positions, faces, total_mass):
+    pos = np.ascontiguousarray(positions, dtype=np.float32)
+    f = np.ascontiguousarray(faces, dtype=np.int32)
+    out = np.zeros(pos.shape[0], dtype=np.float32)
+    _check(lib().ats_mass_area_weighted(_p(pos, ctypes.c_float), pos.shape[0], _p(f, ctypes.c_int), f.shape[0],
+                                        float(total_mass), _p(out, ctypes.c_float)))
+    return out
+
+
+def obj_read(path):
+    nv, nf = ctypes.c_int(0), ctypes.c_int(0)
+    _check(lib().ats_obj_read(path.encode(), ctypes.byref(nv), None, ctypes.byref(nf), None))
+    pos = np.zeros((nv.value, 3), dtype=np.float32)
+    faces = np.zeros((nf.value, 3), dtype=np.int32)
+    _check(lib().ats_obj_read(path.encode(), ctypes.byref(nv), _p(pos, ctypes.c_float), ctypes.byref(nf),
+                              _p(faces, ctypes.c_int)))
+    return pos, faces
+
+
+class Instance:
+    """One cloth mesh with its material: positions (V,3), faces (F,3), mass (V,),
+    fixed (V,), k_stretch, k_bend (effective quadratic bending stiffness)."""
+
+    def __init__(self, positions, faces, mass, fixed, k_stretch, k_bend):
+        self.positions = np.ascontiguousarray(positions, dtype=np.float32)
+        self.faces = np.ascontiguousarray(faces, dtype=np.int32)
+        self.mass = np.ascontiguousarray(mass, dtype=np.float32)
+        self.fixed = np.ascontiguousarray(fixed, dtype=np.uint8)
+        self.k_stretch = float(k_stretch)
+        self.k_bend = float(k_bend)
+
+    @property
+    def num_verts(self):
+        return self.positions.shape[0]
+
+    def desc(self):
+        return InstanceDesc(self.num_verts, _p(self.positions, ctypes.c_float), self.faces.shape[0],
+                            _p(self.faces, ctypes.c_int), _p(self.mass, ctypes.c_float),
+                            _p(self.fixed, ctypes.c_ubyte), self.k_stretch, self.k_bend)
+
+
+class Topology:
+    """Host-only topology of one instance (edges, bending edges, colourings, rest state)."""
+
+    def __init__(self, inst):
+        self._inst = inst
+        d = inst.desc()
+        h = _vp()
+        _check(lib().ats_topology_build(ctypes.byref(d), ctypes.byref(h)))
+        self.h = h
+        c = np.zeros(5, dtype=np.int32)
+        _check(lib().ats_topology_counts(self.h, _p(c, ctypes.c_int)))
+        self.ne, self.nb, self.n_vcolors, self.n_scolors, self.n_bcolors = (int(v) for v in c)
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib().ats_topology_destroy(self.h)
+        except Exception:
+            pass
+
+    def edges(self):
+        e = np.zeros((self.ne, 2), dtype=np.int32)
+        b = np.zeros((self.nb, 4), dtype=np.int32)
+        _check(lib().ats_topology_edges(self.h, _p(e, ctypes.c_int), _p(b, ctypes.c_int)))
+        return e, b
+
+    def rest(self):
+        L = np.zeros(self.ne, dtype=np.float32)
+        Q = np.zeros((self.nb, 4, 4), dtype=np.float32)
+        _check(lib().ats_topology_rest(self.h, _p(L, ctypes.c_float), _p(Q, ctypes.c_float)))
+        return L, Q
+
+    def coloring(self, which):
+        w = COLORING[which]
+        n = {0: self.n_vcolors, 1: self.n_scolors, 2: self.n_bcolors}[w]
+        total = {0: self._inst.num_verts, 1: self.ne, 2: self.nb}[w]
+        prefix = np.zeros(n + 1, dtype=np.int32)
+        items = np.zeros(max(total, 1), dtype=np.int32)
+        _check(lib().ats_topology_coloring(self.h, w, _p(prefix, ctypes.c_int), _p(items, ctypes.c_int)))
+        return [items[prefix[c]:prefix[c + 1]].copy() for c in range(n)]
+
+
+class Cloth:
+    """A solver handle over one or more instances (ats_cloth_create)."""
+
+    def __init__(self, instances, *, implicit_dt=1.0 / 60.0, num_substep=1, iterations=100, damping=2.0,
+                 gravity=(0.0, -9.8, 0.0), threads_per_vertex=0, block_size=0):
+        if isinstance(instances, Instance):
+            instances = [instances]
+        self.instances = list(instances)
+        descs = (InstanceDesc * len(self.instances))(*[i.desc() for i in self.instances])
+        self.params = SolverParams(implicit_dt, num_substep, iterations, damping,
+                                   (ctypes.c_float * 3)(*gravity), threads_per_vertex, block_size)
+        h = _vp()
+        _check(lib().ats_cloth_create(descs, len(self.instances), ctypes.byref(self.params), ctypes.byref(h)))
+        self.h = h
+        info = ClothInfo()
+        _check(lib().ats_cloth_query(self.h, ctypes.byref(info)))
+        self.info = info
+        self.nv = info.num_verts
+        self.iterations = iterations
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().ats_cloth_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # state -------------------------------------------------------------
+    def set_state(self, x, v=None, stream=None):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        vv = None if v is None else np.ascontiguousarray(v, dtype=np.float32)
+        _check(lib().ats_set_state(self.h, _p(x, ctypes.c_float), None if vv is None else _p(vv, ctypes.c_float),
+                                   _stream(stream)))
+
+    def state(self, stream=None):
+        x = np.zeros((self.nv, 3), dtype=np.float32)
+        v = np.zeros((self.nv, 3), dtype=np.float32)
+        _check(lib().ats_get_state(self.h, _p(x, ctypes.c_float), _p(v, ctypes.c_float), _stream(stream)))
+        return x, v
+
+    def positions(self, stream=None):
+        x = np.zeros((self.nv, 3), dtype=np.float32)
+        _check(lib().ats_get_positions(self.h, _p(x, ctypes.c_float), _stream(stream)))
+        return x
+
+    def set_accel(self, accel, stream=None):
+        a = np.ascontiguousarray(np.broadcast_to(np.asarray(accel, dtype=np.float32), (self.info.num_instances, 3)))
+        _check(lib().ats_set_accel(self.h, _p(a, ctypes.c_float), _stream(stream)))
+
+    # steps ---------------------------------------------------------------
+    def predict(self, stream=None):
+        _check(lib().ats_predict_position(self.h, _stream(stream)))
+
+    def vbd_color_sweep(self, color, stream=None):
+        _check(lib().ats_vbd_color_sweep(self.h, int(color), _stream(stream)))
+
+    def update_velocity(self, stream=None):
+        _check(lib().ats_update_velocity(self.h, _stream(stream)))
+
+    def xpbd_reset(self, stream=None):
+        _check(lib().ats_xpbd_reset_constraints(self.h, _stream(stream)))
+
+    def xpbd_stretch_color(self, color, stream=None):
+        _check(lib().ats_xpbd_stretch_color(self.h, int(color), _stream(stream)))
+
+    def xpbd_bending_color(self, color, stream=None):
+        _check(lib().ats_xpbd_bending_color(self.h, int(color), _stream(stream)))
+
+    def frame(self, solver=SOLVER_VBD, stream=None, graph=False):
+        fn = lib().ats_frame_graph if graph else lib().ats_frame
+        _check(fn(self.h, solver, _stream(stream)))
+
+    def energy(self, stream=None):
+        out = np.zeros(3, dtype=np.float64)
+        _check(lib().ats_energy(self.h, _p(out, ctypes.c_double), _stream(stream)))
+        return out
+
+    def residual(self, stream=None):
+        out = np.zeros(self.info.num_instances, dtype=np.float64)
+        _check(lib().ats_residual(self.h, _p(out, ctypes.c_double), _stream(stream)))
+        return out

@@ -1,0 +1,814 @@
+// ats_cloth.cu -- solver handle, sm_100a kernels and the C ABI of libats_b200.so.
+//
+// Each step entry point is one launcher task of the reference
+// (src/heterogeneous/launcher.h FunctionID); a frame is the loop of
+// CpuSolver::physics_step_vbd / physics_step_xpbd (examples/example2_async_iter.cpp:
+// 1017-1143) issued as kernels on one stream, optionally replayed as a CUDA graph.
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/ats_cloth.h"
+#include "ats_kernels.cuh"
+#include "ats_topology.hpp"
+
+namespace ats {
+
+static thread_local std::string g_last_error;
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+namespace {
+
+#define ATS_CUDA(call)                                                                          \
+    do {                                                                                        \
+        cudaError_t _e = (call);                                                                \
+        if (_e != cudaSuccess) {                                                                \
+            set_error(std::string(#call) + ": " + cudaGetErrorString(_e));                      \
+            return ATS_ERR_CUDA;                                                                \
+        }                                                                                       \
+    } while (0)
+
+template <typename T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+    cudaError_t alloc(size_t count) {
+        n = count;
+        if (count == 0) return cudaSuccess;
+        return cudaMalloc((void**)&p, count * sizeof(T));
+    }
+    size_t bytes() const { return n * sizeof(T); }
+};
+
+// ---------------------------------------------------------------- kernels
+
+// Core::predict_position (xpbd_constraints.h:321-384): v_pred = v + h a (0 if pinned),
+// x = x0 + h v_pred.
+__global__ void predict_kernel(float4* __restrict__ x, const float4* __restrict__ x0, const float4* __restrict__ vel,
+                               const float4* __restrict__ vm, const float4* __restrict__ accel, int n, float h) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 p = x0[i], v = vel[i];
+    float4 a = __ldg(&accel[__float_as_int(v.w)]);
+    bool pinned = vm[i].y != 0.f;
+    float vx = v.x + h * a.x, vy = v.y + h * a.y, vz = v.z + h * a.z;
+    if (pinned) vx = vy = vz = 0.f;
+    x[i] = make_float4(p.x + h * vx, p.y + h * vy, p.z + h * vz, 0.f);
+}
+
+// Core::update_velocity (xpbd_constraints.h:535-581): v = (x - x0)/h * damp, x0 = x.
+__global__ void update_kernel(const float4* __restrict__ x, float4* __restrict__ x0, float4* __restrict__ vel, int n,
+                              float h, float damp) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 p = x[i], q = x0[i], v = vel[i];
+    v.x = ((p.x - q.x) / h) * damp;
+    v.y = ((p.y - q.y) / h) * damp;
+    v.z = ((p.z - q.z) / h) * damp;
+    vel[i] = v;
+    x0[i] = make_float4(p.x, p.y, p.z, q.w);
+}
+
+// solve_stretch_mass_spring_template (xpbd_constraints.h:984-1059) for one colour.
+__global__ void xpbd_stretch_kernel(float4* __restrict__ x, const float4* __restrict__ vm, const int2* __restrict__ edge,
+                                    const float* __restrict__ rest, const float* __restrict__ kst,
+                                    float* __restrict__ lambda, int b, int e, float h) {
+    int i = b + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= e) return;
+    int2 ed = edge[i];
+    float4 p0 = x[ed.x], p1 = x[ed.y];
+    float w0 = vm[ed.x].z, w1 = vm[ed.y].z;
+    float lam = lambda[i];
+    float L = rest[i], k = kst[i];
+    float dx = p1.x - p0.x, dy = p1.y - p0.y, dz = p1.z - p0.z;
+    float lsq = dx * dx + dy * dy + dz * dz;
+    if (lsq < 1e-8f) return;
+    float l = sqrtf(lsq);
+    float C = l - L;
+    float gx = -(dx / l), gy = -(dy / l), gz = -(dz / l);
+    float alpha = k < kEps ? 1e9f : 1.f / ((k * h) * h);
+    float denom = alpha + (w0 + w1);
+    float dl = (-C - alpha * lam) / denom;
+    lambda[i] = lam + dl;
+    if (denom != 0.f) {
+        float s0 = dl * w0, s1 = (-dl) * w1;
+        x[ed.x] = make_float4(p0.x + s0 * gx, p0.y + s0 * gy, p0.z + s0 * gz, p0.w);
+        x[ed.y] = make_float4(p1.x + s1 * gx, p1.y + s1 * gy, p1.z + s1 * gz, p1.w);
+    }
+}
+
+// solve_bending_quadratic_template (xpbd_constraints.h:1170-1229, core :1062-1126,
+// get_delta_xpbd_4 :211-236) for one colour. q holds the 10 unique entries of the
+// symmetric Q, then k_b.
+__global__ void xpbd_bending_kernel(float4* __restrict__ x, const float4* __restrict__ vm, const int4* __restrict__ idx,
+                                    const float4* __restrict__ q, float* __restrict__ lambda, int b, int e, float h) {
+    int i = b + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= e) return;
+    int4 id = idx[i];
+    float4 qa = q[3 * i], qb = q[3 * i + 1], qc = q[3 * i + 2];
+    float Q[4][4];
+    Q[0][0] = qa.x; Q[0][1] = Q[1][0] = qa.y; Q[0][2] = Q[2][0] = qa.z; Q[0][3] = Q[3][0] = qa.w;
+    Q[1][1] = qb.x; Q[1][2] = Q[2][1] = qb.y; Q[1][3] = Q[3][1] = qb.z; Q[2][2] = qb.w;
+    Q[2][3] = Q[3][2] = qc.x; Q[3][3] = qc.y;
+    const float kb = qc.z;
+    const int vid[4] = {id.x, id.y, id.z, id.w};
+    float3 p[4];
+    float w[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        float4 t = x[vid[j]];
+        p[j] = make_float3(t.x, t.y, t.z);
+        w[j] = vm[vid[j]].z;
+    }
+    float sum = 0.f;
+#pragma unroll
+    for (int ii = 0; ii < 4; ++ii)
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj)
+            sum += Q[ii][jj] * (p[ii].x * p[jj].x + p[ii].y * p[jj].y + p[ii].z * p[jj].z);
+    float C = 0.5f * sum;
+    float3 g[4];
+    float denom = 0.f;
+#pragma unroll
+    for (int ii = 0; ii < 4; ++ii) {
+        float gx = 0.f, gy = 0.f, gz = 0.f;
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) {
+            gx += Q[ii][jj] * p[jj].x;
+            gy += Q[ii][jj] * p[jj].y;
+            gz += Q[ii][jj] * p[jj].z;
+        }
+        g[ii] = make_float3(gx, gy, gz);
+        denom += w[ii] * (gx * gx + gy * gy + gz * gz);
+    }
+    float alpha = kb < kEps ? 1e12f : 1.f / ((kb * h) * h);
+    denom += alpha;
+    float lam = lambda[i];
+    float dl = (-C - alpha * lam) / denom;
+    lambda[i] = lam + dl;
+    if (denom != 0.f) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            float s = dl * w[j];
+            float4 t = x[vid[j]];
+            x[vid[j]] = make_float4(p[j].x + s * g[j].x, p[j].y + s * g[j].y, p[j].z + s * g[j].z, t.w);
+        }
+    }
+}
+
+// ---- FP64 reductions (deterministic: fixed element -> thread assignment, fixed tree)
+constexpr int kRedThreads = 256;
+constexpr int kRedBlocks = 296;  // 2 x 148 SMs
+
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+    const int t = threadIdx.x;
+    sh[t] = v;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (t < s) sh[t] += sh[t + s];
+        __syncthreads();
+    }
+    double r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+struct EnergyArgs {
+    const float4* x;
+    const float4* x0;
+    const float4* vel;
+    const float4* vm;
+    const float4* accel;
+    int nv;
+    const int2* edge;
+    const float* rest;
+    const float* kst;
+    int ne;
+    const int4* bend;
+    const float* q16;
+    const float* kb;
+    int nb;
+    double h;
+    double* partial;  // 3 * gridDim.x
+};
+
+// Energy::compute_energy_inertia / _stretch_mass_spring / _bending
+// (xpbd_constraints.h:2079-2214), every term in FP64.
+__global__ void __launch_bounds__(kRedThreads) energy_kernel(EnergyArgs a) {
+    __shared__ double sh[kRedThreads];
+    const int stride = gridDim.x * blockDim.x;
+    const int t0 = blockIdx.x * blockDim.x + threadIdx.x;
+    double ei = 0.0, es = 0.0, eb = 0.0;
+    for (int i = t0; i < a.nv; i += stride) {
+        float4 p = a.x[i], q = a.x0[i], v = a.vel[i];
+        float4 acc = a.accel[__float_as_int(v.w)];
+        bool pinned = a.vm[i].y != 0.f;
+        double ax = pinned ? 0.0 : acc.x, ay = pinned ? 0.0 : acc.y, az = pinned ? 0.0 : acc.z;
+        double dx = (double)p.x - ((double)q.x + a.h * v.x + a.h * a.h * ax);
+        double dy = (double)p.y - ((double)q.y + a.h * v.y + a.h * a.h * ay);
+        double dz = (double)p.z - ((double)q.z + a.h * v.z + a.h * a.h * az);
+        ei += (double)q.w / (2.0 * a.h * a.h) * (dx * dx + dy * dy + dz * dz);
+    }
+    for (int i = t0; i < a.ne; i += stride) {
+        int2 e = a.edge[i];
+        float4 p0 = a.x[e.x], p1 = a.x[e.y];
+        double dx = (double)p1.x - p0.x, dy = (double)p1.y - p0.y, dz = (double)p1.z - p0.z;
+        double l2 = dx * dx + dy * dy + dz * dz;
+        if (l2 < 1e-8) continue;
+        double C = sqrt(l2) - (double)a.rest[i];
+        es += 0.5 * (double)a.kst[i] * C * C;
+    }
+    for (int i = t0; i < a.nb; i += stride) {
+        int4 id = a.bend[i];
+        const int vid[4] = {id.x, id.y, id.z, id.w};
+        double p[4][3];
+        for (int j = 0; j < 4; ++j) {
+            float4 t = a.x[vid[j]];
+            p[j][0] = t.x;
+            p[j][1] = t.y;
+            p[j][2] = t.z;
+        }
+        const float* Q = a.q16 + 16 * (size_t)i;
+        double s = 0.0;
+        for (int c = 0; c < 4; ++c)
+            for (int r = 0; r < 4; ++r)
+                s += (double)Q[4 * c + r] * (p[c][0] * p[r][0] + p[c][1] * p[r][1] + p[c][2] * p[r][2]);
+        eb += 0.5 * (double)a.kb[i] * s;
+    }
+    double si = block_sum(ei, sh);
+    double ss = block_sum(es, sh);
+    double sb = block_sum(eb, sh);
+    if (threadIdx.x == 0) {
+        a.partial[3 * blockIdx.x + 0] = si;
+        a.partial[3 * blockIdx.x + 1] = ss;
+        a.partial[3 * blockIdx.x + 2] = sb;
+    }
+}
+
+__global__ void __launch_bounds__(kRedThreads) sum_partials3_kernel(const double* partial, int n, double* out) {
+    __shared__ double sh[kRedThreads];
+    for (int k = 0; k < 3; ++k) {
+        double v = 0.0;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) v += partial[3 * i + k];
+        double s = block_sum(v, sh);
+        if (threadIdx.x == 0) out[k] = s;
+    }
+}
+
+// Squared FP64 gradient of the incremental potential at every free vertex:
+// grad = m/h^2 (x - y) - f_stretch - f_bending, y = x0 + h v + h^2 a.
+struct GradArgs {
+    const float4* x;
+    const float4* x0;
+    const float4* vel;
+    const float4* vm;
+    const float4* accel;
+    const int* st_idx;
+    const float* st_rest;
+    const float* st_w;
+    const int4* slices;
+    int nslices;
+    int tpv;
+    double h;
+    double* g2;  // per vertex (layout order)
+};
+
+__global__ void grad_kernel(GradArgs a) {
+    // one thread per (vertex, lane-group) entry: walk the slice rows of its vertex
+    const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (warp >= a.nslices) return;
+    const int4 sd = a.slices[warp];
+    const int k = lane / a.tpv;
+    if (k >= sd.y) return;
+    if (lane % a.tpv != 0) return;  // the first lane of a vertex walks all its slots
+    const int v = sd.x + k;
+    const float4 xv = a.x[v], p0 = a.x0[v], vv = a.vel[v], mv = a.vm[v];
+    if (mv.y != 0.f) {
+        a.g2[v] = 0.0;
+        return;
+    }
+    const float4 acc = a.accel[__float_as_int(vv.w)];
+    const double h = a.h, m = p0.w;
+    double gx = m / (h * h) * ((double)xv.x - ((double)p0.x + h * vv.x + h * h * acc.x));
+    double gy = m / (h * h) * ((double)xv.y - ((double)p0.y + h * vv.y + h * h * acc.y));
+    double gz = m / (h * h) * ((double)xv.z - ((double)p0.z + h * vv.z + h * h * acc.z));
+    const double ks = mv.w;
+    for (int row = 0; row < sd.w; ++row) {
+        for (int r = 0; r < a.tpv; ++r) {
+            const int e = sd.z + row * 32 + k * a.tpv + r;
+            const int u = a.st_idx[e];
+            if (u == v) continue;
+            const float4 xu = a.x[u];
+            const double dx = (double)xu.x - xv.x, dy = (double)xu.y - xv.y, dz = (double)xu.z - xv.z;
+            const double w = a.st_w[e];
+            gx += w * dx;
+            gy += w * dy;
+            gz += w * dz;
+            const double L = a.st_rest[e];
+            if (L >= 0.0) {
+                const double l = sqrt(dx * dx + dy * dy + dz * dz);
+                if (l > 0.0) {
+                    const double s = ks * (l - L) / l;
+                    gx -= s * dx;
+                    gy -= s * dy;
+                    gz -= s * dz;
+                }
+            }
+        }
+    }
+    a.g2[v] = gx * gx + gy * gy + gz * gz;
+}
+
+__global__ void __launch_bounds__(kRedThreads) segment_sum_kernel(const double* g2, const int* seg, double* out) {
+    __shared__ double sh[kRedThreads];
+    const int b = seg[blockIdx.x], e = seg[blockIdx.x + 1];
+    double v = 0.0;
+    for (int i = b + threadIdx.x; i < e; i += blockDim.x) v += g2[i];
+    double s = block_sum(v, sh);
+    if (threadIdx.x == 0) out[blockIdx.x] = sqrt(s);
+}
+
+}  // namespace
+}  // namespace ats
+
+using namespace ats;
+
+struct ats_cloth {
+    Layout L;
+    ats_solver_params prm{};
+    int device = 0;
+    int block = 128;
+    float h = 0.f, h2inv = 0.f, damp = 1.f;
+    // device arrays
+    DevBuf<float4> x, x0, vel, vm, accel;
+    DevBuf<int> st_idx;
+    DevBuf<float> st_rest, st_w;
+    DevBuf<int4> slices;
+    DevBuf<int2> xs_edge;
+    DevBuf<float> xs_rest, xs_k, xs_lambda;
+    DevBuf<int4> xb_idx;
+    DevBuf<float4> xb_q;
+    DevBuf<float> xb_lambda;
+    DevBuf<int2> en_edge;
+    DevBuf<float> en_rest, en_k, en_q, en_kb;
+    DevBuf<int4> en_bend;
+    DevBuf<int> inst_seg;
+    // scratch for the FP64 reductions
+    DevBuf<double> partial, red_out, g2;
+    std::vector<int> color_slices;
+    cudaStream_t capture_stream = nullptr;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    // pinned staging for state I/O
+    std::vector<float> host4;
+
+    ~ats_cloth() {
+        for (auto& g : graph)
+            if (g) cudaGraphExecDestroy(g);
+        if (capture_stream) cudaStreamDestroy(capture_stream);
+    }
+};
+
+namespace {
+
+inline cudaStream_t S(ats_stream s) { return (cudaStream_t)s; }
+
+template <typename T, typename U>
+int upload(DevBuf<T>& d, const std::vector<U>& h, size_t count) {
+    ATS_CUDA(d.alloc(count));
+    if (count) ATS_CUDA(cudaMemcpy(d.p, h.data(), count * sizeof(T), cudaMemcpyHostToDevice));
+    return ATS_OK;
+}
+
+int check_device() {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        set_error(std::string("no CUDA device: ") + (e == cudaSuccess ? "device count is 0" : cudaGetErrorString(e)));
+        return ATS_ERR_CUDA;
+    }
+    return ATS_OK;
+}
+
+int launch_sweep(ats_cloth* c, int color, cudaStream_t st) {
+    const int sb = c->color_slices[color], se = c->color_slices[color + 1];
+    if (se <= sb) return ATS_OK;
+    SweepArgs a;
+    a.x = c->x.p;
+    a.x0 = c->x0.p;
+    a.vel = c->vel.p;
+    a.vm = c->vm.p;
+    a.st_idx = c->st_idx.p;
+    a.st_rest = c->st_rest.p;
+    a.st_w = c->st_w.p;
+    a.slices = c->slices.p;
+    a.accel = c->accel.p;
+    a.slice_begin = sb;
+    a.slice_end = se;
+    a.h = c->h;
+    a.h2inv = c->h2inv;
+    const int warps_per_block = c->block / 32;
+    const int grid = (se - sb + warps_per_block - 1) / warps_per_block;
+    switch (c->L.tpv) {
+        case 1: vbd_sweep_kernel<1><<<grid, c->block, 0, st>>>(a); break;
+        case 2: vbd_sweep_kernel<2><<<grid, c->block, 0, st>>>(a); break;
+        case 4: vbd_sweep_kernel<4><<<grid, c->block, 0, st>>>(a); break;
+        default: vbd_sweep_kernel<8><<<grid, c->block, 0, st>>>(a); break;
+    }
+    ATS_CUDA(cudaGetLastError());
+    return ATS_OK;
+}
+
+int launch_predict(ats_cloth* c, cudaStream_t st) {
+    const int n = c->L.nv;
+    predict_kernel<<<(n + 255) / 256, 256, 0, st>>>(c->x.p, c->x0.p, c->vel.p, c->vm.p, c->accel.p, n, c->h);
+    ATS_CUDA(cudaGetLastError());
+    return ATS_OK;
+}
+
+int launch_update(ats_cloth* c, cudaStream_t st) {
+    const int n = c->L.nv;
+    update_kernel<<<(n + 255) / 256, 256, 0, st>>>(c->x.p, c->x0.p, c->vel.p, n, c->h, c->damp);
+    ATS_CUDA(cudaGetLastError());
+    return ATS_OK;
+}
+
+int launch_reset(ats_cloth* c, cudaStream_t st) {
+    if (c->xs_lambda.n) ATS_CUDA(cudaMemsetAsync(c->xs_lambda.p, 0, c->xs_lambda.bytes(), st));
+    if (c->xb_lambda.n) ATS_CUDA(cudaMemsetAsync(c->xb_lambda.p, 0, c->xb_lambda.bytes(), st));
+    return ATS_OK;
+}
+
+int launch_xpbd_stretch(ats_cloth* c, int color, cudaStream_t st) {
+    const int b = c->L.xs_color[color], e = c->L.xs_color[color + 1];
+    if (e <= b) return ATS_OK;
+    xpbd_stretch_kernel<<<(e - b + 127) / 128, 128, 0, st>>>(c->x.p, c->vm.p, c->xs_edge.p, c->xs_rest.p, c->xs_k.p,
+                                                               c->xs_lambda.p, b, e, c->h);
+    ATS_CUDA(cudaGetLastError());
+    return ATS_OK;
+}
+
+int launch_xpbd_bending(ats_cloth* c, int color, cudaStream_t st) {
+    const int b = c->L.xb_color[color], e = c->L.xb_color[color + 1];
+    if (e <= b) return ATS_OK;
+    xpbd_bending_kernel<<<(e - b + 127) / 128, 128, 0, st>>>(c->x.p, c->vm.p, c->xb_idx.p, c->xb_q.p, c->xb_lambda.p,
+                                                               b, e, c->h);
+    ATS_CUDA(cudaGetLastError());
+    return ATS_OK;
+}
+
+int enqueue_frame(ats_cloth* c, int solver, cudaStream_t st) {
+    int r;
+    for (int sub = 0; sub < c->prm.num_substep; ++sub) {
+        if ((r = launch_predict(c, st))) return r;
+        if (solver == ATS_SOLVER_XPBD && (r = launch_reset(c, st))) return r;
+        for (int it = 0; it < c->prm.iterations; ++it) {
+            if (solver == ATS_SOLVER_VBD) {
+                for (int col = 0; col < c->L.n_vcolors; ++col)
+                    if ((r = launch_sweep(c, col, st))) return r;
+            } else {
+                for (int col = 0; col < c->L.n_scolors; ++col)
+                    if ((r = launch_xpbd_stretch(c, col, st))) return r;
+                for (int col = 0; col < c->L.n_bcolors; ++col)
+                    if ((r = launch_xpbd_bending(c, col, st))) return r;
+            }
+        }
+        if ((r = launch_update(c, st))) return r;
+    }
+    return ATS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* ats_last_error(void) { return g_last_error.c_str(); }
+
+int ats_cloth_create(const ats_instance_desc* inst, int ninst, const ats_solver_params* prm, ats_cloth** out) {
+    if (!inst || ninst <= 0 || !prm || !out) {
+        set_error("ats_cloth_create: need instances, params and an output pointer");
+        return ATS_ERR_INVALID;
+    }
+    if (!(prm->implicit_dt > 0.f) || prm->num_substep <= 0 || prm->iterations < 0) {
+        set_error("ats_cloth_create: need implicit_dt > 0, num_substep > 0, iterations >= 0");
+        return ATS_ERR_INVALID;
+    }
+    int tpv = prm->threads_per_vertex ? prm->threads_per_vertex : 4;
+    int block = prm->block_size ? prm->block_size : 128;
+    if (block % 32 || block < 32 || block > 256) {
+        set_error("ats_cloth_create: block_size must be a multiple of 32 in [32, 256]");
+        return ATS_ERR_INVALID;
+    }
+    for (int i = 0; i < ninst; ++i)
+        if (!inst[i].mass || !inst[i].fixed) {
+            set_error("ats_cloth_create: every instance needs mass and fixed arrays");
+            return ATS_ERR_INVALID;
+        }
+    int r = check_device();
+    if (r) return r;
+    std::vector<Topology> topos(ninst);
+    std::vector<ats_instance_desc> descs(inst, inst + ninst);
+    std::string err;
+    for (int i = 0; i < ninst; ++i)
+        if (!build_topology(inst[i], topos[i], err)) {
+            set_error("ats_cloth_create: instance " + std::to_string(i) + ": " + err);
+            return ATS_ERR_INVALID;
+        }
+    std::unique_ptr<ats_cloth> c(new (std::nothrow) ats_cloth());
+    if (!c) {
+        set_error("ats_cloth_create: out of memory");
+        return ATS_ERR_NOMEM;
+    }
+    if (!build_layout(topos, descs, tpv, c->L, err)) {
+        set_error("ats_cloth_create: " + err);
+        return ATS_ERR_INVALID;
+    }
+    c->prm = *prm;
+    c->prm.threads_per_vertex = tpv;
+    c->prm.block_size = block;
+    c->block = block;
+    c->h = prm->implicit_dt / float(prm->num_substep);
+    c->h2inv = 1.f / (c->h * c->h);
+    c->damp = std::exp(-prm->damping * c->h);
+    ATS_CUDA(cudaGetDevice(&c->device));
+    Layout& L = c->L;
+    const size_t nv = L.nv;
+    if ((r = upload(c->x, L.x0, nv)) || (r = upload(c->x0, L.x0, nv)) || (r = upload(c->vel, L.vel, nv)) ||
+        (r = upload(c->vm, L.vm, nv)))
+        return r;
+    std::vector<float> acc(4 * (size_t)L.ninst, 0.f);
+    for (int i = 0; i < L.ninst; ++i)
+        for (int k = 0; k < 3; ++k) acc[4 * i + k] = prm->gravity[k];
+    if ((r = upload(c->accel, acc, L.ninst))) return r;
+    if ((r = upload(c->st_idx, L.st_idx, L.st_idx.size())) || (r = upload(c->st_rest, L.st_rest, L.st_rest.size())) ||
+        (r = upload(c->st_w, L.st_w, L.st_w.size())) || (r = upload(c->slices, L.slices, L.slices.size() / 4)))
+        return r;
+    if ((r = upload(c->xs_edge, L.xs_edge, L.xs_rest.size())) || (r = upload(c->xs_rest, L.xs_rest, L.xs_rest.size())) ||
+        (r = upload(c->xs_k, L.xs_k, L.xs_k.size())))
+        return r;
+    ATS_CUDA(c->xs_lambda.alloc(L.xs_rest.size()));
+    if ((r = upload(c->xb_idx, L.xb_idx, L.xb_idx.size() / 4)) || (r = upload(c->xb_q, L.xb_q, L.xb_q.size() / 4)))
+        return r;
+    ATS_CUDA(c->xb_lambda.alloc(L.xb_idx.size() / 4));
+    if ((r = upload(c->en_edge, L.en_edge, L.en_rest.size())) || (r = upload(c->en_rest, L.en_rest, L.en_rest.size())) ||
+        (r = upload(c->en_k, L.en_k, L.en_k.size())) || (r = upload(c->en_bend, L.en_bend, L.en_kb.size())) ||
+        (r = upload(c->en_q, L.en_q, L.en_q.size())) || (r = upload(c->en_kb, L.en_kb, L.en_kb.size())))
+        return r;
+    if ((r = upload(c->inst_seg, L.inst_vbegin, L.inst_vbegin.size()))) return r;
+    ATS_CUDA(c->partial.alloc(3 * (size_t)kRedBlocks));
+    ATS_CUDA(c->red_out.alloc(std::max(3, L.ninst)));
+    ATS_CUDA(c->g2.alloc(nv));
+    c->color_slices = L.color_slices;
+    ATS_CUDA(cudaStreamCreateWithFlags(&c->capture_stream, cudaStreamNonBlocking));
+    ATS_CUDA(cudaDeviceSynchronize());
+    *out = c.release();
+    return ATS_OK;
+}
+
+int ats_cloth_destroy(ats_cloth* c) {
+    if (!c) return ATS_OK;
+    cudaDeviceSynchronize();
+    delete c;
+    return ATS_OK;
+}
+
+int ats_cloth_query(const ats_cloth* c, ats_cloth_info* info) {
+    if (!c || !info) {
+        set_error("ats_cloth_query: null argument");
+        return ATS_ERR_INVALID;
+    }
+    info->num_instances = c->L.ninst;
+    info->num_verts = c->L.nv;
+    info->num_edges = c->L.ne;
+    info->num_bending_edges = c->L.nb;
+    info->num_vertex_colors = c->L.n_vcolors;
+    info->num_stretch_colors = c->L.n_scolors;
+    info->num_bending_colors = c->L.n_bcolors;
+    info->threads_per_vertex = c->L.tpv;
+    info->block_size = c->block;
+    info->stencil_slots = (int)c->L.st_idx.size();
+    info->device_bytes = (long long)(c->x.bytes() + c->x0.bytes() + c->vel.bytes() + c->vm.bytes() + c->accel.bytes() +
+                                     c->st_idx.bytes() + c->st_rest.bytes() + c->st_w.bytes() + c->slices.bytes() +
+                                     c->xs_edge.bytes() + c->xs_rest.bytes() + c->xs_k.bytes() + c->xs_lambda.bytes() +
+                                     c->xb_idx.bytes() + c->xb_q.bytes() + c->xb_lambda.bytes() + c->en_edge.bytes() +
+                                     c->en_rest.bytes() + c->en_k.bytes() + c->en_q.bytes() + c->en_kb.bytes() +
+                                     c->en_bend.bytes() + c->inst_seg.bytes() + c->partial.bytes() +
+                                     c->red_out.bytes() + c->g2.bytes());
+    return ATS_OK;
+}
+
+int ats_set_state(ats_cloth* c, const float* x, const float* v, ats_stream stream) {
+    if (!c || !x) {
+        set_error("ats_set_state: need a handle and positions");
+        return ATS_ERR_INVALID;
+    }
+    const Layout& L = c->L;
+    std::vector<float> hx(4 * (size_t)L.nv), hv(4 * (size_t)L.nv);
+    for (int lv = 0; lv < L.nv; ++lv) {
+        int o = L.to_caller[lv];
+        for (int k = 0; k < 3; ++k) {
+            hx[4 * (size_t)lv + k] = x[3 * (size_t)o + k];
+            hv[4 * (size_t)lv + k] = v ? v[3 * (size_t)o + k] : 0.f;
+        }
+        hx[4 * (size_t)lv + 3] = L.x0[4 * (size_t)lv + 3];  // mass
+        hv[4 * (size_t)lv + 3] = L.vel[4 * (size_t)lv + 3];  // instance id
+    }
+    cudaStream_t st = S(stream);
+    ATS_CUDA(cudaMemcpyAsync(c->x0.p, hx.data(), hx.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+    ATS_CUDA(cudaMemcpyAsync(c->vel.p, hv.data(), hv.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+    ATS_CUDA(cudaMemcpyAsync(c->x.p, c->x0.p, c->x0.bytes(), cudaMemcpyDeviceToDevice, st));
+    ATS_CUDA(cudaStreamSynchronize(st));
+    return ATS_OK;
+}
+
+static int read_back(ats_cloth* c, const float4* src, float* dst, cudaStream_t st) {
+    const Layout& L = c->L;
+    c->host4.resize(4 * (size_t)L.nv);
+    ATS_CUDA(cudaMemcpyAsync(c->host4.data(), src, 16 * (size_t)L.nv, cudaMemcpyDeviceToHost, st));
+    ATS_CUDA(cudaStreamSynchronize(st));
+    for (int lv = 0; lv < L.nv; ++lv) {
+        int o = L.to_caller[lv];
+        for (int k = 0; k < 3; ++k) dst[3 * (size_t)o + k] = c->host4[4 * (size_t)lv + k];
+    }
+    return ATS_OK;
+}
+
+int ats_get_state(ats_cloth* c, float* x, float* v, ats_stream stream) {
+    if (!c || !x) {
+        set_error("ats_get_state: need a handle and an output array");
+        return ATS_ERR_INVALID;
+    }
+    int r = read_back(c, c->x0.p, x, S(stream));
+    if (r || !v) return r;
+    return read_back(c, c->vel.p, v, S(stream));
+}
+
+int ats_get_positions(ats_cloth* c, float* x, ats_stream stream) {
+    if (!c || !x) {
+        set_error("ats_get_positions: need a handle and an output array");
+        return ATS_ERR_INVALID;
+    }
+    return read_back(c, c->x.p, x, S(stream));
+}
+
+int ats_set_accel(ats_cloth* c, const float* accel, ats_stream stream) {
+    if (!c || !accel) {
+        set_error("ats_set_accel: null argument");
+        return ATS_ERR_INVALID;
+    }
+    std::vector<float> a(4 * (size_t)c->L.ninst, 0.f);
+    for (int i = 0; i < c->L.ninst; ++i)
+        for (int k = 0; k < 3; ++k) a[4 * i + k] = accel[3 * i + k];
+    ATS_CUDA(cudaMemcpyAsync(c->accel.p, a.data(), a.size() * sizeof(float), cudaMemcpyHostToDevice, S(stream)));
+    ATS_CUDA(cudaStreamSynchronize(S(stream)));
+    return ATS_OK;
+}
+
+int ats_predict_position(ats_cloth* c, ats_stream stream) {
+    if (!c) { set_error("ats_predict_position: null handle"); return ATS_ERR_INVALID; }
+    return launch_predict(c, S(stream));
+}
+
+int ats_vbd_color_sweep(ats_cloth* c, int color, ats_stream stream) {
+    if (!c || color < 0 || color >= c->L.n_vcolors) {
+        set_error("ats_vbd_color_sweep: null handle or colour out of range");
+        return ATS_ERR_INVALID;
+    }
+    return launch_sweep(c, color, S(stream));
+}
+
+int ats_update_velocity(ats_cloth* c, ats_stream stream) {
+    if (!c) { set_error("ats_update_velocity: null handle"); return ATS_ERR_INVALID; }
+    return launch_update(c, S(stream));
+}
+
+int ats_xpbd_reset_constraints(ats_cloth* c, ats_stream stream) {
+    if (!c) { set_error("ats_xpbd_reset_constraints: null handle"); return ATS_ERR_INVALID; }
+    return launch_reset(c, S(stream));
+}
+
+int ats_xpbd_stretch_color(ats_cloth* c, int color, ats_stream stream) {
+    if (!c || color < 0 || color >= c->L.n_scolors) {
+        set_error("ats_xpbd_stretch_color: null handle or colour out of range");
+        return ATS_ERR_INVALID;
+    }
+    return launch_xpbd_stretch(c, color, S(stream));
+}
+
+int ats_xpbd_bending_color(ats_cloth* c, int color, ats_stream stream) {
+    if (!c || color < 0 || color >= c->L.n_bcolors) {
+        set_error("ats_xpbd_bending_color: null handle or colour out of range");
+        return ATS_ERR_INVALID;
+    }
+    return launch_xpbd_bending(c, color, S(stream));
+}
+
+int ats_frame(ats_cloth* c, int solver, ats_stream stream) {
+    if (!c || (solver != ATS_SOLVER_VBD && solver != ATS_SOLVER_XPBD)) {
+        set_error("ats_frame: null handle or unknown solver");
+        return ATS_ERR_INVALID;
+    }
+    return enqueue_frame(c, solver, S(stream));
+}
+
+int ats_frame_graph(ats_cloth* c, int solver, ats_stream stream) {
+    if (!c || (solver != ATS_SOLVER_VBD && solver != ATS_SOLVER_XPBD)) {
+        set_error("ats_frame_graph: null handle or unknown solver");
+        return ATS_ERR_INVALID;
+    }
+    if (!c->graph[solver]) {
+        cudaGraph_t g = nullptr;
+        ATS_CUDA(cudaStreamBeginCapture(c->capture_stream, cudaStreamCaptureModeThreadLocal));
+        int r = enqueue_frame(c, solver, c->capture_stream);
+        cudaError_t e = cudaStreamEndCapture(c->capture_stream, &g);
+        if (r) {
+            if (g) cudaGraphDestroy(g);
+            return r;
+        }
+        if (e != cudaSuccess) {
+            set_error(std::string("ats_frame_graph: capture failed: ") + cudaGetErrorString(e));
+            return ATS_ERR_CUDA;
+        }
+        e = cudaGraphInstantiate(&c->graph[solver], g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            set_error(std::string("ats_frame_graph: instantiate failed: ") + cudaGetErrorString(e));
+            return ATS_ERR_CUDA;
+        }
+    }
+    ATS_CUDA(cudaGraphLaunch(c->graph[solver], S(stream)));
+    return ATS_OK;
+}
+
+int ats_energy(ats_cloth* c, double* out3, ats_stream stream) {
+    if (!c || !out3) {
+        set_error("ats_energy: null argument");
+        return ATS_ERR_INVALID;
+    }
+    cudaStream_t st = S(stream);
+    EnergyArgs a;
+    a.x = c->x.p;
+    a.x0 = c->x0.p;
+    a.vel = c->vel.p;
+    a.vm = c->vm.p;
+    a.accel = c->accel.p;
+    a.nv = c->L.nv;
+    a.edge = c->en_edge.p;
+    a.rest = c->en_rest.p;
+    a.kst = c->en_k.p;
+    a.ne = c->L.ne;
+    a.bend = c->en_bend.p;
+    a.q16 = c->en_q.p;
+    a.kb = c->en_kb.p;
+    a.nb = c->L.nb;
+    a.h = (double)c->h;
+    a.partial = c->partial.p;
+    energy_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(a);
+    ATS_CUDA(cudaGetLastError());
+    sum_partials3_kernel<<<1, kRedThreads, 0, st>>>(c->partial.p, kRedBlocks, c->red_out.p);
+    ATS_CUDA(cudaGetLastError());
+    ATS_CUDA(cudaMemcpyAsync(out3, c->red_out.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    ATS_CUDA(cudaStreamSynchronize(st));
+    return ATS_OK;
+}
+
+int ats_residual(ats_cloth* c, double* out, ats_stream stream) {
+    if (!c || !out) {
+        set_error("ats_residual: null argument");
+        return ATS_ERR_INVALID;
+    }
+    cudaStream_t st = S(stream);
+    GradArgs a;
+    a.x = c->x.p;
+    a.x0 = c->x0.p;
+    a.vel = c->vel.p;
+    a.vm = c->vm.p;
+    a.accel = c->accel.p;
+    a.st_idx = c->st_idx.p;
+    a.st_rest = c->st_rest.p;
+    a.st_w = c->st_w.p;
+    a.slices = c->slices.p;
+    a.nslices = (int)c->slices.n;
+    a.tpv = c->L.tpv;
+    a.h = (double)c->h;
+    a.g2 = c->g2.p;
+    const int blocks = (a.nslices * 32 + 127) / 128;
+    grad_kernel<<<blocks, 128, 0, st>>>(a);
+    ATS_CUDA(cudaGetLastError());
+    segment_sum_kernel<<<c->L.ninst, kRedThreads, 0, st>>>(c->g2.p, c->inst_seg.p, c->red_out.p);
+    ATS_CUDA(cudaGetLastError());
+    ATS_CUDA(cudaMemcpyAsync(out, c->red_out.p, c->L.ninst * sizeof(double), cudaMemcpyDeviceToHost, st));
+    ATS_CUDA(cudaStreamSynchronize(st));
+    return ATS_OK;
+}
+
+}  // extern "C"
