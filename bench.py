@@ -1,0 +1,323 @@
+"""Benchmark of the CUDA cloth solver (one JSON line on rank 0).
+
+Workload (a step = one simulated frame): a 512 x 512-vertex grid cloth
+(262,144 vertices, 784,385 edges, 782,341 bending edges), k = 1e3 N/m,
+k_b = 1e-2, 0.1 kg area-lumped, two top corners pinned, h = 1/60 s,
+plain Vertex Block Descent with 50 iterations x 4 colours per frame, FP32.
+
+  value  frames/s with the state resident in HBM, device-timed (CUDA events on
+         the launching stream, one event pair per frame, L2 flushed between frames
+         outside the event pairs), summed over ranks.
+  e2e    frames/s through the public C ABI with host arrays: every frame uploads
+         the state (x, v) from host memory, runs the frame and reads (x, v) back.
+  roofline  the colour-sweep kernel: algorithmic bytes per launch
+         (40 V + 12 E + 56 B per iteration, shared by colour) over its mean
+         CUDA-event duration, against the measured HBM copy bandwidth.
+  cpu_baseline  the CPU oracle (a C++ restatement of the reference's CPU VBD,
+         the reference itself does not build here) on a bounded sample of the
+         same workload, rank 0 only.
+
+--impl reference times that CPU implementation alone on this workload with all
+host threads (each step = 10 of the frame's 50 iterations, scaled to frames/s).
+
+Multi-GPU: the single cloth does not partition (a graph split would need a halo
+exchange per colour), so N > 1 runs N independent replicas ("weak" scaling); the
+timing is the max over ranks.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "frames/s to 1e-4 residual: batched+learned VBD vs plain CUDA VBD, 1 B200"
+UNIT = "frames/s"
+WORKLOAD = "c1: 512x512 grid cloth, plain VBD, 50 iterations x 4 colours per frame"
+ITERS = 50
+REF_SAMPLE_ITERS = 10
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--tpv", type=int, default=0)
+    p.add_argument("--block", type=int, default=0)
+    return p.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def alg_bytes_per_iter(nv, ne, nb):
+    return 40 * nv + 12 * ne + 56 * nb
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_port_sample(threads, iters):
+    """Times the CPU oracle on one frame of `iters` iterations of the workload."""
+    from libatssim_b200 import configs
+    from oracle import ats_oracle
+    ats_oracle.build()
+    insts, prm = configs.c1()
+    inst = insts[0]
+    s = ats_oracle.Scene(inst.positions, inst.faces, inst.mass, inst.fixed, dt=prm["implicit_dt"],
+                         substeps=1, iterations=iters, k_stretch=inst.k_stretch, k_bend=inst.k_bend,
+                         damping=prm["damping"], threads=threads)
+    return s
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    s = cpu_port_sample(threads, REF_SAMPLE_ITERS)
+    for _ in range(args.warmup):
+        s.frame()
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        s.frame()
+    dt = time.perf_counter() - t
+    per_frame = dt / args.steps * (ITERS / REF_SAMPLE_ITERS)
+    fps = 1.0 / per_frame
+    out = {"impl": "reference", "metric": METRIC, "value": fps, "unit": UNIT, "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_frame * 1e3, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+           "config": {"workload": WORKLOAD, "vertices": 262144, "iterations": ITERS, "frames": args.steps},
+           "cpu_baseline": {"value": fps, "unit": UNIT, "cores": threads, "kind": "port",
+                            "sample": f"{REF_SAMPLE_ITERS} of {ITERS} iterations per frame, scaled; "
+                                      "C++ restatement of examples/example2_async_iter.cpp VBD"},
+           "e2e": {"value": fps, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def profile_traffic():
+    """dram bytes per sweep launch from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "vbd_sweep_c1_ncu.json")
+    if os.path.exists(p):
+        try:
+            return json.load(open(p)).get("dram_bytes_per_launch")
+        except Exception:
+            return None
+    return None
+
+
+def run_ours(args):
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    import libatssim_b200 as ats
+    from libatssim_b200 import build, configs
+    build.build()
+    insts, prm = configs.c1()
+    cloth = ats.Cloth(insts, threads_per_vertex=args.tpv, block_size=args.block, **prm)
+    stream = torch.cuda.current_stream()
+    tuned = None
+    if not args.tpv and not args.block:
+        tuned = cloth.autotune(iterations=5, stream=stream)
+    info = cloth.info
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    # warm-up (also captures the frame graph)
+    for _ in range(args.warmup):
+        cloth.frame(stream=stream, graph=True)
+    torch.cuda.synchronize()
+
+    # --- device-timed frames, L2 flushed between frames outside the event pairs
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    for i in range(args.steps):
+        flush.fill_(i & 0xFF)
+        starts[i].record(stream)
+        cloth.frame(stream=stream, graph=True)
+        ends[i].record(stream)
+    barrier()
+    clk = clocks.stop()
+    ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_step = ms / args.steps
+    value = world * 1e3 / ms_per_step
+
+    # --- residual reached after the frame's iterations (reported, not timed)
+    x_end, v_end = cloth.state()
+    cloth.predict(stream=stream)
+    r0 = cloth.residual(stream=stream)[0]
+    for _ in range(ITERS):
+        for c in range(info.num_vertex_colors):
+            cloth.vbd_color_sweep(c, stream=stream)
+    r1 = cloth.residual(stream=stream)[0]
+    cloth.set_state(x_end, v_end, stream=stream)
+
+    # --- per-launch sweep duration: CUDA events around ITERS back-to-back iterations
+    # (ITERS x colours sweep launches, chained by programmatic dependent launch as in
+    # the frame), L2 flushed before each repetition as between timed frames
+    reps = []
+    for rep in range(3):
+        flush.fill_(rep)
+        cloth.predict(stream=stream)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        cloth.vbd_iterations(ITERS, stream=stream)
+        e1.record(stream)
+        cloth.update_velocity(stream=stream)
+        reps.append((e0, e1))
+    torch.cuda.synchronize()
+    mean_sweep_ms = float(np.mean([a.elapsed_time(b) for a, b in reps])) / (ITERS * info.num_vertex_colors)
+    bytes_iter = alg_bytes_per_iter(info.num_verts, info.num_edges, info.num_bending_edges)
+    bytes_launch = bytes_iter / info.num_vertex_colors
+    achieved = bytes_launch / (mean_sweep_ms * 1e-3) / 1e9
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        peak = float(json.load(open(peaks_path))["hbm_gbs"])
+        peak_src = "measured"
+    else:
+        peak, peak_src = 6650.0, "fallback"
+
+    # --- end to end through the public API with host arrays
+    x_h, v_h = cloth.state()
+    e2e_steps = max(3, min(args.steps, 10))
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        cloth.set_state(x_h, v_h, stream=stream)
+        cloth.frame(stream=stream, graph=True)
+        x_h, v_h = cloth.state(stream=stream)
+    barrier()
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    state_bytes = 2 * 3 * 4 * info.num_verts
+
+    out = None
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+               "config": {"workload": WORKLOAD, "vertices": info.num_verts, "edges": info.num_edges,
+                          "bending_edges": info.num_bending_edges, "colors": info.num_vertex_colors,
+                          "iterations": ITERS, "threads_per_vertex": info.threads_per_vertex,
+                          "block_size": info.block_size, "autotuned": tuned is not None,
+                          "parallelism": f"replicas{world}",
+                          "l2": "flushed between frames (256 MiB write, outside the event pairs)"},
+               "residual": {"relative_after_frame": float(r1 / r0), "definition":
+                            "||grad G(x)|| / ||grad G(y)||, FP64, free vertices"},
+               "e2e": {"value": world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": state_bytes,
+                       "d2h_bytes_per_step": state_bytes},
+               "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                            "frac": achieved / peak, "traffic": profile_traffic(),
+                            "kernel": f"vbd_sweep_kernel<{info.threads_per_vertex}>", "mean_launch_us": mean_sweep_ms * 1e3,
+                            "alg_bytes_per_launch": bytes_launch, "peak_source": peak_src},
+               "gpu_launches": args.steps * (2 + ITERS * info.num_vertex_colors),
+               "clocks": clk}
+    if rank == 0 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        s = cpu_port_sample(threads, REF_SAMPLE_ITERS)
+        s.frame()
+        t = time.perf_counter()
+        n = 2
+        for _ in range(n):
+            s.frame()
+        per_frame = (time.perf_counter() - t) / n * (ITERS / REF_SAMPLE_ITERS)
+        out["cpu_baseline"] = {"value": 1.0 / per_frame, "unit": UNIT, "cores": threads, "kind": "port",
+                               "sample": f"{n} frames of {REF_SAMPLE_ITERS}/{ITERS} iterations, scaled"}
+    if out is not None:
+        print(json.dumps(out), flush=True)
+    cloth.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

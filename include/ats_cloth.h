@@ -158,6 +158,9 @@ int ats_predict_position(ats_cloth* cloth, ats_stream stream);
 /* id_vbd_all_in_one (launcher.h:80) with cluster_idx = color: inertia + stretch +
  * bending gather and guarded 3x3 solve for every vertex of the colour. */
 int ats_vbd_color_sweep(ats_cloth* cloth, int color, ats_stream stream);
+/* `iterations` full VBD iterations (all colours in order), as
+ * solve_constraints_VBD repeated (example2_async_iter.cpp:1481-1509). */
+int ats_vbd_iterations(ats_cloth* cloth, int iterations, ats_stream stream);
 /* id_xpbd_update_velocity (launcher.h:96): v = (x - x0)/h * exp(-damping h), x0 = x. */
 int ats_update_velocity(ats_cloth* cloth, ats_stream stream);
 /* id_xpbd_reset_constrains (launcher.h:93): lambda = 0. */
@@ -172,6 +175,12 @@ int ats_xpbd_bending_color(ats_cloth* cloth, int color, ats_stream stream);
 int ats_frame(ats_cloth* cloth, int solver, ats_stream stream);
 /* The same frame replayed from a CUDA graph captured on first use (per solver). */
 int ats_frame_graph(ats_cloth* cloth, int solver, ats_stream stream);
+
+/* Times `iterations` VBD iterations for every lanes-per-vertex (1, 2, 4, 8) and
+ * block size (64, 128, 256) on this handle's own mesh, keeps the fastest and
+ * reports it. The iterate x is restored afterwards; captured frame graphs are
+ * dropped (they are re-captured on next use). Synchronises `stream`. */
+int ats_autotune(ats_cloth* cloth, int iterations, ats_stream stream, int* tpv, int* block_size);
 
 /* FP64 incremental-potential energy of the current iterate against the current
  * frame start (Energy::compute_energy_* of xpbd_constraints.h:2079-2214):

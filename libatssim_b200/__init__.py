@@ -97,12 +97,14 @@ _SIGNATURES = {
     "ats_set_accel": [_vp, _fp, _vp],
     "ats_predict_position": [_vp, _vp],
     "ats_vbd_color_sweep": [_vp, ctypes.c_int, _vp],
+    "ats_vbd_iterations": [_vp, ctypes.c_int, _vp],
     "ats_update_velocity": [_vp, _vp],
     "ats_xpbd_reset_constraints": [_vp, _vp],
     "ats_xpbd_stretch_color": [_vp, ctypes.c_int, _vp],
     "ats_xpbd_bending_color": [_vp, ctypes.c_int, _vp],
     "ats_frame": [_vp, ctypes.c_int, _vp],
     "ats_frame_graph": [_vp, ctypes.c_int, _vp],
+    "ats_autotune": [_vp, ctypes.c_int, _vp, _ip, _ip],
     "ats_energy": [_vp, _dp, _vp],
     "ats_residual": [_vp, _dp, _vp],
 }
@@ -301,6 +303,18 @@ class Cloth:
 
     def vbd_color_sweep(self, color, stream=None):
         _check(lib().ats_vbd_color_sweep(self.h, int(color), _stream(stream)))
+
+    def vbd_iterations(self, n, stream=None):
+        _check(lib().ats_vbd_iterations(self.h, int(n), _stream(stream)))
+
+    def autotune(self, iterations=10, stream=None):
+        """Picks lanes-per-vertex and block size by timing; returns (tpv, block)."""
+        t, b = ctypes.c_int(0), ctypes.c_int(0)
+        _check(lib().ats_autotune(self.h, int(iterations), _stream(stream), ctypes.byref(t), ctypes.byref(b)))
+        info = ClothInfo()
+        _check(lib().ats_cloth_query(self.h, ctypes.byref(info)))
+        self.info = info
+        return t.value, b.value
 
     def update_velocity(self, stream=None):
         _check(lib().ats_update_velocity(self.h, _stream(stream)))

@@ -51,18 +51,26 @@ struct DevBuf {
 
 // ---------------------------------------------------------------- kernels
 
+// Explicitly rounded FP32 operations: the predict / update / XPBD kernels evaluate
+// every term in the order of the reference's CPU code with no fused multiply-add,
+// so they round exactly as the CPU restatement does.
+__device__ __forceinline__ float fm(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fa(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fs(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float fdot(float3 a, float3 b) { return fa(fa(fm(a.x, b.x), fm(a.y, b.y)), fm(a.z, b.z)); }
+
 // Core::predict_position (xpbd_constraints.h:321-384): v_pred = v + h a (0 if pinned),
 // x = x0 + h v_pred.
 __global__ void predict_kernel(float4* __restrict__ x, const float4* __restrict__ x0, const float4* __restrict__ vel,
-                               const float4* __restrict__ vm, const float4* __restrict__ accel, int n, float h) {
+                               const float4* __restrict__ vm, const float4* __restrict__ inst, int n, float h) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    float4 p = x0[i], v = vel[i];
-    float4 a = __ldg(&accel[__float_as_int(v.w)]);
-    bool pinned = vm[i].y != 0.f;
-    float vx = v.x + h * a.x, vy = v.y + h * a.y, vz = v.z + h * a.z;
+    float4 p = x0[i], v = vel[i], m = vm[i];
+    float4 a = __ldg(&inst[__float_as_int(m.w)]);
+    bool pinned = m.y != 0.f;
+    float vx = fa(v.x, fm(h, a.x)), vy = fa(v.y, fm(h, a.y)), vz = fa(v.z, fm(h, a.z));
     if (pinned) vx = vy = vz = 0.f;
-    x[i] = make_float4(p.x + h * vx, p.y + h * vy, p.z + h * vz, 0.f);
+    x[i] = make_float4(fa(p.x, fm(h, vx)), fa(p.y, fm(h, vy)), fa(p.z, fm(h, vz)), 0.f);
 }
 
 // Core::update_velocity (xpbd_constraints.h:535-581): v = (x - x0)/h * damp, x0 = x.
@@ -71,9 +79,9 @@ __global__ void update_kernel(const float4* __restrict__ x, float4* __restrict__
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float4 p = x[i], q = x0[i], v = vel[i];
-    v.x = ((p.x - q.x) / h) * damp;
-    v.y = ((p.y - q.y) / h) * damp;
-    v.z = ((p.z - q.z) / h) * damp;
+    v.x = fm(fs(p.x, q.x) / h, damp);
+    v.y = fm(fs(p.y, q.y) / h, damp);
+    v.z = fm(fs(p.z, q.z) / h, damp);
     vel[i] = v;
     x0[i] = make_float4(p.x, p.y, p.z, q.w);
 }
@@ -89,20 +97,20 @@ __global__ void xpbd_stretch_kernel(float4* __restrict__ x, const float4* __rest
     float w0 = vm[ed.x].z, w1 = vm[ed.y].z;
     float lam = lambda[i];
     float L = rest[i], k = kst[i];
-    float dx = p1.x - p0.x, dy = p1.y - p0.y, dz = p1.z - p0.z;
-    float lsq = dx * dx + dy * dy + dz * dz;
-    if (lsq < 1e-8f) return;
+    float3 d = make_float3(fs(p1.x, p0.x), fs(p1.y, p0.y), fs(p1.z, p0.z));
+    float lsq = fdot(d, d);
+    if ((double)lsq < 1e-8) return;
     float l = sqrtf(lsq);
-    float C = l - L;
-    float gx = -(dx / l), gy = -(dy / l), gz = -(dz / l);
-    float alpha = k < kEps ? 1e9f : 1.f / ((k * h) * h);
-    float denom = alpha + (w0 + w1);
-    float dl = (-C - alpha * lam) / denom;
-    lambda[i] = lam + dl;
+    float C = fs(l, L);
+    float gx = -(d.x / l), gy = -(d.y / l), gz = -(d.z / l);
+    float alpha = k < kEps ? 1e9f : 1.f / fm(fm(k, h), h);
+    float denom = fa(alpha, fa(w0, w1));
+    float dl = fs(-C, fm(alpha, lam)) / denom;
+    lambda[i] = fa(lam, dl);
     if (denom != 0.f) {
-        float s0 = dl * w0, s1 = (-dl) * w1;
-        x[ed.x] = make_float4(p0.x + s0 * gx, p0.y + s0 * gy, p0.z + s0 * gz, p0.w);
-        x[ed.y] = make_float4(p1.x + s1 * gx, p1.y + s1 * gy, p1.z + s1 * gz, p1.w);
+        float s0 = fm(dl, w0), s1 = fm(-dl, w1);
+        x[ed.x] = make_float4(fa(p0.x, fm(s0, gx)), fa(p0.y, fm(s0, gy)), fa(p0.z, fm(s0, gz)), p0.w);
+        x[ed.y] = make_float4(fa(p1.x, fm(s1, gx)), fa(p1.y, fm(s1, gy)), fa(p1.z, fm(s1, gz)), p1.w);
     }
 }
 
@@ -129,13 +137,14 @@ __global__ void xpbd_bending_kernel(float4* __restrict__ x, const float4* __rest
         p[j] = make_float3(t.x, t.y, t.z);
         w[j] = vm[vid[j]].z;
     }
+    // C = 1/2 sum_ij Q_ij <x_i, x_j>
     float sum = 0.f;
 #pragma unroll
     for (int ii = 0; ii < 4; ++ii)
 #pragma unroll
-        for (int jj = 0; jj < 4; ++jj)
-            sum += Q[ii][jj] * (p[ii].x * p[jj].x + p[ii].y * p[jj].y + p[ii].z * p[jj].z);
-    float C = 0.5f * sum;
+        for (int jj = 0; jj < 4; ++jj) sum = fa(sum, fm(Q[ii][jj], fdot(p[ii], p[jj])));
+    float C = fm(0.5f, sum);
+    // gradient_i = sum_j Q_ij x_j (the negated force of the reference)
     float3 g[4];
     float denom = 0.f;
 #pragma unroll
@@ -143,26 +152,51 @@ __global__ void xpbd_bending_kernel(float4* __restrict__ x, const float4* __rest
         float gx = 0.f, gy = 0.f, gz = 0.f;
 #pragma unroll
         for (int jj = 0; jj < 4; ++jj) {
-            gx += Q[ii][jj] * p[jj].x;
-            gy += Q[ii][jj] * p[jj].y;
-            gz += Q[ii][jj] * p[jj].z;
+            gx = fa(gx, fm(Q[ii][jj], p[jj].x));
+            gy = fa(gy, fm(Q[ii][jj], p[jj].y));
+            gz = fa(gz, fm(Q[ii][jj], p[jj].z));
         }
         g[ii] = make_float3(gx, gy, gz);
-        denom += w[ii] * (gx * gx + gy * gy + gz * gz);
+        denom = fa(denom, fm(w[ii], fdot(g[ii], g[ii])));
     }
-    float alpha = kb < kEps ? 1e12f : 1.f / ((kb * h) * h);
-    denom += alpha;
+    float alpha = kb < kEps ? 1e12f : 1.f / fm(fm(kb, h), h);
+    denom = fa(denom, alpha);
     float lam = lambda[i];
-    float dl = (-C - alpha * lam) / denom;
-    lambda[i] = lam + dl;
+    float dl = fs(-C, fm(alpha, lam)) / denom;
+    lambda[i] = fa(lam, dl);
     if (denom != 0.f) {
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            float s = dl * w[j];
+            float s = fm(dl, w[j]);
             float4 t = x[vid[j]];
-            x[vid[j]] = make_float4(p[j].x + s * g[j].x, p[j].y + s * g[j].y, p[j].z + s * g[j].z, t.w);
+            x[vid[j]] = make_float4(fa(p[j].x, fm(s, g[j].x)), fa(p[j].y, fm(s, g[j].y)), fa(p[j].z, fm(s, g[j].z)), t.w);
         }
     }
+}
+
+// State I/O between the caller's vertex order (3 floats per vertex) and the layout.
+__global__ void scatter_state_kernel(const float* __restrict__ xc, const float* __restrict__ vc,
+                                     const int* __restrict__ to_caller, float4* __restrict__ x, float4* __restrict__ x0,
+                                     float4* __restrict__ vel, int n, int has_v) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const size_t o = 3 * (size_t)to_caller[i];
+    const float m = x0[i].w;
+    float4 p = make_float4(xc[o], xc[o + 1], xc[o + 2], m);
+    x0[i] = p;
+    x[i] = make_float4(p.x, p.y, p.z, 0.f);
+    vel[i] = has_v ? make_float4(vc[o], vc[o + 1], vc[o + 2], 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+__global__ void gather_state_kernel(const float4* __restrict__ src, const int* __restrict__ to_caller,
+                                    float* __restrict__ dst, int n) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const size_t o = 3 * (size_t)to_caller[i];
+    const float4 p = src[i];
+    dst[o] = p.x;
+    dst[o + 1] = p.y;
+    dst[o + 2] = p.z;
 }
 
 // ---- FP64 reductions (deterministic: fixed element -> thread assignment, fixed tree)
@@ -187,7 +221,7 @@ struct EnergyArgs {
     const float4* x0;
     const float4* vel;
     const float4* vm;
-    const float4* accel;
+    const float4* inst;
     int nv;
     const int2* edge;
     const float* rest;
@@ -209,9 +243,9 @@ __global__ void __launch_bounds__(kRedThreads) energy_kernel(EnergyArgs a) {
     const int t0 = blockIdx.x * blockDim.x + threadIdx.x;
     double ei = 0.0, es = 0.0, eb = 0.0;
     for (int i = t0; i < a.nv; i += stride) {
-        float4 p = a.x[i], q = a.x0[i], v = a.vel[i];
-        float4 acc = a.accel[__float_as_int(v.w)];
-        bool pinned = a.vm[i].y != 0.f;
+        float4 p = a.x[i], q = a.x0[i], v = a.vel[i], mv = a.vm[i];
+        float4 acc = a.inst[__float_as_int(mv.w)];
+        bool pinned = mv.y != 0.f;
         double ax = pinned ? 0.0 : acc.x, ay = pinned ? 0.0 : acc.y, az = pinned ? 0.0 : acc.z;
         double dx = (double)p.x - ((double)q.x + a.h * v.x + a.h * a.h * ax);
         double dy = (double)p.y - ((double)q.y + a.h * v.y + a.h * a.h * ay);
@@ -271,7 +305,7 @@ struct GradArgs {
     const float4* x0;
     const float4* vel;
     const float4* vm;
-    const float4* accel;
+    const float4* inst;
     const int* st_idx;
     const float* st_rest;
     const float* st_w;
@@ -297,12 +331,12 @@ __global__ void grad_kernel(GradArgs a) {
         a.g2[v] = 0.0;
         return;
     }
-    const float4 acc = a.accel[__float_as_int(vv.w)];
+    const float4 acc = a.inst[__float_as_int(mv.w)];
     const double h = a.h, m = p0.w;
     double gx = m / (h * h) * ((double)xv.x - ((double)p0.x + h * vv.x + h * h * acc.x));
     double gy = m / (h * h) * ((double)xv.y - ((double)p0.y + h * vv.y + h * h * acc.y));
     double gz = m / (h * h) * ((double)xv.z - ((double)p0.z + h * vv.z + h * h * acc.z));
-    const double ks = mv.w;
+    const double ks = acc.w;
     for (int row = 0; row < sd.w; ++row) {
         for (int r = 0; r < a.tpv; ++r) {
             const int e = sd.z + row * 32 + k * a.tpv + r;
@@ -329,12 +363,23 @@ __global__ void grad_kernel(GradArgs a) {
     a.g2[v] = gx * gx + gy * gy + gz * gz;
 }
 
-__global__ void __launch_bounds__(kRedThreads) segment_sum_kernel(const double* g2, const int* seg, double* out) {
+// Deterministic per-instance sum of g2 over the instance's layout range, two levels:
+// block (chunk j, instance i) sums a fixed strided subset, then one block per
+// instance adds the kSegChunks partials in order.
+constexpr int kSegChunks = 32;
+__global__ void __launch_bounds__(kRedThreads) segment_partial_kernel(const double* g2, const int* seg, double* partial) {
     __shared__ double sh[kRedThreads];
-    const int b = seg[blockIdx.x], e = seg[blockIdx.x + 1];
+    const int i = blockIdx.y, j = blockIdx.x;
+    const int b = seg[i], e = seg[i + 1];
     double v = 0.0;
-    for (int i = b + threadIdx.x; i < e; i += blockDim.x) v += g2[i];
+    for (int t = b + j * kRedThreads + threadIdx.x; t < e; t += kSegChunks * kRedThreads) v += g2[t];
     double s = block_sum(v, sh);
+    if (threadIdx.x == 0) partial[i * kSegChunks + j] = s;
+}
+
+__global__ void __launch_bounds__(kSegChunks) segment_final_kernel(const double* partial, double* out) {
+    __shared__ double sh[kSegChunks];
+    double s = block_sum(partial[blockIdx.x * kSegChunks + threadIdx.x], sh);
     if (threadIdx.x == 0) out[blockIdx.x] = sqrt(s);
 }
 
@@ -350,7 +395,7 @@ struct ats_cloth {
     int block = 128;
     float h = 0.f, h2inv = 0.f, damp = 1.f;
     // device arrays
-    DevBuf<float4> x, x0, vel, vm, accel;
+    DevBuf<float4> x, x0, vel, vm, inst;
     DevBuf<int> st_idx;
     DevBuf<float> st_rest, st_w;
     DevBuf<int4> slices;
@@ -363,18 +408,31 @@ struct ats_cloth {
     DevBuf<float> en_rest, en_k, en_q, en_kb;
     DevBuf<int4> en_bend;
     DevBuf<int> inst_seg;
-    // scratch for the FP64 reductions
-    DevBuf<double> partial, red_out, g2;
-    std::vector<int> color_slices;
+    DevBuf<int> to_caller;
+    DevBuf<float> io_x, io_v;  // caller-order staging of the state
+    // scratch of the FP64 reductions
+    DevBuf<double> partial, seg_partial, red_out, g2;
     cudaStream_t capture_stream = nullptr;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
-    // pinned staging for state I/O
-    std::vector<float> host4;
 
-    ~ats_cloth() {
+    void drop_graphs() {
         for (auto& g : graph)
-            if (g) cudaGraphExecDestroy(g);
+            if (g) {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
+    }
+    ~ats_cloth() {
+        drop_graphs();
         if (capture_stream) cudaStreamDestroy(capture_stream);
+    }
+    size_t device_bytes() const {
+        return x.bytes() + x0.bytes() + vel.bytes() + vm.bytes() + inst.bytes() + st_idx.bytes() + st_rest.bytes() +
+               st_w.bytes() + slices.bytes() + xs_edge.bytes() + xs_rest.bytes() + xs_k.bytes() + xs_lambda.bytes() +
+               xb_idx.bytes() + xb_q.bytes() + xb_lambda.bytes() + en_edge.bytes() + en_rest.bytes() + en_k.bytes() +
+               en_q.bytes() + en_kb.bytes() + en_bend.bytes() + inst_seg.bytes() + to_caller.bytes() + io_x.bytes() +
+               io_v.bytes() + partial.bytes() +
+               seg_partial.bytes() + red_out.bytes() + g2.bytes();
     }
 };
 
@@ -384,6 +442,10 @@ inline cudaStream_t S(ats_stream s) { return (cudaStream_t)s; }
 
 template <typename T, typename U>
 int upload(DevBuf<T>& d, const std::vector<U>& h, size_t count) {
+    if (d.p) {
+        cudaFree(d.p);
+        d.p = nullptr;
+    }
     ATS_CUDA(d.alloc(count));
     if (count) ATS_CUDA(cudaMemcpy(d.p, h.data(), count * sizeof(T), cudaMemcpyHostToDevice));
     return ATS_OK;
@@ -399,8 +461,32 @@ int check_device() {
     return ATS_OK;
 }
 
+int upload_stencil(ats_cloth* c) {
+    int r;
+    const Layout& L = c->L;
+    if ((r = upload(c->st_idx, L.st_idx, L.st_idx.size())) || (r = upload(c->st_rest, L.st_rest, L.st_rest.size())) ||
+        (r = upload(c->st_w, L.st_w, L.st_w.size())) || (r = upload(c->slices, L.slices, L.slices.size() / 4)))
+        return r;
+    return ATS_OK;
+}
+
+template <int TPV, int R>
+cudaError_t sweep_launch(dim3 grid, dim3 block, cudaStream_t st, const SweepArgs& a) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, vbd_sweep_kernel<TPV, R>, a);
+}
+
 int launch_sweep(ats_cloth* c, int color, cudaStream_t st) {
-    const int sb = c->color_slices[color], se = c->color_slices[color + 1];
+    const int sb = c->L.color_slices[color], se = c->L.color_slices[color + 1];
     if (se <= sb) return ATS_OK;
     SweepArgs a;
     a.x = c->x.p;
@@ -411,26 +497,30 @@ int launch_sweep(ats_cloth* c, int color, cudaStream_t st) {
     a.st_rest = c->st_rest.p;
     a.st_w = c->st_w.p;
     a.slices = c->slices.p;
-    a.accel = c->accel.p;
+    a.inst = c->inst.p;
     a.slice_begin = sb;
     a.slice_end = se;
     a.h = c->h;
     a.h2inv = c->h2inv;
     const int warps_per_block = c->block / 32;
-    const int grid = (se - sb + warps_per_block - 1) / warps_per_block;
+    const dim3 grid((se - sb + warps_per_block - 1) / warps_per_block), block(c->block);
+    cudaError_t e;
     switch (c->L.tpv) {
-        case 1: vbd_sweep_kernel<1><<<grid, c->block, 0, st>>>(a); break;
-        case 2: vbd_sweep_kernel<2><<<grid, c->block, 0, st>>>(a); break;
-        case 4: vbd_sweep_kernel<4><<<grid, c->block, 0, st>>>(a); break;
-        default: vbd_sweep_kernel<8><<<grid, c->block, 0, st>>>(a); break;
+        case 1: e = sweep_launch<1, 12>(grid, block, st, a); break;
+        case 2: e = sweep_launch<2, 6>(grid, block, st, a); break;
+        case 4: e = sweep_launch<4, 3>(grid, block, st, a); break;
+        default: e = sweep_launch<8, 2>(grid, block, st, a); break;
     }
-    ATS_CUDA(cudaGetLastError());
+    if (e != cudaSuccess) {
+        set_error(std::string("vbd sweep launch: ") + cudaGetErrorString(e));
+        return ATS_ERR_CUDA;
+    }
     return ATS_OK;
 }
 
 int launch_predict(ats_cloth* c, cudaStream_t st) {
     const int n = c->L.nv;
-    predict_kernel<<<(n + 255) / 256, 256, 0, st>>>(c->x.p, c->x0.p, c->vel.p, c->vm.p, c->accel.p, n, c->h);
+    predict_kernel<<<(n + 255) / 256, 256, 0, st>>>(c->x.p, c->x0.p, c->vel.p, c->vm.p, c->inst.p, n, c->h);
     ATS_CUDA(cudaGetLastError());
     return ATS_OK;
 }
@@ -466,22 +556,28 @@ int launch_xpbd_bending(ats_cloth* c, int color, cudaStream_t st) {
     return ATS_OK;
 }
 
+int enqueue_iterations(ats_cloth* c, int solver, int iterations, cudaStream_t st) {
+    int r;
+    for (int it = 0; it < iterations; ++it) {
+        if (solver == ATS_SOLVER_VBD) {
+            for (int col = 0; col < c->L.n_vcolors; ++col)
+                if ((r = launch_sweep(c, col, st))) return r;
+        } else {
+            for (int col = 0; col < c->L.n_scolors; ++col)
+                if ((r = launch_xpbd_stretch(c, col, st))) return r;
+            for (int col = 0; col < c->L.n_bcolors; ++col)
+                if ((r = launch_xpbd_bending(c, col, st))) return r;
+        }
+    }
+    return ATS_OK;
+}
+
 int enqueue_frame(ats_cloth* c, int solver, cudaStream_t st) {
     int r;
     for (int sub = 0; sub < c->prm.num_substep; ++sub) {
         if ((r = launch_predict(c, st))) return r;
         if (solver == ATS_SOLVER_XPBD && (r = launch_reset(c, st))) return r;
-        for (int it = 0; it < c->prm.iterations; ++it) {
-            if (solver == ATS_SOLVER_VBD) {
-                for (int col = 0; col < c->L.n_vcolors; ++col)
-                    if ((r = launch_sweep(c, col, st))) return r;
-            } else {
-                for (int col = 0; col < c->L.n_scolors; ++col)
-                    if ((r = launch_xpbd_stretch(c, col, st))) return r;
-                for (int col = 0; col < c->L.n_bcolors; ++col)
-                    if ((r = launch_xpbd_bending(c, col, st))) return r;
-            }
-        }
+        if ((r = enqueue_iterations(c, solver, c->prm.iterations, st))) return r;
         if ((r = launch_update(c, st))) return r;
     }
     return ATS_OK;
@@ -502,8 +598,8 @@ int ats_cloth_create(const ats_instance_desc* inst, int ninst, const ats_solver_
         set_error("ats_cloth_create: need implicit_dt > 0, num_substep > 0, iterations >= 0");
         return ATS_ERR_INVALID;
     }
-    int tpv = prm->threads_per_vertex ? prm->threads_per_vertex : 4;
-    int block = prm->block_size ? prm->block_size : 128;
+    const int tpv = prm->threads_per_vertex ? prm->threads_per_vertex : 4;
+    const int block = prm->block_size ? prm->block_size : 128;
     if (block % 32 || block < 32 || block > 256) {
         set_error("ats_cloth_create: block_size must be a multiple of 32 in [32, 256]");
         return ATS_ERR_INVALID;
@@ -528,10 +624,11 @@ int ats_cloth_create(const ats_instance_desc* inst, int ninst, const ats_solver_
         set_error("ats_cloth_create: out of memory");
         return ATS_ERR_NOMEM;
     }
-    if (!build_layout(topos, descs, tpv, c->L, err)) {
+    if (!build_layout(topos, descs, prm->gravity, tpv, c->L, err)) {
         set_error("ats_cloth_create: " + err);
         return ATS_ERR_INVALID;
     }
+    topos.clear();
     c->prm = *prm;
     c->prm.threads_per_vertex = tpv;
     c->prm.block_size = block;
@@ -540,18 +637,12 @@ int ats_cloth_create(const ats_instance_desc* inst, int ninst, const ats_solver_
     c->h2inv = 1.f / (c->h * c->h);
     c->damp = std::exp(-prm->damping * c->h);
     ATS_CUDA(cudaGetDevice(&c->device));
-    Layout& L = c->L;
+    const Layout& L = c->L;
     const size_t nv = L.nv;
     if ((r = upload(c->x, L.x0, nv)) || (r = upload(c->x0, L.x0, nv)) || (r = upload(c->vel, L.vel, nv)) ||
-        (r = upload(c->vm, L.vm, nv)))
+        (r = upload(c->vm, L.vm, nv)) || (r = upload(c->inst, L.inst, L.ninst)))
         return r;
-    std::vector<float> acc(4 * (size_t)L.ninst, 0.f);
-    for (int i = 0; i < L.ninst; ++i)
-        for (int k = 0; k < 3; ++k) acc[4 * i + k] = prm->gravity[k];
-    if ((r = upload(c->accel, acc, L.ninst))) return r;
-    if ((r = upload(c->st_idx, L.st_idx, L.st_idx.size())) || (r = upload(c->st_rest, L.st_rest, L.st_rest.size())) ||
-        (r = upload(c->st_w, L.st_w, L.st_w.size())) || (r = upload(c->slices, L.slices, L.slices.size() / 4)))
-        return r;
+    if ((r = upload_stencil(c.get()))) return r;
     if ((r = upload(c->xs_edge, L.xs_edge, L.xs_rest.size())) || (r = upload(c->xs_rest, L.xs_rest, L.xs_rest.size())) ||
         (r = upload(c->xs_k, L.xs_k, L.xs_k.size())))
         return r;
@@ -564,10 +655,13 @@ int ats_cloth_create(const ats_instance_desc* inst, int ninst, const ats_solver_
         (r = upload(c->en_q, L.en_q, L.en_q.size())) || (r = upload(c->en_kb, L.en_kb, L.en_kb.size())))
         return r;
     if ((r = upload(c->inst_seg, L.inst_vbegin, L.inst_vbegin.size()))) return r;
+    if ((r = upload(c->to_caller, L.to_caller, nv))) return r;
+    ATS_CUDA(c->io_x.alloc(3 * nv));
+    ATS_CUDA(c->io_v.alloc(3 * nv));
     ATS_CUDA(c->partial.alloc(3 * (size_t)kRedBlocks));
+    ATS_CUDA(c->seg_partial.alloc((size_t)kSegChunks * L.ninst));
     ATS_CUDA(c->red_out.alloc(std::max(3, L.ninst)));
     ATS_CUDA(c->g2.alloc(nv));
-    c->color_slices = L.color_slices;
     ATS_CUDA(cudaStreamCreateWithFlags(&c->capture_stream, cudaStreamNonBlocking));
     ATS_CUDA(cudaDeviceSynchronize());
     *out = c.release();
@@ -596,13 +690,7 @@ int ats_cloth_query(const ats_cloth* c, ats_cloth_info* info) {
     info->threads_per_vertex = c->L.tpv;
     info->block_size = c->block;
     info->stencil_slots = (int)c->L.st_idx.size();
-    info->device_bytes = (long long)(c->x.bytes() + c->x0.bytes() + c->vel.bytes() + c->vm.bytes() + c->accel.bytes() +
-                                     c->st_idx.bytes() + c->st_rest.bytes() + c->st_w.bytes() + c->slices.bytes() +
-                                     c->xs_edge.bytes() + c->xs_rest.bytes() + c->xs_k.bytes() + c->xs_lambda.bytes() +
-                                     c->xb_idx.bytes() + c->xb_q.bytes() + c->xb_lambda.bytes() + c->en_edge.bytes() +
-                                     c->en_rest.bytes() + c->en_k.bytes() + c->en_q.bytes() + c->en_kb.bytes() +
-                                     c->en_bend.bytes() + c->inst_seg.bytes() + c->partial.bytes() +
-                                     c->red_out.bytes() + c->g2.bytes());
+    info->device_bytes = (long long)c->device_bytes();
     return ATS_OK;
 }
 
@@ -611,34 +699,22 @@ int ats_set_state(ats_cloth* c, const float* x, const float* v, ats_stream strea
         set_error("ats_set_state: need a handle and positions");
         return ATS_ERR_INVALID;
     }
-    const Layout& L = c->L;
-    std::vector<float> hx(4 * (size_t)L.nv), hv(4 * (size_t)L.nv);
-    for (int lv = 0; lv < L.nv; ++lv) {
-        int o = L.to_caller[lv];
-        for (int k = 0; k < 3; ++k) {
-            hx[4 * (size_t)lv + k] = x[3 * (size_t)o + k];
-            hv[4 * (size_t)lv + k] = v ? v[3 * (size_t)o + k] : 0.f;
-        }
-        hx[4 * (size_t)lv + 3] = L.x0[4 * (size_t)lv + 3];  // mass
-        hv[4 * (size_t)lv + 3] = L.vel[4 * (size_t)lv + 3];  // instance id
-    }
     cudaStream_t st = S(stream);
-    ATS_CUDA(cudaMemcpyAsync(c->x0.p, hx.data(), hx.size() * sizeof(float), cudaMemcpyHostToDevice, st));
-    ATS_CUDA(cudaMemcpyAsync(c->vel.p, hv.data(), hv.size() * sizeof(float), cudaMemcpyHostToDevice, st));
-    ATS_CUDA(cudaMemcpyAsync(c->x.p, c->x0.p, c->x0.bytes(), cudaMemcpyDeviceToDevice, st));
+    const int n = c->L.nv;
+    ATS_CUDA(cudaMemcpyAsync(c->io_x.p, x, 12 * (size_t)n, cudaMemcpyHostToDevice, st));
+    if (v) ATS_CUDA(cudaMemcpyAsync(c->io_v.p, v, 12 * (size_t)n, cudaMemcpyHostToDevice, st));
+    scatter_state_kernel<<<(n + 255) / 256, 256, 0, st>>>(c->io_x.p, c->io_v.p, c->to_caller.p, c->x.p, c->x0.p,
+                                                          c->vel.p, n, v ? 1 : 0);
+    ATS_CUDA(cudaGetLastError());
     ATS_CUDA(cudaStreamSynchronize(st));
     return ATS_OK;
 }
 
-static int read_back(ats_cloth* c, const float4* src, float* dst, cudaStream_t st) {
-    const Layout& L = c->L;
-    c->host4.resize(4 * (size_t)L.nv);
-    ATS_CUDA(cudaMemcpyAsync(c->host4.data(), src, 16 * (size_t)L.nv, cudaMemcpyDeviceToHost, st));
-    ATS_CUDA(cudaStreamSynchronize(st));
-    for (int lv = 0; lv < L.nv; ++lv) {
-        int o = L.to_caller[lv];
-        for (int k = 0; k < 3; ++k) dst[3 * (size_t)o + k] = c->host4[4 * (size_t)lv + k];
-    }
+static int read_back(ats_cloth* c, const float4* src, float* dst, float* staging, cudaStream_t st) {
+    const int n = c->L.nv;
+    gather_state_kernel<<<(n + 255) / 256, 256, 0, st>>>(src, c->to_caller.p, staging, n);
+    ATS_CUDA(cudaGetLastError());
+    ATS_CUDA(cudaMemcpyAsync(dst, staging, 12 * (size_t)n, cudaMemcpyDeviceToHost, st));
     return ATS_OK;
 }
 
@@ -647,9 +723,12 @@ int ats_get_state(ats_cloth* c, float* x, float* v, ats_stream stream) {
         set_error("ats_get_state: need a handle and an output array");
         return ATS_ERR_INVALID;
     }
-    int r = read_back(c, c->x0.p, x, S(stream));
-    if (r || !v) return r;
-    return read_back(c, c->vel.p, v, S(stream));
+    cudaStream_t st = S(stream);
+    int r = read_back(c, c->x0.p, x, c->io_x.p, st);
+    if (!r && v) r = read_back(c, c->vel.p, v, c->io_v.p, st);
+    if (r) return r;
+    ATS_CUDA(cudaStreamSynchronize(st));
+    return ATS_OK;
 }
 
 int ats_get_positions(ats_cloth* c, float* x, ats_stream stream) {
@@ -657,7 +736,11 @@ int ats_get_positions(ats_cloth* c, float* x, ats_stream stream) {
         set_error("ats_get_positions: need a handle and an output array");
         return ATS_ERR_INVALID;
     }
-    return read_back(c, c->x.p, x, S(stream));
+    cudaStream_t st = S(stream);
+    int r = read_back(c, c->x.p, x, c->io_x.p, st);
+    if (r) return r;
+    ATS_CUDA(cudaStreamSynchronize(st));
+    return ATS_OK;
 }
 
 int ats_set_accel(ats_cloth* c, const float* accel, ats_stream stream) {
@@ -665,10 +748,10 @@ int ats_set_accel(ats_cloth* c, const float* accel, ats_stream stream) {
         set_error("ats_set_accel: null argument");
         return ATS_ERR_INVALID;
     }
-    std::vector<float> a(4 * (size_t)c->L.ninst, 0.f);
     for (int i = 0; i < c->L.ninst; ++i)
-        for (int k = 0; k < 3; ++k) a[4 * i + k] = accel[3 * i + k];
-    ATS_CUDA(cudaMemcpyAsync(c->accel.p, a.data(), a.size() * sizeof(float), cudaMemcpyHostToDevice, S(stream)));
+        for (int k = 0; k < 3; ++k) c->L.inst[4 * i + k] = accel[3 * i + k];
+    ATS_CUDA(cudaMemcpyAsync(c->inst.p, c->L.inst.data(), c->L.inst.size() * sizeof(float), cudaMemcpyHostToDevice,
+                             S(stream)));
     ATS_CUDA(cudaStreamSynchronize(S(stream)));
     return ATS_OK;
 }
@@ -684,6 +767,14 @@ int ats_vbd_color_sweep(ats_cloth* c, int color, ats_stream stream) {
         return ATS_ERR_INVALID;
     }
     return launch_sweep(c, color, S(stream));
+}
+
+int ats_vbd_iterations(ats_cloth* c, int iterations, ats_stream stream) {
+    if (!c || iterations < 0) {
+        set_error("ats_vbd_iterations: null handle or negative count");
+        return ATS_ERR_INVALID;
+    }
+    return enqueue_iterations(c, ATS_SOLVER_VBD, iterations, S(stream));
 }
 
 int ats_update_velocity(ats_cloth* c, ats_stream stream) {
@@ -749,6 +840,75 @@ int ats_frame_graph(ats_cloth* c, int solver, ats_stream stream) {
     return ATS_OK;
 }
 
+int ats_autotune(ats_cloth* c, int iterations, ats_stream stream, int* out_tpv, int* out_block) {
+    if (!c || iterations <= 0) {
+        set_error("ats_autotune: null handle or iterations <= 0");
+        return ATS_ERR_INVALID;
+    }
+    cudaStream_t st = S(stream);
+    // keep the iterate: the trial sweeps move it
+    DevBuf<float4> saved;
+    ATS_CUDA(saved.alloc(c->L.nv));
+    ATS_CUDA(cudaMemcpyAsync(saved.p, c->x.p, c->x.bytes(), cudaMemcpyDeviceToDevice, st));
+    cudaEvent_t e0, e1;
+    ATS_CUDA(cudaEventCreate(&e0));
+    ATS_CUDA(cudaEventCreate(&e1));
+    const int tpvs[4] = {1, 2, 4, 8};
+    const int blocks[3] = {64, 128, 256};
+    float best = 1e30f;
+    int best_tpv = c->L.tpv, best_block = c->block;
+    std::string err;
+    int r = ATS_OK;
+    for (int tpv : tpvs) {
+        if (!build_slices(c->L, tpv, err) || (r = upload_stencil(c))) {
+            if (!r) {
+                set_error("ats_autotune: " + err);
+                r = ATS_ERR_INVALID;
+            }
+            break;
+        }
+        for (int b : blocks) {
+            c->block = b;
+            if ((r = enqueue_iterations(c, ATS_SOLVER_VBD, 1, st))) break;  // warm-up
+            cudaEventRecord(e0, st);
+            if ((r = enqueue_iterations(c, ATS_SOLVER_VBD, iterations, st))) break;
+            cudaEventRecord(e1, st);
+            cudaError_t ce = cudaEventSynchronize(e1);
+            if (ce != cudaSuccess) {
+                set_error(std::string("ats_autotune: ") + cudaGetErrorString(ce));
+                r = ATS_ERR_CUDA;
+                break;
+            }
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (ms < best) {
+                best = ms;
+                best_tpv = tpv;
+                best_block = b;
+            }
+        }
+        if (r) break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (!r && (!build_slices(c->L, best_tpv, err) || (r = upload_stencil(c)))) {
+        if (!r) {
+            set_error("ats_autotune: " + err);
+            r = ATS_ERR_INVALID;
+        }
+    }
+    c->block = best_block;
+    c->prm.threads_per_vertex = c->L.tpv;
+    c->prm.block_size = best_block;
+    c->drop_graphs();
+    ATS_CUDA(cudaMemcpyAsync(c->x.p, saved.p, c->x.bytes(), cudaMemcpyDeviceToDevice, st));
+    ATS_CUDA(cudaStreamSynchronize(st));
+    if (r) return r;
+    if (out_tpv) *out_tpv = c->L.tpv;
+    if (out_block) *out_block = c->block;
+    return ATS_OK;
+}
+
 int ats_energy(ats_cloth* c, double* out3, ats_stream stream) {
     if (!c || !out3) {
         set_error("ats_energy: null argument");
@@ -760,7 +920,7 @@ int ats_energy(ats_cloth* c, double* out3, ats_stream stream) {
     a.x0 = c->x0.p;
     a.vel = c->vel.p;
     a.vm = c->vm.p;
-    a.accel = c->accel.p;
+    a.inst = c->inst.p;
     a.nv = c->L.nv;
     a.edge = c->en_edge.p;
     a.rest = c->en_rest.p;
@@ -792,7 +952,7 @@ int ats_residual(ats_cloth* c, double* out, ats_stream stream) {
     a.x0 = c->x0.p;
     a.vel = c->vel.p;
     a.vm = c->vm.p;
-    a.accel = c->accel.p;
+    a.inst = c->inst.p;
     a.st_idx = c->st_idx.p;
     a.st_rest = c->st_rest.p;
     a.st_w = c->st_w.p;
@@ -804,7 +964,10 @@ int ats_residual(ats_cloth* c, double* out, ats_stream stream) {
     const int blocks = (a.nslices * 32 + 127) / 128;
     grad_kernel<<<blocks, 128, 0, st>>>(a);
     ATS_CUDA(cudaGetLastError());
-    segment_sum_kernel<<<c->L.ninst, kRedThreads, 0, st>>>(c->g2.p, c->inst_seg.p, c->red_out.p);
+    segment_partial_kernel<<<dim3(kSegChunks, c->L.ninst), kRedThreads, 0, st>>>(c->g2.p, c->inst_seg.p,
+                                                                                   c->seg_partial.p);
+    ATS_CUDA(cudaGetLastError());
+    segment_final_kernel<<<c->L.ninst, kSegChunks, 0, st>>>(c->seg_partial.p, c->red_out.p);
     ATS_CUDA(cudaGetLastError());
     ATS_CUDA(cudaMemcpyAsync(out, c->red_out.p, c->L.ninst * sizeof(double), cudaMemcpyDeviceToHost, st));
     ATS_CUDA(cudaStreamSynchronize(st));

@@ -1,10 +1,11 @@
-// ats_kernels.cuh -- sm_100a kernels of the cloth solver.
+// ats_kernels.cuh -- the VBD colour-sweep kernel (sm_100a).
 //
-// Data layout in HBM (all float4 = 16 B, one 128-bit load per vertex record):
-//   x   [V]  current iterate, w unused
-//   x0  [V]  frame / substep start position, w = mass
-//   vel [V]  velocity, w = instance id (int bits)
-//   vm  [V]  {k_b * sum Q_oo (bending Hessian diagonal), pin boost (0 / 1e9), inverse mass, k_stretch}
+// Data layout in HBM (float4 = 16 B, one 128-bit load per vertex record):
+//   x     [V]  current iterate, w unused
+//   x0    [V]  frame / substep start position, w = mass
+//   vel   [V]  velocity, w unused
+//   vm    [V]  {k_b * sum Q_oo (bending Hessian diagonal), pin boost (0 / 1e9), inverse mass, instance id bits}
+//   inst  [I]  per instance {external acceleration xyz, k_stretch}
 // Vertices are ordered instance-major then colour-major, so the vertices of one
 // colour of one instance are contiguous and every own-vertex access of a sweep is
 // coalesced. The neighbour stencil of a vertex (1-ring plus the far corners of its
@@ -30,10 +31,48 @@ struct SweepArgs {
     const float* __restrict__ st_rest;
     const float* __restrict__ st_w;
     const int4* __restrict__ slices;
-    const float4* __restrict__ accel;  // per instance, xyz
+    const float4* __restrict__ inst;
     int slice_begin, slice_end;
     float h, h2inv;
 };
+
+// Programmatic dependent launch: a sweep may start while the previous sweep of the
+// stream drains; everything it reads before grid_dependency_wait() is constant for
+// the life of the handle (stencil, slices, per-vertex material, instance table),
+// everything after it (x, x0, vel) is ordered behind the previous kernel.
+__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void allow_dependent_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+// Accumulates one neighbour into the force f and the symmetric Hessian h.
+__device__ __forceinline__ void vbd_neighbour(float4 xv, float4 xu, float L, float w, float ks, float& fx, float& fy,
+                                              float& fz, float& h00, float& h01, float& h02, float& h11, float& h12,
+                                              float& h22) {
+    const float dx = xu.x - xv.x, dy = xu.y - xv.y, dz = xu.z - xv.z;
+    // quadratic bending in relative coordinates: -sum_u W_vu (x_u - x_v)
+    fx -= w * dx;
+    fy -= w * dy;
+    fz -= w * dz;
+    if (L >= 0.f) {
+        // mass-spring stretch towards neighbour u, d = x_u - x_v:
+        // f = k C d / l, He = k/l^2 d d^T + k max(1 - L/l, 0) (I - d d^T / l^2)
+        const float l = fmaxf(sqrtf(dx * dx + dy * dy + dz * dz), kEps);
+        const float inv = 1.f / l;
+        const float C = l - L;
+        const float kc = ks * C * inv;
+        fx += kc * dx;
+        fy += kc * dy;
+        fz += kc * dz;
+        const float xsq = inv * inv;
+        const float b = ks * fmaxf(1.f - L * inv, 0.f);
+        const float c = ks * xsq - b * xsq;
+        h00 += c * dx * dx + b;
+        h01 += c * dx * dy;
+        h02 += c * dx * dz;
+        h11 += c * dy * dy + b;
+        h12 += c * dy * dz;
+        h22 += c * dz * dz + b;
+    }
+}
 
 // One VBD colour sweep: for every vertex of the colour, inertia + mass-spring
 // stretch + quadratic bending gradient and Hessian (reference:
@@ -42,57 +81,67 @@ struct SweepArgs {
 // example2_async_iter.cpp:993-1014, all in registers (Hf never goes to memory).
 // Bending is linear in x, so the per-bending-edge terms -k_b sum_j Q[o][j] x_j are
 // merged per (vertex, neighbour) into one weight W and applied in relative
-// coordinates -sum_u W_vu (x_u - x_v), which is the same force because every row of
-// Q sums to zero.
-template <int TPV>
+// coordinates, the same force because every row of Q sums to zero.
+// R rows are loaded up front (all stencil entries, then all gathers) so that a
+// warp has R independent loads in flight; rows beyond R go through a loop.
+template <int TPV, int R>
 __global__ void __launch_bounds__(256) vbd_sweep_kernel(SweepArgs a) {
     const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     const int slice = a.slice_begin + warp;
-    if (slice >= a.slice_end) return;
     const int lane = threadIdx.x & 31;
+    if (slice >= a.slice_end) {
+        grid_dependency_wait();
+        allow_dependent_launch();
+        return;
+    }
     const int4 sd = __ldg(&a.slices[slice]);  // vbegin, nverts, entry offset, rows
     const int k = lane / TPV;
-    const bool active = k < sd.y;
+    const bool leader = k < sd.y && (lane % TPV) == 0;
     const int v = sd.x + min(k, sd.y - 1);
-    const float4 xv = a.x[v];
+    const int base = sd.z + lane;
+
+    // constant data: stencil rows, material, instance parameters
+    int u[R];
+    float L[R], w[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        if (r < sd.w) {
+            u[r] = __ldg(&a.st_idx[base + r * 32]);
+            L[r] = __ldg(&a.st_rest[base + r * 32]);
+            w[r] = __ldg(&a.st_w[base + r * 32]);
+        } else {
+            u[r] = v;
+            L[r] = -1.f;
+            w[r] = 0.f;
+        }
+    }
     const float4 mv = __ldg(&a.vm[v]);
-    const float ks = mv.w;
+    const float4 ip = __ldg(&a.inst[__float_as_int(mv.w)]);
+    const float ks = ip.w;
+
+    grid_dependency_wait();
+    allow_dependent_launch();
+
+    // positions and frame-start state (ordered behind the previous kernel)
+    const float4 xv = a.x[v];
+    float4 xu[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) xu[r] = a.x[u[r]];  // other colours: not written by this launch
+    float4 p0 = make_float4(0.f, 0.f, 0.f, 0.f), vv = p0;
+    if (leader) {
+        p0 = a.x0[v];
+        vv = a.vel[v];
+    }
 
     float fx = 0.f, fy = 0.f, fz = 0.f;
     float h00 = 0.f, h01 = 0.f, h02 = 0.f, h11 = 0.f, h12 = 0.f, h22 = 0.f;
-    const int base = sd.z + lane;
-#pragma unroll 4
-    for (int row = 0; row < sd.w; ++row) {
-        const int e = base + row * 32;
-        const int u = __ldg(&a.st_idx[e]);
-        const float L = __ldg(&a.st_rest[e]);
-        const float w = __ldg(&a.st_w[e]);
-        // neighbours belong to other colours: nothing in this launch writes them
-        const float4 xu = __ldg(&a.x[u]);
-        const float dx = xu.x - xv.x, dy = xu.y - xv.y, dz = xu.z - xv.z;
-        // quadratic bending, relative form
-        fx -= w * dx;
-        fy -= w * dy;
-        fz -= w * dz;
-        if (L >= 0.f) {
-            // mass-spring stretch towards neighbour u (d = x_u - x_v)
-            const float l = fmaxf(sqrtf(dx * dx + dy * dy + dz * dz), kEps);
-            const float inv = 1.f / l;
-            const float C = l - L;
-            const float kc = ks * C * inv;
-            fx += kc * dx;
-            fy += kc * dy;
-            fz += kc * dz;
-            const float xsq = inv * inv;
-            const float b = ks * fmaxf(1.f - L * inv, 0.f);
-            const float c = ks * xsq - b * xsq;
-            h00 += c * dx * dx + b;
-            h01 += c * dx * dy;
-            h02 += c * dx * dz;
-            h11 += c * dy * dy + b;
-            h12 += c * dy * dz;
-            h22 += c * dz * dz + b;
-        }
+#pragma unroll
+    for (int r = 0; r < R; ++r) vbd_neighbour(xv, xu[r], L[r], w[r], ks, fx, fy, fz, h00, h01, h02, h11, h12, h22);
+    for (int r = R; r < sd.w; ++r) {
+        const int e = base + r * 32;
+        const int uu = __ldg(&a.st_idx[e]);
+        vbd_neighbour(xv, a.x[uu], __ldg(&a.st_rest[e]), __ldg(&a.st_w[e]), ks, fx, fy, fz, h00, h01, h02, h11, h12,
+                      h22);
     }
     // reduce the TPV lanes of a vertex
 #pragma unroll
@@ -107,23 +156,20 @@ __global__ void __launch_bounds__(256) vbd_sweep_kernel(SweepArgs a) {
         h12 += __shfl_xor_sync(0xffffffffu, h12, o);
         h22 += __shfl_xor_sync(0xffffffffu, h22, o);
     }
-    if (!active || (lane % TPV) != 0) return;
+    if (!leader) return;
 
     // inertia: H += m/h^2 I (+1e9 I pinned), f += -m/h^2 ((x - x0) - v h) + m a
-    const float4 p0 = __ldg(&a.x0[v]);
-    const float4 vv = __ldg(&a.vel[v]);
-    const float4 acc = __ldg(&a.accel[__float_as_int(vv.w)]);
     const float m = p0.w;
     const float mh = m * a.h2inv;
-    fx += -mh * ((xv.x - p0.x) - vv.x * a.h) + m * acc.x;
-    fy += -mh * ((xv.y - p0.y) - vv.y * a.h) + m * acc.y;
-    fz += -mh * ((xv.z - p0.z) - vv.z * a.h) + m * acc.z;
+    fx += -mh * ((xv.x - p0.x) - vv.x * a.h) + m * ip.x;
+    fy += -mh * ((xv.y - p0.y) - vv.y * a.h) + m * ip.y;
+    fz += -mh * ((xv.z - p0.z) - vv.z * a.h) + m * ip.z;
     const float dg = mh + mv.y + mv.x;
     h00 += dg;
     h11 += dg;
     h22 += dg;
 
-    // symmetric 3x3 solve by adjugate / determinant
+    // symmetric 3x3 solve by adjugate / determinant, guarded by |det| > FLT_EPSILON
     const float c00 = h11 * h22 - h12 * h12;
     const float c01 = h02 * h12 - h01 * h22;
     const float c02 = h01 * h12 - h02 * h11;

@@ -188,18 +188,63 @@ bool build_topology(const ats_instance_desc& d, Topology& t, std::string& err) {
     return true;
 }
 
-bool build_layout(const std::vector<Topology>& topos, const std::vector<ats_instance_desc>& descs, int tpv,
-                  Layout& L, std::string& err) {
+bool build_slices(Layout& L, int tpv, std::string& err) {
     if (tpv != 1 && tpv != 2 && tpv != 4 && tpv != 8) {
         err = "threads_per_vertex must be 1, 2, 4 or 8";
         return false;
     }
-    L = Layout();
     L.tpv = tpv;
-    L.ninst = (int)topos.size();
     const int vps = 32 / tpv;  // vertices per slice (one warp)
+    L.st_idx.clear();
+    L.st_rest.clear();
+    L.st_w.clear();
+    L.slices.clear();
+    L.color_slices.assign(1, 0);
+    // entry (row, thread th) of a slice = vertex th / tpv, slot row * tpv + th % tpv
+    for (int c = 0; c < L.n_vcolors; ++c) {
+        for (int ri = L.run_off[c]; ri < L.run_off[c + 1]; ++ri) {
+            const int b = L.runs[2 * ri], e = L.runs[2 * ri + 1];
+            for (int s = b; s < e; s += vps) {
+                const int n = std::min(vps, e - s);
+                int width = 0;
+                for (int k = 0; k < n; ++k) width = std::max(width, L.nb_off[s + k + 1] - L.nb_off[s + k]);
+                const int rows = (width + tpv - 1) / tpv;
+                const size_t off = L.st_idx.size();
+                L.st_idx.resize(off + 32 * (size_t)rows);
+                L.st_rest.resize(off + 32 * (size_t)rows);
+                L.st_w.resize(off + 32 * (size_t)rows);
+                for (int row = 0; row < rows; ++row)
+                    for (int th = 0; th < 32; ++th) {
+                        const int k = th / tpv, slot = row * tpv + th % tpv;
+                        const size_t at = off + 32 * (size_t)row + th;
+                        const int self = s + std::min(k, n - 1);
+                        if (k < n && slot < L.nb_off[s + k + 1] - L.nb_off[s + k]) {
+                            const int q = L.nb_off[s + k] + slot;
+                            L.st_idx[at] = L.nb_u[q];
+                            L.st_rest[at] = L.nb_rest[q];
+                            L.st_w[at] = L.nb_w[q];
+                        } else {
+                            L.st_idx[at] = self;
+                            L.st_rest[at] = -1.f;
+                            L.st_w[at] = 0.f;
+                        }
+                    }
+                L.slices.push_back(s);
+                L.slices.push_back(n);
+                L.slices.push_back((int)off);
+                L.slices.push_back(rows);
+            }
+        }
+        L.color_slices.push_back((int)L.slices.size() / 4);
+    }
+    return true;
+}
+
+bool build_layout(const std::vector<Topology>& topos, const std::vector<ats_instance_desc>& descs, const float* gravity,
+                  int tpv, Layout& L, std::string& err) {
+    L = Layout();
+    L.ninst = (int)topos.size();
     L.inst_vbegin.assign(1, 0);
-    L.inst_orig_vbegin.assign(1, 0);
     for (const auto& t : topos) {
         L.nv += t.nv;
         L.ne += t.ne();
@@ -208,24 +253,27 @@ bool build_layout(const std::vector<Topology>& topos, const std::vector<ats_inst
         L.n_scolors = std::max(L.n_scolors, t.nsc());
         L.n_bcolors = std::max(L.n_bcolors, t.nbc());
         L.inst_vbegin.push_back(L.nv);
-        L.inst_orig_vbegin.push_back(L.nv);
     }
     L.to_layout.assign(L.nv, -1);
     L.to_caller.assign(L.nv, -1);
     L.x0.assign(4 * (size_t)L.nv, 0.f);
     L.vel.assign(4 * (size_t)L.nv, 0.f);
     L.vm.assign(4 * (size_t)L.nv, 0.f);
+    L.inst.assign(4 * (size_t)L.ninst, 0.f);
+    for (int i = 0; i < L.ninst; ++i) {
+        for (int k = 0; k < 3; ++k) L.inst[4 * i + k] = gravity[k];
+        L.inst[4 * i + 3] = descs[i].k_stretch;
+    }
 
     // vertex order: instance-major, colour-major, increasing vertex id in a colour
     std::vector<std::vector<int>> inst_colour_begin(L.ninst);  // layout id where colour c starts
     for (int i = 0; i < L.ninst; ++i) {
         const Topology& t = topos[i];
-        int base = L.inst_vbegin[i];
-        int p = base;
+        int p = L.inst_vbegin[i];
         for (int c = 0; c < t.nvc(); ++c) {
             inst_colour_begin[i].push_back(p);
             for (int k = t.vcol_off[c]; k < t.vcol_off[c + 1]; ++k) {
-                int orig = L.inst_orig_vbegin[i] + t.vcol[k];
+                int orig = L.inst_vbegin[i] + t.vcol[k];
                 L.to_layout[orig] = p;
                 L.to_caller[p] = orig;
                 ++p;
@@ -237,8 +285,20 @@ bool build_layout(const std::vector<Topology>& topos, const std::vector<ats_inst
             return false;
         }
     }
+    L.run_off.assign(1, 0);
+    for (int c = 0; c < L.n_vcolors; ++c) {
+        for (int i = 0; i < L.ninst; ++i) {
+            if (c >= topos[i].nvc()) continue;
+            int b = inst_colour_begin[i][c], e = inst_colour_begin[i][c + 1];
+            if (e > b) {
+                L.runs.push_back(b);
+                L.runs.push_back(e);
+            }
+        }
+        L.run_off.push_back((int)L.runs.size() / 2);
+    }
 
-    // per-vertex data and neighbour stencils (in layout ids)
+    // per-vertex data and neighbour lists (in layout ids, sorted by neighbour id)
     struct Nb {
         int u;
         float rest;
@@ -248,8 +308,7 @@ bool build_layout(const std::vector<Topology>& topos, const std::vector<ats_inst
     for (int i = 0; i < L.ninst; ++i) {
         const Topology& t = topos[i];
         const ats_instance_desc& d = descs[i];
-        const int ob = L.inst_orig_vbegin[i];
-        std::vector<double> hdiag(t.nv, 0.0);
+        const int ob = L.inst_vbegin[i];
         for (int v = 0; v < t.nv; ++v) {
             int lv = L.to_layout[ob + v];
             std::map<int, Nb> m;
@@ -259,12 +318,13 @@ bool build_layout(const std::vector<Topology>& topos, const std::vector<ats_inst
                 int lu = L.to_layout[ob + u];
                 m[lu] = Nb{lu, t.rest[e], 0.0};
             }
+            double hdiag = 0.0;
             for (int k = t.vb_off[v]; k < t.vb_off[v + 1]; ++k) {
                 int e = t.vb[k];
                 const int* be = &t.bending[4 * e];
                 int o = be[0] == v ? 0 : be[1] == v ? 1 : be[2] == v ? 2 : 3;
-                const float* Q = &t.q[16 * (size_t)e];  // Q[col][row], row-col symmetric
-                hdiag[v] += (double)Q[4 * o + o];
+                const float* Q = &t.q[16 * (size_t)e];  // Q[col][row], symmetric
+                hdiag += (double)Q[4 * o + o];
                 for (int j = 0; j < 4; ++j) {
                     if (j == o) continue;
                     int lu = L.to_layout[ob + be[j]];
@@ -273,65 +333,35 @@ bool build_layout(const std::vector<Topology>& topos, const std::vector<ats_inst
                     it->second.w += (double)Q[4 * o + j];
                 }
             }
-            for (auto& kv : m) sten[lv].push_back(kv.second);
-            const float kb = d.k_bend;
-            for (auto& nb : sten[lv]) nb.w = (double)kb * nb.w;
-            float mass = d.mass[v];
-            bool fixed = d.fixed[v] != 0;
+            const double kb = d.k_bend;
+            for (auto& kv : m) {
+                kv.second.w *= kb;
+                sten[lv].push_back(kv.second);
+            }
+            const float mass = d.mass[v];
+            const bool fixed = d.fixed[v] != 0;
             L.x0[4 * (size_t)lv + 0] = t.pos[3 * v];
             L.x0[4 * (size_t)lv + 1] = t.pos[3 * v + 1];
             L.x0[4 * (size_t)lv + 2] = t.pos[3 * v + 2];
             L.x0[4 * (size_t)lv + 3] = mass;
-            int inst = i;
-            std::memcpy(&L.vel[4 * (size_t)lv + 3], &inst, 4);
-            L.vm[4 * (size_t)lv + 0] = (float)((double)kb * hdiag[v]);
+            L.vm[4 * (size_t)lv + 0] = (float)(kb * hdiag);
             L.vm[4 * (size_t)lv + 1] = fixed ? 1e9f : 0.f;
             L.vm[4 * (size_t)lv + 2] = fixed ? 0.f : 1.0f / mass;
-            L.vm[4 * (size_t)lv + 3] = d.k_stretch;
+            int inst_id = i;
+            std::memcpy(&L.vm[4 * (size_t)lv + 3], &inst_id, 4);
         }
     }
-
-    // sliced-ELL: per (instance, colour) run of vertices, slices of vps vertices;
-    // entry (row s, thread t) of a slice = vertex t / tpv, slot s * tpv + t % tpv.
-    L.color_slices.assign(L.n_vcolors + 1, 0);
-    std::vector<std::vector<int>> per_colour(L.n_vcolors);
-    for (int c = 0; c < L.n_vcolors; ++c) {
-        for (int i = 0; i < L.ninst; ++i) {
-            if (c >= topos[i].nvc()) continue;
-            int b = inst_colour_begin[i][c], e = inst_colour_begin[i][c + 1];
-            for (int s = b; s < e; s += vps) {
-                int n = std::min(vps, e - s);
-                int width = 0;
-                for (int k = 0; k < n; ++k) width = std::max(width, (int)sten[s + k].size());
-                int rows = (width + tpv - 1) / tpv;
-                int off = (int)L.st_idx.size();
-                L.st_idx.resize(off + 32 * (size_t)rows);
-                L.st_rest.resize(off + 32 * (size_t)rows);
-                L.st_w.resize(off + 32 * (size_t)rows);
-                for (int row = 0; row < rows; ++row)
-                    for (int th = 0; th < 32; ++th) {
-                        int k = th / tpv, slot = row * tpv + th % tpv;
-                        size_t at = off + 32 * (size_t)row + th;
-                        int self = s + std::min(k, n - 1);
-                        if (k < n && slot < (int)sten[s + k].size()) {
-                            const Nb& nb = sten[s + k][slot];
-                            L.st_idx[at] = nb.u;
-                            L.st_rest[at] = nb.rest;
-                            L.st_w[at] = (float)nb.w;
-                        } else {
-                            L.st_idx[at] = self;
-                            L.st_rest[at] = -1.f;
-                            L.st_w[at] = 0.f;
-                        }
-                    }
-                L.slices.push_back(s);
-                L.slices.push_back(n);
-                L.slices.push_back(off);
-                L.slices.push_back(rows);
-            }
+    L.nb_off.assign(1, 0);
+    for (int lv = 0; lv < L.nv; ++lv) {
+        for (const Nb& nb : sten[lv]) {
+            L.nb_u.push_back(nb.u);
+            L.nb_rest.push_back(nb.rest);
+            L.nb_w.push_back((float)nb.w);
         }
-        L.color_slices[c + 1] = (int)L.slices.size() / 4;
+        L.nb_off.push_back((int)L.nb_u.size());
     }
+    sten.clear();
+    if (!build_slices(L, tpv, err)) return false;
 
     // XPBD constraints, colour-major over instances (example2_async_iter.cpp:648-695)
     L.xs_color.assign(1, 0);
@@ -339,7 +369,7 @@ bool build_layout(const std::vector<Topology>& topos, const std::vector<ats_inst
         for (int i = 0; i < L.ninst; ++i) {
             const Topology& t = topos[i];
             if (c >= t.nsc()) continue;
-            const int ob = L.inst_orig_vbegin[i];
+            const int ob = L.inst_vbegin[i];
             for (int k = t.scol_off[c]; k < t.scol_off[c + 1]; ++k) {
                 int e = t.scol[k];
                 L.xs_edge.push_back(L.to_layout[ob + t.edges[2 * e]]);
@@ -355,7 +385,7 @@ bool build_layout(const std::vector<Topology>& topos, const std::vector<ats_inst
         for (int i = 0; i < L.ninst; ++i) {
             const Topology& t = topos[i];
             if (c >= t.nbc()) continue;
-            const int ob = L.inst_orig_vbegin[i];
+            const int ob = L.inst_vbegin[i];
             for (int k = t.bcol_off[c]; k < t.bcol_off[c + 1]; ++k) {
                 int e = t.bcol[k];
                 for (int j = 0; j < 4; ++j) L.xb_idx.push_back(L.to_layout[ob + t.bending[4 * e + j]]);
@@ -372,7 +402,7 @@ bool build_layout(const std::vector<Topology>& topos, const std::vector<ats_inst
     // energy terms in original element order
     for (int i = 0; i < L.ninst; ++i) {
         const Topology& t = topos[i];
-        const int ob = L.inst_orig_vbegin[i];
+        const int ob = L.inst_vbegin[i];
         for (int e = 0; e < t.ne(); ++e) {
             L.en_edge.push_back(L.to_layout[ob + t.edges[2 * e]]);
             L.en_edge.push_back(L.to_layout[ob + t.edges[2 * e + 1]]);

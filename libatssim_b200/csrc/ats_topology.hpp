@@ -48,18 +48,24 @@ struct Layout {
     int tpv = 4;          // lanes per vertex in the VBD sweep
     int nv = 0, ne = 0, nb = 0, ninst = 0;
     int n_vcolors = 0, n_scolors = 0, n_bcolors = 0;
-    std::vector<int> inst_vbegin;   // ninst + 1, in layout order
-    std::vector<int> inst_orig_vbegin;  // ninst + 1, caller order
+    std::vector<int> inst_vbegin;   // ninst + 1, in layout order (= caller order offsets)
     std::vector<int> to_layout;     // caller vertex id -> layout id
     std::vector<int> to_caller;     // layout id -> caller vertex id
     // per-vertex, layout order (float4 as 4 floats)
     std::vector<float> x0;          // xyz rest position, w = mass
-    std::vector<float> vel;         // xyz 0, w = instance id (int bits)
-    std::vector<float> vm;          // {bending Hessian diagonal k_b sum Q_oo, pin boost (0 / 1e9), inv mass, k_stretch}
-    // sliced-ELL stencil: slice = 32/tpv vertices, row r holds 32 entries
+    std::vector<float> vel;         // zeros
+    std::vector<float> vm;          // {bending Hessian diagonal k_b sum Q_oo, pin boost (0 / 1e9), inv mass, instance id bits}
+    std::vector<float> inst;        // per instance {gravity xyz, k_stretch}
+    // neighbour lists (CSR, layout order): neighbour id, rest length (-1 = not an
+    // edge), bending weight k_b sum_b Q_b[o_v][o_u]
+    std::vector<int> nb_off, nb_u;
+    std::vector<float> nb_rest, nb_w;
+    std::vector<int> runs;          // per colour c: runs[c] .. runs of (begin, end) layout ranges
+    std::vector<int> run_off;       // n_vcolors + 1 offsets into runs (pairs)
+    // sliced-ELL stencil for the current tpv: slice = 32/tpv vertices, row r holds 32 entries
     std::vector<int> st_idx;        // neighbour layout id (self for padding)
     std::vector<float> st_rest;     // rest length, -1 = not an edge (bending-only neighbour or padding)
-    std::vector<float> st_w;        // k_b * sum_b Q_b[o_v][o_u]
+    std::vector<float> st_w;        // bending weight
     std::vector<int> slices;        // 4 ints per slice: vbegin, nverts, entry offset, rows
     std::vector<int> color_slices;  // n_vcolors + 1 offsets into slices
     // XPBD, colour-major over all instances
@@ -73,11 +79,13 @@ struct Layout {
     std::vector<int> en_edge;       // 2 per edge
     std::vector<float> en_rest, en_k;
     std::vector<int> en_bend;       // 4 per bending edge
-    std::vector<float> en_q;        // 16 per bending edge (column-major), times 1 (k_b separate)
+    std::vector<float> en_q;        // 16 per bending edge (column-major)
     std::vector<float> en_kb;
 };
 
-bool build_layout(const std::vector<Topology>& topos, const std::vector<ats_instance_desc>& descs, int tpv,
-                  Layout& L, std::string& err);
+bool build_layout(const std::vector<Topology>& topos, const std::vector<ats_instance_desc>& descs, const float* gravity,
+                  int tpv, Layout& L, std::string& err);
+// (Re)builds the sliced-ELL stencil of L for `tpv` lanes per vertex.
+bool build_slices(Layout& L, int tpv, std::string& err);
 
 }  // namespace ats

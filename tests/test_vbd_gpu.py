@@ -1,0 +1,222 @@
+"""CUDA VBD / XPBD against the CPU oracle, through the C ABI.
+
+Bars: positions within 1e-4 relative L2 after 30 frames in FP32 (FP32 summation
+order differs: the CUDA sweep merges bending terms per neighbour); FP64 energies
+and residuals within 1e-6 relative of the oracle's on the same positions.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from libatssim_b200 import configs
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def oracle_scene(oracle, inst, prm, threads=4):
+    return oracle.Scene(inst.positions, inst.faces, inst.mass, inst.fixed, dt=prm["implicit_dt"],
+                        substeps=prm["num_substep"], iterations=prm["iterations"], k_stretch=inst.k_stretch,
+                        k_bend=inst.k_bend, damping=prm["damping"], threads=threads)
+
+
+def perturbed_state(inst, seed, vscale=0.3, xscale=1e-3):
+    rng = np.random.RandomState(seed)
+    x = inst.positions + xscale * rng.standard_normal(inst.positions.shape).astype(np.float32)
+    v = vscale * rng.standard_normal(inst.positions.shape).astype(np.float32)
+    return x.astype(np.float32), v
+
+
+@pytest.mark.parametrize("tpv", [1, 2, 4, 8])
+def test_one_frame_matches_oracle(ats, oracle, tpv):
+    insts, prm = configs.c0()
+    prm = dict(prm, iterations=3)
+    inst = insts[0]
+    x, v = perturbed_state(inst, seed=tpv)
+    cloth = ats.Cloth(insts, threads_per_vertex=tpv, **prm)
+    cloth.set_state(x, v)
+    cloth.frame()
+    xg, vg = cloth.state()
+    s = oracle_scene(oracle, inst, prm)
+    s.set_state(x, v)
+    s.frame()
+    xo, vo = s.state()
+    assert rel_l2(xg, xo) < 1e-6
+    assert rel_l2(vg - v, vo - v) < 1e-4
+
+
+def test_c0_thirty_frames_vbd(ats, oracle):
+    insts, prm = configs.c0()
+    cloth = ats.Cloth(insts, **prm)
+    s = oracle_scene(oracle, insts[0], prm, threads=8)
+    for _ in range(30):
+        cloth.frame(graph=True)
+    s.run(30)
+    xg, vg = cloth.state()
+    xo, vo = s.state()
+    rest = insts[0].positions
+    err = rel_l2(xg, xo)
+    assert err < 1e-4, err
+    # the cloth has fallen well away from rest: the comparison is not trivial
+    assert np.linalg.norm(xo - rest) / np.linalg.norm(rest) > 0.05
+    assert rel_l2(xg - rest, xo - rest) < 1e-3
+
+
+def test_c0_thirty_frames_xpbd(ats, oracle):
+    insts, prm = configs.c0()
+    prm = dict(prm, iterations=20)
+    cloth = ats.Cloth(insts, **prm)
+    s = oracle_scene(oracle, insts[0], prm, threads=8)
+    for _ in range(30):
+        cloth.frame(ats.SOLVER_XPBD)
+    s.run(30, solver="xpbd")
+    xg, _ = cloth.state()
+    xo, _ = s.state()
+    # predict / update / XPBD kernels round every term as the oracle does
+    assert rel_l2(xg, xo) < 1e-6
+
+
+def test_square8k_energy_log_matches_reference(ats, oracle):
+    """GPU reproduction of documents/example2_async_convergence.py:78-80."""
+    m = np.load(os.path.join(GOLD, "square8k_mesh.npz"))
+    insts, prm = configs.reference_square(m["positions"], m["faces"])
+    cloth = ats.Cloth(insts, **prm)
+    for _ in range(30):
+        cloth.frame(graph=True)
+    gold = np.array(json.load(open(os.path.join(GOLD, "example2_energy_frame30.json")))["list_sync"])
+    cloth.predict()
+    log = [cloth.energy()[:2].sum()]
+    for _ in range(100):
+        for c in range(cloth.info.num_vertex_colors):
+            cloth.vbd_color_sweep(c)
+        log.append(cloth.energy()[:2].sum())
+    cloth.update_velocity()
+    log = np.array(log)
+    assert np.max(np.abs(log - gold) / gold) < 2e-5
+    assert (np.diff(log) < 0).all()
+
+
+def test_energy_and_residual_match_oracle(ats, oracle):
+    insts, prm = configs.c0()
+    inst = insts[0]
+    x, v = perturbed_state(inst, seed=7, vscale=0.1)
+    cloth = ats.Cloth(insts, **prm)
+    cloth.set_state(x, v)
+    cloth.predict()
+    for c in range(cloth.info.num_vertex_colors):
+        cloth.vbd_color_sweep(c)
+    xm = cloth.positions()
+    s = oracle_scene(oracle, inst, prm)
+    s.set_state(x, v)
+    s.begin_frame()
+    e = cloth.energy()
+    eo = s.energy_of(xm, with_bending=False)
+    assert abs(e[0] + e[1] - eo) / eo < 1e-6
+    r = cloth.residual()[0]
+    ro = s.grad_norm_of(xm)
+    assert abs(r - ro) / ro < 1e-6
+
+
+def test_graph_replay_is_bit_identical_to_eager(ats):
+    insts, prm = configs.c0()
+    a = ats.Cloth(insts, **prm)
+    b = ats.Cloth(insts, **prm)
+    for _ in range(3):
+        a.frame()
+        b.frame(graph=True)
+    xa, va = a.state()
+    xb, vb = b.state()
+    assert np.array_equal(xa, xb) and np.array_equal(va, vb)
+
+
+def test_lane_variants_agree(ats):
+    insts, prm = configs.c0()
+    out = []
+    for tpv in (1, 2, 4, 8):
+        c = ats.Cloth(insts, threads_per_vertex=tpv, **prm)
+        for _ in range(5):
+            c.frame(graph=True)
+        out.append(c.state()[0])
+    for o in out[1:]:
+        assert rel_l2(o, out[0]) < 1e-5
+
+
+def test_autotune_keeps_state_and_parity(ats, oracle):
+    insts, prm = configs.c0()
+    cloth = ats.Cloth(insts, **prm)
+    cloth.frame()
+    x_before = cloth.positions()
+    tpv, block = cloth.autotune(iterations=2)
+    assert tpv in (1, 2, 4, 8) and block in (64, 128, 256)
+    assert cloth.info.threads_per_vertex == tpv and cloth.info.block_size == block
+    assert np.array_equal(cloth.positions(), x_before)
+    for _ in range(9):
+        cloth.frame(graph=True)
+    s = oracle_scene(oracle, insts[0], prm, threads=8)
+    s.run(10)
+    assert rel_l2(cloth.state()[0], s.state()[0]) < 1e-4
+
+
+def test_batched_instances_equal_separate_handles(ats):
+    insts, prm = configs.c2(num_instances=5, seed=3, side_range=(8, 40))
+    prm = dict(prm, iterations=10)
+    batch = ats.Cloth(insts, **prm)
+    for _ in range(3):
+        batch.frame(graph=True)
+    xb, vb = batch.state()
+    off = 0
+    for inst in insts:
+        one = ats.Cloth([inst], **prm)
+        for _ in range(3):
+            one.frame()
+        x1, v1 = one.state()
+        n = inst.num_verts
+        assert np.array_equal(xb[off:off + n], x1)
+        assert np.array_equal(vb[off:off + n], v1)
+        off += n
+
+
+def test_residual_decreases_over_iterations(ats):
+    insts, prm = configs.c0()
+    cloth = ats.Cloth(insts, **prm)
+    for _ in range(5):
+        cloth.frame()
+    cloth.predict()
+    r0 = cloth.residual()[0]
+    for _ in range(50):
+        for c in range(cloth.info.num_vertex_colors):
+            cloth.vbd_color_sweep(c)
+    assert cloth.residual()[0] < 0.5 * r0
+
+
+def test_pinned_vertices_stay(ats, oracle):
+    """Pins are the reference's 1e9 penalty on the inertia Hessian
+    (xpbd_constraints.h:4056-4060), so they move by (tension / 1e9) per iteration."""
+    insts, prm = configs.c0()
+    cloth = ats.Cloth(insts, **prm)
+    s = oracle_scene(oracle, insts[0], prm, threads=8)
+    for _ in range(10):
+        cloth.frame(graph=True)
+    s.run(10)
+    x, _ = cloth.state()
+    xo, _ = s.state()
+    pinned = insts[0].fixed.astype(bool)
+    drift = np.abs(x[pinned] - insts[0].positions[pinned]).max()
+    drift_o = np.abs(xo[pinned] - insts[0].positions[pinned]).max()
+    assert drift < 1e-4 and abs(drift - drift_o) < 0.05 * drift_o + 1e-9
+    assert x[~pinned, 1].min() < -0.1
+
+
+def test_bad_color_is_rejected(ats):
+    insts, prm = configs.c0()
+    cloth = ats.Cloth(insts, **prm)
+    with pytest.raises(ats.AtsError):
+        cloth.vbd_color_sweep(cloth.info.num_vertex_colors)
+    with pytest.raises(ats.AtsError):
+        cloth.xpbd_stretch_color(-1)
