@@ -191,6 +191,27 @@ int ats_energy(ats_cloth* cloth, double* out3, ats_stream stream);
  * y = x0 + h v + h^2 a). Synchronises `stream`. */
 int ats_residual(ats_cloth* cloth, double* out_per_instance, ats_stream stream);
 
+/* FP64 energy of one cloth state given as plain device arrays, with no device
+ * allocation. It has no counterpart in the reference. It is for callers that cannot
+ * call cudaMalloc: programs whose GPU memory belongs to their own allocator (an
+ * engine or framework that reserves the device heap up front), or per-frame loops
+ * that cannot afford the device-wide synchronisation cudaMalloc / cudaFree may
+ * cause. The caller passes device arrays in its own vertex order: x, x_start, v
+ * (3 floats per vertex), mass, fixed (num_verts), edges (2 ints each) with
+ * rest_length, bending (4 ints each) with q (16 floats each, column-major as
+ * ats_topology_rest returns it); accel is 3 host floats, h the substep dt. out3
+ * (device, 3 doubles) receives inertia, stretch and bending, the terms ats_energy
+ * computes. Scratch is a static 96 KiB device array that every GPU which loads the
+ * library keeps until exit: at most 8,388,608 vertices, edges and bending edges per
+ * call (larger calls fail with ATS_ERR_INVALID). The first call on a device looks
+ * up that array's device address; make that first call before any stream capture.
+ * Calls share the array: calls that overlap on the GPU race and may return wrong
+ * sums. Enqueues on `stream` and returns without synchronising. */
+int ats_energy_noalloc(const float* x, const float* x_start, const float* v, const float* mass,
+                       const unsigned char* fixed, int num_verts, const int* edges, const float* rest_length,
+                       int num_edges, const int* bending, const float* q, int num_bending_edges, float k_stretch,
+                       float k_bend, const float* accel, float h, double* out3, ats_stream stream);
+
 /* Message of the last failed call on this thread ("" if none). */
 const char* ats_last_error(void);
 

@@ -107,6 +107,8 @@ _SIGNATURES = {
     "ats_autotune": [_vp, ctypes.c_int, _vp, _ip, _ip],
     "ats_energy": [_vp, _dp, _vp],
     "ats_residual": [_vp, _dp, _vp],
+    "ats_energy_noalloc": [_vp, _vp, _vp, _vp, _vp, ctypes.c_int, _vp, _vp, ctypes.c_int, _vp, _vp, ctypes.c_int,
+                           ctypes.c_float, ctypes.c_float, _fp, ctypes.c_float, _vp, _vp],
 }
 
 
@@ -143,6 +145,17 @@ def _stream(stream):
     if hasattr(stream, "cuda_stream"):
         return ctypes.c_void_p(stream.cuda_stream)
     return ctypes.c_void_p(int(stream))
+
+
+def energy_noalloc(x, x_start, v, mass, fixed, num_verts, edges, rest_length, num_edges, bending, q,
+                   num_bending_edges, k_stretch, k_bend, accel, h, out3, stream=None):
+    """ats_energy_noalloc: FP64 energy terms of plain device arrays (all array
+    arguments are device addresses as ints) into the device array out3, using only
+    the library's static scratch (no device allocation). Enqueues on `stream`."""
+    acc = np.ascontiguousarray(accel, dtype=np.float32)
+    _check(lib().ats_energy_noalloc(x, x_start, v, mass, fixed, int(num_verts), edges, rest_length, int(num_edges),
+                                    bending, q, int(num_bending_edges), float(k_stretch), float(k_bend),
+                                    _p(acc, ctypes.c_float), float(h), out3, _stream(stream)))
 
 
 # ---------------------------------------------------------------- mesh helpers
