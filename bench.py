@@ -27,7 +27,6 @@ timing is the max over ranks.
 import argparse
 import json
 import os
-import subprocess
 import sys
 import threading
 import time
@@ -68,55 +67,56 @@ def alg_bytes_per_iter(nv, ne, nb):
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    """SM clock and throttle reasons polled through NVML during the timed region
+    (nvidia-smi's 200 ms period is longer than the region itself)."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+               0x80: "hw_power_brake_slowdown"}
 
-    def __init__(self, gpu):
-        self.gpu = gpu
-        self.proc = None
-        self.lines = []
+    def __init__(self, torch_device):
+        self.dev = torch_device
+        self.samples = []
+        self.reasons = set()
+        self.stop_flag = False
+        self.handle = None
+        self.max_mhz = None
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
-        except Exception:
-            self.proc = None
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            pr = torch.cuda.get_device_properties(self.dev)
+            bus = "%08X:%02X:%02X.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+            self.handle = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.handle, pynvml.NVML_CLOCK_SM)
+            self.nvml = pynvml
+        except Exception as e:  # no NVML: report it
+            self.error = str(e)
+            return
+        self.t = threading.Thread(target=self._poll, daemon=True)
+        self.t.start()
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def _poll(self):
+        nv = self.nvml
+        while not self.stop_flag:
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self.handle, nv.NVML_CLOCK_SM))
+                mask = nv.nvmlDeviceGetCurrentClocksEventReasons(self.handle)
+                for bit, name in self.REASONS.items():
+                    if mask & bit:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(0.002)
 
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                smax.append(float(f[2]))
-            except ValueError:
-                continue
-            for n, val in zip(names, f[5:9]):
-                if val.lower() == "active":
-                    reasons.add(n)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        self.stop_flag = True
+        if self.handle is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "note": getattr(self, "error", "no NVML")}
+        self.t.join(timeout=2)
+        return {"sm_mhz": float(np.median(self.samples)) if self.samples else None, "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
 
 
 def cpu_port_sample(threads, iters):
@@ -162,10 +162,11 @@ def profile_traffic():
     p = os.path.join(ROOT, "profiles", "vbd_sweep_c1_ncu.json")
     if os.path.exists(p):
         try:
-            return json.load(open(p)).get("dram_bytes_per_launch")
+            d = json.load(open(p))
+            return d.get("dram_bytes_per_launch"), d.get("dram_bytes_per_launch_warm")
         except Exception:
-            return None
-    return None
+            return None, None
+    return None, None
 
 
 def run_ours(args):
@@ -272,6 +273,7 @@ def run_ours(args):
         e2e_s = float(t.item())
     state_bytes = 2 * 3 * 4 * info.num_verts
 
+    traffic = profile_traffic()
     out = None
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -288,7 +290,7 @@ def run_ours(args):
                "e2e": {"value": world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": state_bytes,
                        "d2h_bytes_per_step": state_bytes},
                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                            "frac": achieved / peak, "traffic": profile_traffic(),
+                            "frac": achieved / peak, "traffic": traffic[0], "traffic_warm_in_frame": traffic[1],
                             "kernel": f"vbd_sweep_kernel<{info.threads_per_vertex}>", "mean_launch_us": mean_sweep_ms * 1e3,
                             "alg_bytes_per_launch": bytes_launch, "peak_source": peak_src},
                "gpu_launches": args.steps * (2 + ITERS * info.num_vertex_colors),

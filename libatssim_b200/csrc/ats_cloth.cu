@@ -306,9 +306,8 @@ struct GradArgs {
     const float4* vel;
     const float4* vm;
     const float4* inst;
-    const int* st_idx;
+    const int2* st_iw;
     const float* st_rest;
-    const float* st_w;
     const int4* slices;
     int nslices;
     int tpv;
@@ -337,18 +336,20 @@ __global__ void grad_kernel(GradArgs a) {
     double gy = m / (h * h) * ((double)xv.y - ((double)p0.y + h * vv.y + h * h * acc.y));
     double gz = m / (h * h) * ((double)xv.z - ((double)p0.z + h * vv.z + h * h * acc.z));
     const double ks = acc.w;
-    for (int row = 0; row < sd.w; ++row) {
+    const int rows = sd.w & 0xffff, erows = sd.w >> 16;
+    for (int row = 0; row < rows; ++row) {
         for (int r = 0; r < a.tpv; ++r) {
             const int e = sd.z + row * 32 + k * a.tpv + r;
-            const int u = a.st_idx[e];
+            const int2 iw = a.st_iw[e];
+            const int u = iw.x;
             if (u == v) continue;
             const float4 xu = a.x[u];
             const double dx = (double)xu.x - xv.x, dy = (double)xu.y - xv.y, dz = (double)xu.z - xv.z;
-            const double w = a.st_w[e];
+            const double w = __int_as_float(iw.y);
             gx += w * dx;
             gy += w * dy;
             gz += w * dz;
-            const double L = a.st_rest[e];
+            const double L = row < erows ? a.st_rest[e] : -1.0;
             if (L >= 0.0) {
                 const double l = sqrt(dx * dx + dy * dy + dz * dz);
                 if (l > 0.0) {
@@ -396,8 +397,8 @@ struct ats_cloth {
     float h = 0.f, h2inv = 0.f, damp = 1.f;
     // device arrays
     DevBuf<float4> x, x0, vel, vm, inst;
-    DevBuf<int> st_idx;
-    DevBuf<float> st_rest, st_w;
+    DevBuf<int2> st_iw;
+    DevBuf<float> st_rest;
     DevBuf<int4> slices;
     DevBuf<int2> xs_edge;
     DevBuf<float> xs_rest, xs_k, xs_lambda;
@@ -427,8 +428,8 @@ struct ats_cloth {
         if (capture_stream) cudaStreamDestroy(capture_stream);
     }
     size_t device_bytes() const {
-        return x.bytes() + x0.bytes() + vel.bytes() + vm.bytes() + inst.bytes() + st_idx.bytes() + st_rest.bytes() +
-               st_w.bytes() + slices.bytes() + xs_edge.bytes() + xs_rest.bytes() + xs_k.bytes() + xs_lambda.bytes() +
+        return x.bytes() + x0.bytes() + vel.bytes() + vm.bytes() + inst.bytes() + st_iw.bytes() + st_rest.bytes() +
+               slices.bytes() + xs_edge.bytes() + xs_rest.bytes() + xs_k.bytes() + xs_lambda.bytes() +
                xb_idx.bytes() + xb_q.bytes() + xb_lambda.bytes() + en_edge.bytes() + en_rest.bytes() + en_k.bytes() +
                en_q.bytes() + en_kb.bytes() + en_bend.bytes() + inst_seg.bytes() + to_caller.bytes() + io_x.bytes() +
                io_v.bytes() + partial.bytes() +
@@ -464,13 +465,13 @@ int check_device() {
 int upload_stencil(ats_cloth* c) {
     int r;
     const Layout& L = c->L;
-    if ((r = upload(c->st_idx, L.st_idx, L.st_idx.size())) || (r = upload(c->st_rest, L.st_rest, L.st_rest.size())) ||
-        (r = upload(c->st_w, L.st_w, L.st_w.size())) || (r = upload(c->slices, L.slices, L.slices.size() / 4)))
+    if ((r = upload(c->st_iw, L.st_iw, L.st_rest.size())) || (r = upload(c->st_rest, L.st_rest, L.st_rest.size())) ||
+        (r = upload(c->slices, L.slices, L.slices.size() / 4)))
         return r;
     return ATS_OK;
 }
 
-template <int TPV, int R>
+template <int TPV, int RE, int RB>
 cudaError_t sweep_launch(dim3 grid, dim3 block, cudaStream_t st, const SweepArgs& a) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = grid;
@@ -482,7 +483,7 @@ cudaError_t sweep_launch(dim3 grid, dim3 block, cudaStream_t st, const SweepArgs
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, vbd_sweep_kernel<TPV, R>, a);
+    return cudaLaunchKernelEx(&cfg, vbd_sweep_kernel<TPV, RE, RB>, a);
 }
 
 int launch_sweep(ats_cloth* c, int color, cudaStream_t st) {
@@ -493,9 +494,8 @@ int launch_sweep(ats_cloth* c, int color, cudaStream_t st) {
     a.x0 = c->x0.p;
     a.vel = c->vel.p;
     a.vm = c->vm.p;
-    a.st_idx = c->st_idx.p;
+    a.st_iw = c->st_iw.p;
     a.st_rest = c->st_rest.p;
-    a.st_w = c->st_w.p;
     a.slices = c->slices.p;
     a.inst = c->inst.p;
     a.slice_begin = sb;
@@ -506,10 +506,10 @@ int launch_sweep(ats_cloth* c, int color, cudaStream_t st) {
     const dim3 grid((se - sb + warps_per_block - 1) / warps_per_block), block(c->block);
     cudaError_t e;
     switch (c->L.tpv) {
-        case 1: e = sweep_launch<1, 12>(grid, block, st, a); break;
-        case 2: e = sweep_launch<2, 6>(grid, block, st, a); break;
-        case 4: e = sweep_launch<4, 3>(grid, block, st, a); break;
-        default: e = sweep_launch<8, 2>(grid, block, st, a); break;
+        case 1: e = sweep_launch<1, 6, 6>(grid, block, st, a); break;
+        case 2: e = sweep_launch<2, 3, 3>(grid, block, st, a); break;
+        case 4: e = sweep_launch<4, 2, 2>(grid, block, st, a); break;
+        default: e = sweep_launch<8, 1, 1>(grid, block, st, a); break;
     }
     if (e != cudaSuccess) {
         set_error(std::string("vbd sweep launch: ") + cudaGetErrorString(e));
@@ -689,7 +689,7 @@ int ats_cloth_query(const ats_cloth* c, ats_cloth_info* info) {
     info->num_bending_colors = c->L.n_bcolors;
     info->threads_per_vertex = c->L.tpv;
     info->block_size = c->block;
-    info->stencil_slots = (int)c->L.st_idx.size();
+    info->stencil_slots = (int)c->L.st_rest.size();
     info->device_bytes = (long long)c->device_bytes();
     return ATS_OK;
 }
@@ -953,9 +953,8 @@ int ats_residual(ats_cloth* c, double* out, ats_stream stream) {
     a.vel = c->vel.p;
     a.vm = c->vm.p;
     a.inst = c->inst.p;
-    a.st_idx = c->st_idx.p;
+    a.st_iw = c->st_iw.p;
     a.st_rest = c->st_rest.p;
-    a.st_w = c->st_w.p;
     a.slices = c->slices.p;
     a.nslices = (int)c->slices.n;
     a.tpv = c->L.tpv;

@@ -11,8 +11,11 @@
 // coalesced. The neighbour stencil of a vertex (1-ring plus the far corners of its
 // bending edges) is stored sliced-ELL: a slice is one warp, 32/TPV vertices with
 // TPV lanes each; row r of a slice is 32 consecutive entries, entry (r, lane) is
-// slot r*TPV + lane%TPV of vertex lane/TPV. Each row is one coalesced 128 B load
-// per array (index, rest length, bending weight).
+// slot r*TPV + lane%TPV of vertex lane/TPV. The first "edge rows" hold the
+// neighbours joined by an edge ({index, bending weight} 8 B + rest length 4 B), the
+// remaining rows the bending-only neighbours ({index, weight} 8 B), so a row is one
+// or two coalesced loads and the spring math is skipped warp-uniformly on
+// bending-only rows.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -27,9 +30,8 @@ struct SweepArgs {
     const float4* __restrict__ x0;
     const float4* __restrict__ vel;
     const float4* __restrict__ vm;
-    const int* __restrict__ st_idx;
+    const int2* __restrict__ st_iw;
     const float* __restrict__ st_rest;
-    const float* __restrict__ st_w;
     const int4* __restrict__ slices;
     const float4* __restrict__ inst;
     int slice_begin, slice_end;
@@ -43,28 +45,28 @@ struct SweepArgs {
 __device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void allow_dependent_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
-// Accumulates one neighbour into the force f and the symmetric Hessian h.
-__device__ __forceinline__ void vbd_neighbour(float4 xv, float4 xu, float L, float w, float ks, float& fx, float& fy,
-                                              float& fz, float& h00, float& h01, float& h02, float& h11, float& h12,
-                                              float& h22) {
+// Adds the spring to neighbour u (d = x_u - x_v, rest length L) and the bending
+// term -w d to the force f and the symmetric Hessian h:
+// f += k C d / l, He = k/l^2 d d^T + k max(1 - L/l, 0) (I - d d^T / l^2),
+// with l = max(|d|, FLT_EPSILON) as VBD::compute_stretch_mass_spring.
+__device__ __forceinline__ void vbd_edge(float4 xv, float4 xu, float L, float w, float ks, float& fx, float& fy,
+                                         float& fz, float& h00, float& h01, float& h02, float& h11, float& h12,
+                                         float& h22) {
     const float dx = xu.x - xv.x, dy = xu.y - xv.y, dz = xu.z - xv.z;
-    // quadratic bending in relative coordinates: -sum_u W_vu (x_u - x_v)
     fx -= w * dx;
     fy -= w * dy;
     fz -= w * dz;
     if (L >= 0.f) {
-        // mass-spring stretch towards neighbour u, d = x_u - x_v:
-        // f = k C d / l, He = k/l^2 d d^T + k max(1 - L/l, 0) (I - d d^T / l^2)
-        const float l = fmaxf(sqrtf(dx * dx + dy * dy + dz * dz), kEps);
-        const float inv = 1.f / l;
-        const float C = l - L;
-        const float kc = ks * C * inv;
+        const float l2 = dx * dx + dy * dy + dz * dz;
+        const float inv = rsqrtf(fmaxf(l2, kEps * kEps));
+        const float l = fmaxf(l2 * inv, kEps);
+        const float kc = ks * (l - L) * inv;
         fx += kc * dx;
         fy += kc * dy;
         fz += kc * dz;
         const float xsq = inv * inv;
         const float b = ks * fmaxf(1.f - L * inv, 0.f);
-        const float c = ks * xsq - b * xsq;
+        const float c = (ks - b) * xsq;
         h00 += c * dx * dx + b;
         h01 += c * dx * dy;
         h02 += c * dx * dz;
@@ -72,6 +74,13 @@ __device__ __forceinline__ void vbd_neighbour(float4 xv, float4 xu, float L, flo
         h12 += c * dy * dz;
         h22 += c * dz * dz + b;
     }
+}
+
+// Bending-only neighbour: quadratic bending in relative coordinates, -w (x_u - x_v).
+__device__ __forceinline__ void vbd_bend(float4 xv, float4 xu, float w, float& fx, float& fy, float& fz) {
+    fx -= w * (xu.x - xv.x);
+    fy -= w * (xu.y - xv.y);
+    fz -= w * (xu.z - xv.z);
 }
 
 // One VBD colour sweep: for every vertex of the colour, inertia + mass-spring
@@ -82,9 +91,10 @@ __device__ __forceinline__ void vbd_neighbour(float4 xv, float4 xu, float L, flo
 // Bending is linear in x, so the per-bending-edge terms -k_b sum_j Q[o][j] x_j are
 // merged per (vertex, neighbour) into one weight W and applied in relative
 // coordinates, the same force because every row of Q sums to zero.
-// R rows are loaded up front (all stencil entries, then all gathers) so that a
-// warp has R independent loads in flight; rows beyond R go through a loop.
-template <int TPV, int R>
+// RE edge rows and RB bending rows are loaded up front (all stencil entries, then
+// all gathers) so that a thread has RE + RB independent loads in flight; rows
+// beyond them go through loops.
+template <int TPV, int RE, int RB>
 __global__ void __launch_bounds__(256) vbd_sweep_kernel(SweepArgs a) {
     const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     const int slice = a.slice_begin + warp;
@@ -94,25 +104,37 @@ __global__ void __launch_bounds__(256) vbd_sweep_kernel(SweepArgs a) {
         allow_dependent_launch();
         return;
     }
-    const int4 sd = __ldg(&a.slices[slice]);  // vbegin, nverts, entry offset, rows
+    const int4 sd = __ldg(&a.slices[slice]);  // vbegin, nverts, entry offset, rows | edge rows << 16
+    const int rows = sd.w & 0xffff, erows = sd.w >> 16, brows = rows - erows;
     const int k = lane / TPV;
     const bool leader = k < sd.y && (lane % TPV) == 0;
     const int v = sd.x + min(k, sd.y - 1);
     const int base = sd.z + lane;
+    const int bbase = base + erows * 32;
 
     // constant data: stencil rows, material, instance parameters
-    int u[R];
-    float L[R], w[R];
+    int ue[RE], ub[RB];
+    float we[RE], le[RE], wb[RB];
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-        if (r < sd.w) {
-            u[r] = __ldg(&a.st_idx[base + r * 32]);
-            L[r] = __ldg(&a.st_rest[base + r * 32]);
-            w[r] = __ldg(&a.st_w[base + r * 32]);
-        } else {
-            u[r] = v;
-            L[r] = -1.f;
-            w[r] = 0.f;
+    for (int r = 0; r < RE; ++r) {
+        ue[r] = v;
+        we[r] = 0.f;
+        le[r] = -1.f;
+        if (r < erows) {
+            const int2 iw = __ldg(&a.st_iw[base + r * 32]);
+            ue[r] = iw.x;
+            we[r] = __int_as_float(iw.y);
+            le[r] = __ldg(&a.st_rest[base + r * 32]);
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < RB; ++r) {
+        ub[r] = v;
+        wb[r] = 0.f;
+        if (r < brows) {
+            const int2 iw = __ldg(&a.st_iw[bbase + r * 32]);
+            ub[r] = iw.x;
+            wb[r] = __int_as_float(iw.y);
         }
     }
     const float4 mv = __ldg(&a.vm[v]);
@@ -122,11 +144,14 @@ __global__ void __launch_bounds__(256) vbd_sweep_kernel(SweepArgs a) {
     grid_dependency_wait();
     allow_dependent_launch();
 
-    // positions and frame-start state (ordered behind the previous kernel)
+    // positions and frame-start state (ordered behind the previous kernel); the
+    // neighbours belong to other colours, which this launch does not write
     const float4 xv = a.x[v];
-    float4 xu[R];
+    float4 xe[RE], xb[RB];
 #pragma unroll
-    for (int r = 0; r < R; ++r) xu[r] = a.x[u[r]];  // other colours: not written by this launch
+    for (int r = 0; r < RE; ++r) xe[r] = a.x[ue[r]];
+#pragma unroll
+    for (int r = 0; r < RB; ++r) xb[r] = a.x[ub[r]];
     float4 p0 = make_float4(0.f, 0.f, 0.f, 0.f), vv = p0;
     if (leader) {
         p0 = a.x0[v];
@@ -136,12 +161,17 @@ __global__ void __launch_bounds__(256) vbd_sweep_kernel(SweepArgs a) {
     float fx = 0.f, fy = 0.f, fz = 0.f;
     float h00 = 0.f, h01 = 0.f, h02 = 0.f, h11 = 0.f, h12 = 0.f, h22 = 0.f;
 #pragma unroll
-    for (int r = 0; r < R; ++r) vbd_neighbour(xv, xu[r], L[r], w[r], ks, fx, fy, fz, h00, h01, h02, h11, h12, h22);
-    for (int r = R; r < sd.w; ++r) {
-        const int e = base + r * 32;
-        const int uu = __ldg(&a.st_idx[e]);
-        vbd_neighbour(xv, a.x[uu], __ldg(&a.st_rest[e]), __ldg(&a.st_w[e]), ks, fx, fy, fz, h00, h01, h02, h11, h12,
-                      h22);
+    for (int r = 0; r < RE; ++r) vbd_edge(xv, xe[r], le[r], we[r], ks, fx, fy, fz, h00, h01, h02, h11, h12, h22);
+    for (int r = RE; r < erows; ++r) {
+        const int2 iw = __ldg(&a.st_iw[base + r * 32]);
+        vbd_edge(xv, a.x[iw.x], __ldg(&a.st_rest[base + r * 32]), __int_as_float(iw.y), ks, fx, fy, fz, h00, h01, h02,
+                 h11, h12, h22);
+    }
+#pragma unroll
+    for (int r = 0; r < RB; ++r) vbd_bend(xv, xb[r], wb[r], fx, fy, fz);
+    for (int r = RB; r < brows; ++r) {
+        const int2 iw = __ldg(&a.st_iw[bbase + r * 32]);
+        vbd_bend(xv, a.x[iw.x], __int_as_float(iw.y), fx, fy, fz);
     }
     // reduce the TPV lanes of a vertex
 #pragma unroll

@@ -1,0 +1,475 @@
+// ats_launcher.cpp -- task DAG, HEFT scheduling and launch for the Launcher API.
+//
+// Scheduling follows the reference scheduler (src/heterogeneous/launcher.cpp):
+//   * topological order: depth-first post-order, reversed (launcher.cpp:25-73, 139-191);
+//   * standardizing_dag: one zero-cost root and terminal (:1587-1714);
+//   * upward rank with the mean computation cost over the processors that implement a
+//     task and a constant mean edge cost of  sum(startup) + (1 + sum(startup))
+//     (:1716-2364, RankMetricMEAN), re-chained along set_constraint_task_orders;
+//   * HEFT earliest-finish-time with insertion into idle slots (:2369-2401, 2521-2563,
+//     2742-2947), communication cost = weight / speed, or the UMA constant delay
+//     when that matrix is given (:2465-2484).
+// Launch runs on Linux: CPU implementations on the calling thread, GPU
+// implementations enqueue on their own CUDA streams; a device-sync hook drains the
+// GPU where a host task depends on GPU work and at the end of a launch.
+
+#include "../../include/ats_launcher.hpp"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <functional>
+#include <stack>
+
+namespace Launcher {
+
+const std::map<FunctionID, std::string> taskNames = {
+    {id_xpbd_non, "id_xpbd_non"},
+    {id_additional_root, "id_additional_root"},
+    {id_additional_terminal, "id_additional_terminal"},
+    {id_task_heft_2002, "id_task_heft_2002"},
+    {id_xpbd_constraint_stretch_mass_spring, "id_xpbd_constraint_stretch_mass_spring"},
+    {id_xpbd_constraint_bending, "id_xpbd_constraint_bending"},
+    {id_xpbd_constraint_last_node, "id_xpbd_constraint_last_node"},
+    {id_xpbd_constraint_self_collision_vv_half_cloth, "id_xpbd_constraint_self_collision_vv_half_cloth"},
+    {id_vbd_evaluate_inertia, "id_vbd_evaluate_inertia"},
+    {id_vbd_evaluate_stretch_mass_spring, "id_vbd_evaluate_stretch_mass_spring"},
+    {id_vbd_evaluate_bending, "id_vbd_evaluate_bending"},
+    {id_vbd_step, "id_vbd_step"},
+    {id_vbd_all_in_one, "id_vbd_all_in_one"},
+    {id_xpbd_predict_position, "id_xpbd_predict_position"},
+    {id_xpbd_reset_constrains, "id_xpbd_reset_constrains"},
+    {id_xpbd_reset_collision_constrains, "id_xpbd_reset_collision_constrains"},
+    {id_xpbd_update_velocity, "id_xpbd_update_velocity"},
+    {id_xpbd_copy_to_cpu_gpu, "id_xpbd_copy_to_cpu_gpu"},
+    {id_xpbd_read_and_solve_conflict, "id_xpbd_read_and_solve_conflict"},
+};
+
+static const char* name_of(FunctionID f) {
+    auto it = taskNames.find(f);
+    return it == taskNames.end() ? "unknown" : it->second.c_str();
+}
+
+bool Task::has_implementation(const DeviceType& t) const {
+    for (const auto& imp : list_implementation)
+        if (imp.device == t) return true;
+    return false;
+}
+
+const Implementation& Task::get_implementation(const DeviceType& t, bool& find) const {
+    static const Implementation none;
+    for (const auto& imp : list_implementation)
+        if (imp.device == t) {
+            find = true;
+            return imp;
+        }
+    find = false;
+    return list_implementation.empty() ? none : list_implementation[0];
+}
+
+uint Scheduler::add_task(const Task& task) {
+    list_task.push_back(task);
+    return (uint)list_task.size() - 1;
+}
+
+uint Scheduler::find_task_by_func_id(const FunctionID id) const {
+    for (uint t = 0; t < list_task.size(); ++t)
+        if (list_task[t].func_id == id) return t;
+    return -1u;
+}
+
+void Scheduler::set_connect(const uint& a, const uint& b, const float& weight) {
+    list_task[a].add_front(b);
+    list_task[a].list_weight.push_back(weight);
+    list_task[b].add_back(a);
+}
+
+float Scheduler::delete_connect(const uint& a, const uint& b) {
+    Task& ta = list_task[a];
+    Task& tb = list_task[b];
+    auto it = std::find(ta.successors.begin(), ta.successors.end(), b);
+    if (it == ta.successors.end()) {
+        std::fprintf(stderr, "delete_connect: %u is not a successor of %u\n", b, a);
+        return 0.f;
+    }
+    const size_t k = it - ta.successors.begin();
+    const float w = ta.list_weight[k];
+    ta.successors.erase(it);
+    ta.list_weight.erase(ta.list_weight.begin() + k);
+    auto jt = std::find(tb.predecessors.begin(), tb.predecessors.end(), a);
+    if (jt != tb.predecessors.end()) tb.predecessors.erase(jt);
+    return w;
+}
+
+bool Scheduler::topological_sort() {
+    const uint n = (uint)list_task.size();
+    std::vector<uint8_t> state(n, 0);  // 0 new, 1 on the current path, 2 finished
+    std::vector<uint> post;
+    post.reserve(n);
+    bool cyclic = false;
+    // iterative DFS: (node, next successor position)
+    for (uint s = 0; s < n && !cyclic; ++s) {
+        if (state[s]) continue;
+        std::stack<std::pair<uint, size_t>> st;
+        st.push({s, 0});
+        state[s] = 1;
+        while (!st.empty() && !cyclic) {
+            auto& top = st.top();
+            const Task& t = list_task[top.first];
+            if (top.second < t.successors.size()) {
+                const uint nx = t.successors[top.second++];
+                if (state[nx] == 0) {
+                    state[nx] = 1;
+                    st.push({nx, 0});
+                } else if (state[nx] == 1) {
+                    cyclic = true;
+                }
+            } else {
+                state[top.first] = 2;
+                post.push_back(top.first);
+                st.pop();
+            }
+        }
+    }
+    if (cyclic) {
+        std::fprintf(stderr, "topological_sort: the task graph contains a cycle\n");
+        list_order.clear();
+        return false;
+    }
+    list_order.assign(post.rbegin(), post.rend());
+    return true;
+}
+
+void Scheduler::profile_from(const std::vector<std::pair<FunctionID, uint>>& map_tasks,
+                             const std::vector<std::vector<double>>& map_costs, std::vector<double>& cost_total) {
+    if (map_costs.empty()) return;
+    const uint nprocs = (uint)map_costs.back().size();
+    std::vector<double> sum(nprocs, 0.0);
+    computation_matrix.assign(list_task.size(), std::vector<float>(nprocs, inf));
+    for (uint t = 0; t < list_task.size(); ++t) {
+        const Task& task = list_task[t];
+        const std::vector<double>* costs = nullptr;
+        for (size_t i = 0; i < map_tasks.size(); ++i)
+            if (map_tasks[i].first == task.func_id && map_tasks[i].second == task.cluster_idx) {
+                costs = &map_costs[i];
+                break;
+            }
+        static const std::vector<double> zeros(16, 0.0);
+        if (!costs) {
+            std::fprintf(stderr, "profile_from: no cost for task %s / %u\n", name_of(task.func_id), task.cluster_idx);
+            costs = &zeros;
+        }
+        for (uint p = 0; p < nprocs; ++p) {
+            const double c = p < costs->size() ? (*costs)[p] : 0.0;
+            if (c < 0) {
+                std::fprintf(stderr, "profile_from: negative cost for %s\n", name_of(task.func_id));
+                return;
+            }
+            computation_matrix[t][p] = task.has_implementation(p) ? (float)c : inf;
+            sum[p] += c;
+        }
+    }
+    if (cost_total.empty()) cost_total = sum;
+    summary_of_costs_each_device = cost_total;
+}
+
+void Scheduler::standardizing_dag(const std::vector<std::function<void(const LaunchParam&)>>& empty_fns) {
+    const uint nprocs = (uint)communication_startup.size();
+    std::vector<Implementation> empty;
+    for (uint p = 0; p < nprocs; ++p)
+        empty.push_back(Implementation(p, p < empty_fns.size() ? empty_fns[p] : [](const LaunchParam&) {}));
+    std::vector<uint> sources;
+    for (uint t = 0; t < list_task.size(); ++t)
+        if (list_task[t].predecessors.empty()) sources.push_back(t);
+    root_node = add_task(Task(id_additional_root, 0, false, true, empty));
+    computation_matrix.push_back(std::vector<float>(nprocs, 0.f));
+    list_order.insert(list_order.begin(), root_node);
+    for (uint t : sources) set_connect(root_node, t, 0.f);
+    std::vector<uint> sinks;
+    for (uint t = 0; t < list_task.size(); ++t)
+        if (list_task[t].successors.empty()) sinks.push_back(t);
+    terminal_node = add_task(Task(id_additional_terminal, 0, false, true, empty));
+    computation_matrix.push_back(std::vector<float>(nprocs, 0.f));
+    list_order.push_back(terminal_node);
+    for (uint t : sinks) set_connect(t, terminal_node, 0.f);
+}
+
+double Scheduler::avg_cost(uint tid, uint nprocs) const {
+    double s = 0.0, n = 0.0;
+    for (uint p = 0; p < nprocs; ++p)
+        if (computation_matrix[tid][p] != inf) {
+            s += computation_matrix[tid][p];
+            n += 1.0;
+        }
+    return n > 0 ? s / n : 0.0;
+}
+
+void Scheduler::compute_ranku(uint nprocs) {
+    const uint n = (uint)list_task.size();
+    double startup = 0.0;
+    for (uint p = 0; p < nprocs && p < communication_startup.size(); ++p) startup += communication_startup[p];
+    const double mean_edge = startup + (1.0 + startup);
+    avg_weight.assign(n, {});
+    for (uint t = 0; t < n; ++t) avg_weight[t].assign(list_task[t].successors.size(), mean_edge);
+    ranku.assign(n, 0.0);
+    auto rank_from_successors = [&](uint node) {
+        double best = -1.0;
+        const Task& t = list_task[node];
+        for (size_t j = 0; j < t.successors.size(); ++j) best = std::max(best, avg_weight[node][j] + ranku[t.successors[j]]);
+        if (best < 0.0) std::fprintf(stderr, "compute_ranku: task %u has no successor rank\n", node);
+        return avg_cost(node, nprocs) + best;
+    };
+    ranku[terminal_node] = avg_cost(terminal_node, nprocs);
+    for (uint i = 1; i < n; ++i) {
+        const uint node = list_order[n - 1 - i];
+        ranku[node] = rank_from_successors(node);
+    }
+    ranku[root_node] = inf;
+    if (!constraint_task_orders.empty()) {
+        // chain the constraint tasks so that their ranks follow the given order
+        std::vector<uint8_t> fixed(n, 0);
+        const size_t k = constraint_task_orders.size();
+        fixed[constraint_task_orders.back()] = 1;
+        for (size_t i = 1; i < k; ++i) {
+            const uint cur = constraint_task_orders[k - 1 - i], nxt = constraint_task_orders[k - i];
+            const double w = avg_weight[cur].empty() ? mean_edge : avg_weight[cur][0];
+            ranku[cur] = avg_cost(cur, nprocs) + w + ranku[nxt];
+            fixed[cur] = 1;
+        }
+        for (uint i = 1; i < n; ++i) {
+            const uint node = list_order[n - 1 - i];
+            if (!fixed[node]) ranku[node] = rank_from_successors(node);
+        }
+        ranku[root_node] = inf;
+    }
+}
+
+float Scheduler::fn_get_communication_cost(uint proc, uint pred, uint node) const {
+    const Task& pt = list_task[pred];
+    auto it = std::find(pt.successors.begin(), pt.successors.end(), node);
+    if (it == pt.successors.end()) return 0.f;
+    const float w = pt.list_weight[it - pt.successors.begin()];
+    if (w == 0.f) return 0.f;
+    const uint pp = task_schedules[pred].proc;
+    if (!communication_cost_matrix_uma.empty()) return communication_cost_matrix_uma[pp][proc];
+    if (pp == proc) return communication_speed_matrix[pp][proc];
+    return w / communication_speed_matrix[pp][proc];
+}
+
+float Scheduler::fn_get_inner_communication_cost(uint proc) const {
+    return !communication_cost_matrix_uma.empty() ? communication_cost_matrix_uma[proc][proc]
+                                                  : communication_speed_matrix[proc][proc];
+}
+
+ScheduleEvent Scheduler::compute_eft(uint node, uint proc) const {
+    float ready = 0.f;
+    for (uint pred : list_task[node].predecessors)
+        ready = std::max(ready, task_schedules[pred].end + fn_get_communication_cost(proc, pred, node));
+    const float ct = computation_matrix[node][proc];
+    const float inner = fn_get_inner_communication_cost(proc);
+    const auto& jobs = proc_schedules[proc];
+    for (size_t i = 0; i < jobs.size(); ++i) {
+        const ScheduleEvent& prev = jobs[i];
+        if (i == 0 && prev.start > ready + ct + inner) return ScheduleEvent(node, proc, ready, ready + ct);
+        const float start = std::max(ready, prev.end + inner);
+        if (i + 1 == jobs.size()) return ScheduleEvent(node, proc, start, start + ct);
+        if (jobs[i + 1].start - start > ct) return ScheduleEvent(node, proc, start, start + ct);
+    }
+    return ScheduleEvent(node, proc, ready, ready + ct);
+}
+
+void Scheduler::scheduler_dag() {
+    const uint nprocs = (uint)communication_startup.size();
+    const uint n = (uint)list_task.size();
+    if (list_order.size() != n || root_node == -1u || terminal_node == -1u || computation_matrix.size() != n) {
+        std::fprintf(stderr, "scheduler_dag: call topological_sort, set the computation matrix and standardizing_dag first\n");
+        return;
+    }
+    compute_ranku(nprocs);
+    sorted_nodes.resize(n);
+    for (uint t = 0; t < n; ++t) sorted_nodes[t] = t;
+    std::stable_sort(sorted_nodes.begin(), sorted_nodes.end(), [&](uint a, uint b) { return ranku[a] > ranku[b]; });
+    if (safety_check) {
+        std::vector<uint> pos(n);
+        for (uint i = 0; i < n; ++i) pos[sorted_nodes[i]] = i;
+        for (uint i = 0; i < n; ++i)
+            for (uint pred : list_task[sorted_nodes[i]].predecessors)
+                if (pos[pred] >= i)
+                    std::fprintf(stderr, "scheduler_dag: task %u is ranked before its predecessor %u\n", sorted_nodes[i],
+                                 pred);
+    }
+    if (sorted_nodes[0] != root_node) {
+        auto it = std::find(sorted_nodes.begin(), sorted_nodes.end(), root_node);
+        std::swap(sorted_nodes[0], *it);
+    }
+    task_schedules.assign(n, ScheduleEvent());
+    proc_schedules.assign(nprocs, {});
+    for (uint node : sorted_nodes) {
+        ScheduleEvent best(node, 0, inf, inf);
+        for (uint p = 0; p < nprocs; ++p) {
+            ScheduleEvent e = compute_eft(node, p);
+            if (print_detail)
+                std::printf("  task %u on proc %u: [%g, %g]\n", node, p, (double)e.start, (double)e.end);
+            if (e.start >= inf) {
+                std::fprintf(stderr, "scheduler_dag: infinite start for task %u\n", node);
+                return;
+            }
+            if (e.end < best.end) best = e;
+        }
+        task_schedules[node] = best;
+        list_task[node].is_allocated_to_main_device = best.proc == 0;
+        auto& jobs = proc_schedules[best.proc];
+        jobs.push_back(best);
+        std::sort(jobs.begin(), jobs.end());
+    }
+}
+
+void Scheduler::make_wait_events() {
+    wait_events.clear();
+    if (proc_schedules.empty()) return;
+    for (uint t = 0; t < list_task.size(); ++t)
+        for (uint pred : list_task[t].predecessors)
+            if (task_schedules[pred].proc != task_schedules[t].proc)
+                wait_events.push_back(WaitEvent{t, task_schedules[t].proc, pred});
+}
+
+float Scheduler::get_scheduled_end_time() const {
+    float end = 0.f;
+    for (const auto& jobs : proc_schedules)
+        if (!jobs.empty()) end = std::max(end, jobs.back().end);
+    return end;
+}
+
+std::vector<float> Scheduler::get_scheduled_speedups() const {
+    const float end = get_scheduled_end_time();
+    std::vector<float> s(proc_schedules.size(), 0.f);
+    for (size_t p = 0; p < s.size() && p < summary_of_costs_each_device.size(); ++p)
+        s[p] = (float)((summary_of_costs_each_device[p] - end) / end);
+    return s;
+}
+
+void Scheduler::print_proc_schedules() const {
+    for (size_t p = 0; p < proc_schedules.size(); ++p) {
+        std::printf("Processor %zu:\n", p);
+        for (const auto& e : proc_schedules[p])
+            std::printf("  task %u [%s, cluster %u] from %g to %g\n", e.task_id, name_of(list_task[e.task_id].func_id),
+                        list_task[e.task_id].cluster_idx, (double)e.start, (double)e.end);
+    }
+}
+
+void Scheduler::print_speedups_to_each_device() const {
+    const float end = get_scheduled_end_time();
+    const auto s = get_scheduled_speedups();
+    for (size_t p = 0; p < s.size(); ++p)
+        std::printf("Speedup to proc %zu = %4.2f%% (From %4.2f to %4.2f )\n", p, (double)s[p] * 100.0,
+                    p < summary_of_costs_each_device.size() ? summary_of_costs_each_device[p] : 0.0, (double)end);
+}
+
+void Scheduler::print_sort_by_typology() const {
+    for (uint t : list_order)
+        std::printf("  task %u in iteration %d cluster %u => %s\n", t, (int)list_task[t].iter_idx, list_task[t].cluster_idx,
+                    name_of(list_task[t].func_id));
+}
+
+void Scheduler::set_device_sync(DeviceType d, std::function<void()> fn) { device_sync[d] = std::move(fn); }
+
+void Scheduler::drain(DeviceType d) const {
+    auto it = device_sync.find(d);
+    if (it != device_sync.end()) {
+        it->second();
+    } else if (d != DeviceTypeCpu) {
+        cudaError_t e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) std::fprintf(stderr, "launch: device sync failed: %s\n", cudaGetErrorString(e));
+    }
+}
+
+void Scheduler::launch(LaunchMode mode, const std::function<LaunchParam(const Task&)>& task_to_param, bool fully_not_wait,
+                       const std::vector<std::function<void()>>& /*assemble_impl*/) {
+    const std::vector<uint>& order = !sorted_nodes.empty() ? sorted_nodes : list_order;
+    if (order.empty()) {
+        std::fprintf(stderr, "launch: neither a topological nor a ranked order; call topological_sort first\n");
+        return;
+    }
+    auto run = [&](uint tid, DeviceType d, bool& found) {
+        const Task& t = list_task[tid];
+        const Implementation& imp = t.get_implementation(d, found);
+        if (!found && d != DeviceTypeCpu) drain(d);
+        imp.launch_task(task_to_param(t));
+    };
+    if (mode == LaunchModeCpu) {
+        for (uint tid : order) {
+            bool found;
+            if (!list_task[tid].has_implementation(DeviceTypeCpu)) {
+                std::fprintf(stderr, "launch: task %u has no CPU implementation\n", tid);
+                return;
+            }
+            run(tid, DeviceTypeCpu, found);
+        }
+        return;
+    }
+    if (mode == LaunchModeGpu) {
+        for (uint tid : order) {
+            bool found;
+            run(tid, DeviceTypeGpu, found);
+        }
+        if (!fully_not_wait) drain(DeviceTypeGpu);
+        return;
+    }
+    if (proc_schedules.empty()) {
+        std::fprintf(stderr, "launch: this mode needs scheduler_dag() first\n");
+        return;
+    }
+    // scheduled modes: tasks in order of scheduled start
+    std::vector<ScheduleEvent> plan;
+    for (const auto& jobs : proc_schedules) plan.insert(plan.end(), jobs.begin(), jobs.end());
+    std::stable_sort(plan.begin(), plan.end(), [](const ScheduleEvent& a, const ScheduleEvent& b) {
+        return a.start != b.start ? a.start < b.start : a.proc < b.proc;
+    });
+    if (mode == LaunchModePartialCPU || mode == LaunchModePartialGPU) {
+        const uint want = mode == LaunchModePartialCPU ? 0u : 1u;
+        for (const auto& e : plan)
+            if (e.proc == want) {
+                bool found;
+                run(e.task_id, want, found);
+            }
+        if (!fully_not_wait && want != DeviceTypeCpu) drain(want);
+        return;
+    }
+    if (mode == LaunchModeSequeceHetero) {
+        for (const auto& e : plan) {
+            bool found;
+            run(e.task_id, DeviceTypeCpu, found);
+        }
+        return;
+    }
+    // Hetero / ProgressiveHetero / FakeHetero: each task on its scheduled device. A
+    // host task that depends on device work not yet drained waits for it first;
+    // device work that depends on host tasks is enqueued after them (start order).
+    const bool synchronous = mode == LaunchModeFakeHetero;
+    std::vector<uint8_t> pending(list_task.size(), 0);  // device task enqueued, not yet drained
+    for (const auto& e : plan) {
+        const Task& t = list_task[e.task_id];
+        if (e.proc == DeviceTypeCpu) {
+            bool wait = false;
+            for (uint pred : t.predecessors) wait |= pending[pred] != 0;
+            if (wait) {
+                drain(DeviceTypeGpu);
+                std::fill(pending.begin(), pending.end(), 0);
+            }
+            bool found;
+            run(e.task_id, DeviceTypeCpu, found);
+        } else {
+            bool found;
+            run(e.task_id, e.proc, found);
+            pending[e.task_id] = 1;
+            if (synchronous) {
+                drain(e.proc);
+                pending[e.task_id] = 0;
+            }
+        }
+    }
+    if (!fully_not_wait) drain(DeviceTypeGpu);
+}
+
+}  // namespace Launcher

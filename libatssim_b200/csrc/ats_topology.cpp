@@ -195,44 +195,64 @@ bool build_slices(Layout& L, int tpv, std::string& err) {
     }
     L.tpv = tpv;
     const int vps = 32 / tpv;  // vertices per slice (one warp)
-    L.st_idx.clear();
+    L.st_iw.clear();
     L.st_rest.clear();
-    L.st_w.clear();
     L.slices.clear();
     L.color_slices.assign(1, 0);
-    // entry (row, thread th) of a slice = vertex th / tpv, slot row * tpv + th % tpv
+    // Per vertex: edge neighbours first (rest >= 0), then bending-only neighbours.
+    // The neighbour lists are sorted by layout id inside each group.
+    auto n_edges = [&](int v) {
+        int c = 0;
+        for (int q = L.nb_off[v]; q < L.nb_off[v + 1]; ++q) c += L.nb_rest[q] >= 0.f;
+        return c;
+    };
+    std::vector<int> order;
     for (int c = 0; c < L.n_vcolors; ++c) {
         for (int ri = L.run_off[c]; ri < L.run_off[c + 1]; ++ri) {
             const int b = L.runs[2 * ri], e = L.runs[2 * ri + 1];
             for (int s = b; s < e; s += vps) {
                 const int n = std::min(vps, e - s);
-                int width = 0;
-                for (int k = 0; k < n; ++k) width = std::max(width, L.nb_off[s + k + 1] - L.nb_off[s + k]);
-                const int rows = (width + tpv - 1) / tpv;
-                const size_t off = L.st_idx.size();
-                L.st_idx.resize(off + 32 * (size_t)rows);
+                int max_e = 0, max_b = 0;
+                for (int k = 0; k < n; ++k) {
+                    const int ne = n_edges(s + k);
+                    max_e = std::max(max_e, ne);
+                    max_b = std::max(max_b, L.nb_off[s + k + 1] - L.nb_off[s + k] - ne);
+                }
+                const int erows = (max_e + tpv - 1) / tpv, brows = (max_b + tpv - 1) / tpv;
+                const int rows = erows + brows;
+                const size_t off = L.st_rest.size();
+                L.st_iw.resize(2 * (off + 32 * (size_t)rows));
                 L.st_rest.resize(off + 32 * (size_t)rows);
-                L.st_w.resize(off + 32 * (size_t)rows);
-                for (int row = 0; row < rows; ++row)
-                    for (int th = 0; th < 32; ++th) {
-                        const int k = th / tpv, slot = row * tpv + th % tpv;
+                for (int th = 0; th < 32; ++th) {
+                    const int k = th / tpv;
+                    const int self = s + std::min(k, n - 1);
+                    // this vertex's neighbours split into edge / bending-only slots
+                    std::vector<int> eq, bq;
+                    if (k < n)
+                        for (int q = L.nb_off[s + k]; q < L.nb_off[s + k + 1]; ++q)
+                            (L.nb_rest[q] >= 0.f ? eq : bq).push_back(q);
+                    for (int row = 0; row < rows; ++row) {
+                        const bool edge_row = row < erows;
+                        const int slot = (edge_row ? row : row - erows) * tpv + th % tpv;
+                        const std::vector<int>& src = edge_row ? eq : bq;
                         const size_t at = off + 32 * (size_t)row + th;
-                        const int self = s + std::min(k, n - 1);
-                        if (k < n && slot < L.nb_off[s + k + 1] - L.nb_off[s + k]) {
-                            const int q = L.nb_off[s + k] + slot;
-                            L.st_idx[at] = L.nb_u[q];
-                            L.st_rest[at] = L.nb_rest[q];
-                            L.st_w[at] = L.nb_w[q];
-                        } else {
-                            L.st_idx[at] = self;
-                            L.st_rest[at] = -1.f;
-                            L.st_w[at] = 0.f;
+                        int idx = self;
+                        float w = 0.f, rest = -1.f;
+                        if (slot < (int)src.size()) {
+                            const int q = src[slot];
+                            idx = L.nb_u[q];
+                            w = L.nb_w[q];
+                            rest = L.nb_rest[q];
                         }
+                        L.st_iw[2 * at] = idx;
+                        std::memcpy(&L.st_iw[2 * at + 1], &w, 4);
+                        L.st_rest[at] = rest;
                     }
+                }
                 L.slices.push_back(s);
                 L.slices.push_back(n);
                 L.slices.push_back((int)off);
-                L.slices.push_back(rows);
+                L.slices.push_back(rows | (erows << 16));
             }
         }
         L.color_slices.push_back((int)L.slices.size() / 4);

@@ -62,11 +62,12 @@ struct Layout {
     std::vector<float> nb_rest, nb_w;
     std::vector<int> runs;          // per colour c: runs[c] .. runs of (begin, end) layout ranges
     std::vector<int> run_off;       // n_vcolors + 1 offsets into runs (pairs)
-    // sliced-ELL stencil for the current tpv: slice = 32/tpv vertices, row r holds 32 entries
-    std::vector<int> st_idx;        // neighbour layout id (self for padding)
-    std::vector<float> st_rest;     // rest length, -1 = not an edge (bending-only neighbour or padding)
-    std::vector<float> st_w;        // bending weight
-    std::vector<int> slices;        // 4 ints per slice: vbegin, nverts, entry offset, rows
+    // sliced-ELL stencil for the current tpv: slice = 32/tpv vertices, row r holds 32
+    // entries; the first edge rows hold edge neighbours, the remaining rows the
+    // bending-only neighbours (far corners of bending edges)
+    std::vector<int> st_iw;         // 2 per entry: neighbour layout id (self for padding), bending weight bits
+    std::vector<float> st_rest;     // per entry: rest length (edge rows only), -1 = padding
+    std::vector<int> slices;        // 4 ints per slice: vbegin, nverts, entry offset, rows | edge rows << 16
     std::vector<int> color_slices;  // n_vcolors + 1 offsets into slices
     // XPBD, colour-major over all instances
     std::vector<int> xs_edge;       // 2 per constraint (layout ids)

@@ -1,0 +1,63 @@
+"""The Launcher API (include/ats_launcher.hpp) through C++ driver programs.
+
+HEFT known answer of examples/example1_heft2002.cpp / README.md:25-31 (makespan 91,
+speedups 39.56 / 42.86 / 57.14 %), and the VBD task graph of
+examples/example2_async_iter.cpp:1305-1384 launched through the scheduler with a CUDA
+implementation, which must give exactly the positions of ats_frame.
+"""
+import json
+import os
+import subprocess
+
+import pytest
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+@pytest.fixture(scope="module")
+def programs(ats):
+    from libatssim_b200 import build
+    return build.build_tests()
+
+
+def heft_input(d):
+    lines = [f"3 {len(d['computation'])} {len(d['edges'])}"]
+    lines += [" ".join(str(c) for c in row) for row in d["computation"]]
+    lines += [f"{a} {b} {w}" for a, b, w in d["edges"]]
+    return "\n".join(lines) + "\n"
+
+
+def test_heft_2002_known_answer(programs):
+    d = json.load(open(os.path.join(GOLD, "heft2002.json")))
+    r = subprocess.run([programs["heft_case"]], input=heft_input(d), capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0, r.stderr
+    out = json.loads(r.stdout)
+    assert out["makespan"] == d["makespan"] == 91.0
+    assert out["speedups_percent"] == d["speedups_percent"]
+    # 10 tasks + added root and terminal, all launched in schedule order
+    assert out["launched"] == 12
+    # every task starts after its predecessors finish
+    sched = {t: (p, s, e) for t, p, s, e in out["schedule"]}
+    for a, b, _ in d["edges"]:
+        assert sched[b][1] >= sched[a][2] - 1e-6
+
+
+def test_heft_rejects_cycles(programs):
+    d = json.load(open(os.path.join(GOLD, "heft2002.json")))
+    d = dict(d, edges=d["edges"] + [[10, 1, 1.0]])
+    r = subprocess.run([programs["heft_case"]], input=heft_input(d), capture_output=True, text=True, timeout=60)
+    assert r.returncode == 3
+    assert "cycle" in r.stderr
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["gpu", "hetero", "fake"])
+def test_vbd_task_graph_through_scheduler(programs, mode):
+    r = subprocess.run([programs["vbd_dag"], "32", "8", "4", mode], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    out = json.loads(r.stdout)
+    assert out["max_abs_diff"] == 0.0
+    assert out["max_displacement"] > 1e-3
+    # predict + 8 x 4 colours + last node + update + root + terminal, all on the B200
+    assert out["tasks"] == 1 + 8 * 4 + 2 + 2
+    assert out["tasks_on_gpu"] >= 8 * 4
