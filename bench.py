@@ -39,6 +39,7 @@ sys.path.insert(0, ROOT)
 METRIC = "frames/s to 1e-4 residual: batched+learned VBD vs plain CUDA VBD, 1 B200"
 UNIT = "frames/s"
 WORKLOAD = "c1: 512x512 grid cloth, plain VBD, 50 iterations x 4 colours per frame"
+WORKLOAD_C2 = "c2: 256 batched grid cloths, side U{16..256}, plain VBD, 50 iterations per frame"
 ITERS = 50
 REF_SAMPLE_ITERS = 10
 
@@ -52,6 +53,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--tpv", type=int, default=0)
     p.add_argument("--block", type=int, default=0)
+    p.add_argument("--workload", default="c1", choices=["c1", "c2"],
+                   help="c1: 512x512 cloth (the headline); c2: 256 batched instances")
     return p.parse_args()
 
 
@@ -180,8 +183,10 @@ def run_ours(args):
     import libatssim_b200 as ats
     from libatssim_b200 import build, configs
     build.build()
-    insts, prm = configs.c1()
+    insts, prm = configs.c1() if args.workload == "c1" else configs.c2()
+    t_create = time.perf_counter()
     cloth = ats.Cloth(insts, threads_per_vertex=args.tpv, block_size=args.block, **prm)
+    t_create = time.perf_counter() - t_create
     stream = torch.cuda.current_stream()
     tuned = None
     if not args.tpv and not args.block:
@@ -279,7 +284,8 @@ def run_ours(args):
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-               "config": {"workload": WORKLOAD, "vertices": info.num_verts, "edges": info.num_edges,
+               "config": {"workload": WORKLOAD if args.workload == "c1" else WORKLOAD_C2,
+                          "instances": info.num_instances, "create_s": t_create, "vertices": info.num_verts, "edges": info.num_edges,
                           "bending_edges": info.num_bending_edges, "colors": info.num_vertex_colors,
                           "iterations": ITERS, "threads_per_vertex": info.threads_per_vertex,
                           "block_size": info.block_size, "autotuned": tuned is not None,
@@ -295,7 +301,7 @@ def run_ours(args):
                             "alg_bytes_per_launch": bytes_launch, "peak_source": peak_src},
                "gpu_launches": args.steps * (2 + ITERS * info.num_vertex_colors),
                "clocks": clk}
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and not args.no_cpu_baseline and args.workload == "c1":
         threads = os.cpu_count() or 1
         s = cpu_port_sample(threads, REF_SAMPLE_ITERS)
         s.frame()

@@ -139,6 +139,10 @@ int ats_cloth_create(const ats_instance_desc* instances, int num_instances, cons
 int ats_cloth_destroy(ats_cloth* cloth);
 int ats_cloth_query(const ats_cloth* cloth, ats_cloth_info* info);
 
+/* Device order of the vertices: layout_of_caller[i] = position of caller vertex i in
+ * the instance-major, colour-major device layout (recorded samples follow it). */
+int ats_cloth_vertex_order(const ats_cloth* cloth, int* layout_of_caller);
+
 /* Frame-end state (x, v), 3 floats per vertex, original order, instances concatenated.
  * Replaces SolverInterface::restart_system / load_saved_state and the frame_end read
  * (example2_async_iter.cpp:1575-1614). Both calls synchronise `stream`. v may be null. */
@@ -176,6 +180,19 @@ int ats_frame(ats_cloth* cloth, int solver, ats_stream stream);
 /* The same frame replayed from a CUDA graph captured on first use (per solver). */
 int ats_frame_graph(ats_cloth* cloth, int solver, ats_stream stream);
 
+/* One VBD frame iterated to a residual: predict, then VBD iterations in chunks of
+ * `check_every`, after each chunk the FP64 residual of every instance; an instance
+ * stops (its sweeps are skipped) once ||grad G(x)|| <= tol ||grad G(y)|| or after
+ * max_iterations; then the velocity update. iterations / residual (host, one per
+ * instance, nullable) receive the iterations used and the final relative residual.
+ * The residual is the SURVEY definition: incremental-potential gradient over free
+ * vertices, y the inertial prediction. Synchronises `stream` after every chunk. */
+int ats_frame_to_residual(ats_cloth* cloth, double tol, int check_every, int max_iterations, int* iterations,
+                          double* residual, ats_stream stream);
+/* The same with one tolerance per instance (host array). */
+int ats_frame_to_residuals(ats_cloth* cloth, const double* tols, int check_every, int max_iterations, int* iterations,
+                           double* residual, ats_stream stream);
+
 /* Times `iterations` VBD iterations for every lanes-per-vertex (1, 2, 4, 8) and
  * block size (64, 128, 256) on this handle's own mesh, keeps the fastest and
  * reports it. The iterate x is restored afterwards; captured frame graphs are
@@ -211,6 +228,67 @@ int ats_energy_noalloc(const float* x, const float* x_start, const float* v, con
                        const unsigned char* fixed, int num_verts, const int* edges, const float* rest_length,
                        int num_edges, const int* bending, const float* q, int num_bending_edges, float k_stretch,
                        float k_bend, const float* accel, float h, double* out3, ats_stream stream);
+
+/* ---------------------------------------------------------------- learned warm start
+ * No counterpart in the reference: a per-vertex MLP (24 -> 64 -> 64 -> 64 -> 3, exact
+ * GELU, BF16 weights and activations, FP32 accumulation on the tensor cores) predicts
+ * the frame's solved position; the plain VBD iterations always run afterwards.
+ * Features of vertex v (h the substep, s = 9.8 h^2, y the inertial prediction):
+ * h v / s, (y - x0) / s, and (x0_u - x0_v) / rest length of the edge neighbours in six
+ * rest directions (+x, +x+z, +z, -x, -x-z, -z; zero where there is none). Output:
+ * (x - y) / s; the guess is y + s * output, pinned vertices keep y. */
+typedef struct ats_mlp ats_mlp;
+typedef struct ats_dataset ats_dataset;
+
+/* Parameter count (10115): FP32 master layout W1[24][64] b1[64] W2[64][64] b2 W3 b3
+ * W4[64][3] b4[3], W[in][out] row-major. */
+int ats_mlp_param_count(void);
+int ats_mlp_create(unsigned long long seed, ats_mlp** out);
+int ats_mlp_destroy(ats_mlp* mlp);
+int ats_mlp_get_params(const ats_mlp* mlp, float* params);
+/* Replaces the parameters and resets the optimiser state. */
+int ats_mlp_set_params(ats_mlp* mlp, const float* params);
+/* Input / output normalisation (54 floats): in_mean[24], in_scale[24] (1/std),
+ * out_mean[3], out_std[3]; the network sees (f - in_mean) * in_scale and its raw
+ * output o gives out_mean + out_std * o. A new model has the identity. */
+int ats_mlp_get_normalization(const ats_mlp* mlp, float* norm);
+int ats_mlp_set_normalization(ats_mlp* mlp, const float* norm);
+/* Sets the normalisation from the FP64 column means / standard deviations of `data`. */
+int ats_mlp_fit_normalization(ats_mlp* mlp, const ats_dataset* data, ats_stream stream);
+/* Network outputs of n feature rows (24 floats each) into outputs (3 floats each),
+ * normalisation applied. */
+int ats_mlp_infer(const ats_mlp* mlp, const float* features, int n, float* outputs, ats_stream stream);
+/* Gradient (FP32, ats_mlp_param_count floats) of the mean squared error over n
+ * samples in normalised target space, and the loss; the parameters are not changed. */
+int ats_mlp_gradient(ats_mlp* mlp, const float* features, const float* targets, int n, float* grad, float* loss,
+                     ats_stream stream);
+
+/* Training samples (features, targets) kept on the device. */
+int ats_dataset_create(long long capacity, ats_dataset** out);
+int ats_dataset_destroy(ats_dataset* data);
+int ats_dataset_size(const ats_dataset* data, long long* n);
+int ats_dataset_read(const ats_dataset* data, long long first, long long count, float* features, float* targets);
+/* Records one frame of `cloth` as samples: call ats_record_frame_begin right after
+ * ats_predict_position (features and y), run the iterations, then
+ * ats_record_frame_end before ats_update_velocity (target (x - y)/s of every free vertex). */
+int ats_record_frame_begin(ats_cloth* cloth, ats_stream stream);
+int ats_record_frame_end(ats_cloth* cloth, ats_dataset* data, ats_stream stream);
+/* `steps` Adam steps on batches of `batch` samples drawn from `data` (seeded);
+ * mean_loss (nullable) = mean loss of the last 20 steps. Synchronises `stream`. */
+int ats_mlp_train(ats_mlp* mlp, const ats_dataset* data, int steps, int batch, float lr, unsigned long long seed,
+                  float* mean_loss, ats_stream stream);
+/* After ats_predict_position: x = learned guess. With fallback != 0 an instance keeps
+ * y when its FP64 incremental potential G(guess) > G(y); used (host, one per instance,
+ * nullable) receives 1 where the guess was kept (synchronises `stream` then). */
+int ats_warm_start(ats_cloth* cloth, const ats_mlp* mlp, int fallback, int* used, ats_stream stream);
+/* ats_frame with the learned guess between predict and the iterations. */
+int ats_frame_warm(ats_cloth* cloth, const ats_mlp* mlp, int fallback, ats_stream stream);
+/* ats_frame_to_residual with the learned guess; the residual stays relative to
+ * ||grad G(y)|| of the inertial prediction. tols (host, one per instance) overrides
+ * tol when not null. */
+int ats_frame_warm_to_residual(ats_cloth* cloth, const ats_mlp* mlp, int fallback, double tol, const double* tols,
+                               int check_every, int max_iterations, int* iterations, double* residual, int* used,
+                               ats_stream stream);
 
 /* Message of the last failed call on this thread ("" if none). */
 const char* ats_last_error(void);

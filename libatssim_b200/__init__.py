@@ -91,6 +91,7 @@ _SIGNATURES = {
     "ats_cloth_create": [ctypes.POINTER(InstanceDesc), ctypes.c_int, ctypes.POINTER(SolverParams), ctypes.POINTER(_vp)],
     "ats_cloth_destroy": [_vp],
     "ats_cloth_query": [_vp, ctypes.POINTER(ClothInfo)],
+    "ats_cloth_vertex_order": [_vp, _ip],
     "ats_set_state": [_vp, _fp, _fp, _vp],
     "ats_get_state": [_vp, _fp, _fp, _vp],
     "ats_get_positions": [_vp, _fp, _vp],
@@ -106,7 +107,29 @@ _SIGNATURES = {
     "ats_frame_graph": [_vp, ctypes.c_int, _vp],
     "ats_autotune": [_vp, ctypes.c_int, _vp, _ip, _ip],
     "ats_energy": [_vp, _dp, _vp],
+    "ats_frame_to_residual": [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, _ip, _dp, _vp],
     "ats_residual": [_vp, _dp, _vp],
+    "ats_mlp_create": [ctypes.c_ulonglong, ctypes.POINTER(_vp)],
+    "ats_mlp_destroy": [_vp],
+    "ats_mlp_get_params": [_vp, _fp],
+    "ats_mlp_set_params": [_vp, _fp],
+    "ats_mlp_infer": [_vp, _fp, ctypes.c_int, _fp, _vp],
+    "ats_mlp_get_normalization": [_vp, _fp],
+    "ats_mlp_set_normalization": [_vp, _fp],
+    "ats_mlp_fit_normalization": [_vp, _vp, _vp],
+    "ats_mlp_gradient": [_vp, _fp, _fp, ctypes.c_int, _fp, _fp, _vp],
+    "ats_dataset_create": [ctypes.c_longlong, ctypes.POINTER(_vp)],
+    "ats_dataset_destroy": [_vp],
+    "ats_dataset_size": [_vp, ctypes.POINTER(ctypes.c_longlong)],
+    "ats_dataset_read": [_vp, ctypes.c_longlong, ctypes.c_longlong, _fp, _fp],
+    "ats_record_frame_begin": [_vp, _vp],
+    "ats_record_frame_end": [_vp, _vp, _vp],
+    "ats_mlp_train": [_vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_ulonglong, _fp, _vp],
+    "ats_warm_start": [_vp, _vp, ctypes.c_int, _ip, _vp],
+    "ats_frame_warm": [_vp, _vp, ctypes.c_int, _vp],
+    "ats_frame_warm_to_residual": [_vp, _vp, ctypes.c_int, ctypes.c_double, _dp, ctypes.c_int, ctypes.c_int, _ip, _dp,
+                                   _ip, _vp],
+    "ats_frame_to_residuals": [_vp, _dp, ctypes.c_int, ctypes.c_int, _ip, _dp, _vp],
     "ats_energy_noalloc": [_vp, _vp, _vp, _vp, _vp, ctypes.c_int, _vp, _vp, ctypes.c_int, _vp, _vp, ctypes.c_int,
                            ctypes.c_float, ctypes.c_float, _fp, ctypes.c_float, _vp, _vp],
 }
@@ -125,6 +148,8 @@ def lib():
             fn.restype = ctypes.c_int
         L.ats_last_error.restype = ctypes.c_char_p
         L.ats_last_error.argtypes = []
+        L.ats_mlp_param_count.restype = ctypes.c_int
+        L.ats_mlp_param_count.argtypes = []
         _lib = L
     return _lib
 
@@ -288,6 +313,12 @@ class Cloth:
         except Exception:
             pass
 
+    def vertex_order(self):
+        """layout_of_caller: device position of every caller vertex."""
+        out = np.zeros(self.nv, dtype=np.int32)
+        _check(lib().ats_cloth_vertex_order(self.h, _p(out, ctypes.c_int)))
+        return out
+
     # state -------------------------------------------------------------
     def set_state(self, x, v=None, stream=None):
         x = np.ascontiguousarray(x, dtype=np.float32)
@@ -345,6 +376,50 @@ class Cloth:
         fn = lib().ats_frame_graph if graph else lib().ats_frame
         _check(fn(self.h, solver, _stream(stream)))
 
+    def frame_warm(self, mlp, fallback=True, stream=None):
+        _check(lib().ats_frame_warm(self.h, mlp.h, int(fallback), _stream(stream)))
+
+    def warm_start(self, mlp, fallback=True, stream=None):
+        used = np.zeros(self.info.num_instances, dtype=np.int32)
+        _check(lib().ats_warm_start(self.h, mlp.h, int(fallback), _p(used, ctypes.c_int), _stream(stream)))
+        return used
+
+    def frame_warm_to_residual(self, mlp, tol, fallback=True, check_every=10, max_iterations=1000, stream=None):
+        """frame_to_residual with the learned guess; tol is a float or one value per
+        instance; returns (iterations, residual, used)."""
+        n = self.info.num_instances
+        it = np.zeros(n, dtype=np.int32)
+        res = np.zeros(n, dtype=np.float64)
+        used = np.zeros(n, dtype=np.int32)
+        tols = None if np.isscalar(tol) else np.ascontiguousarray(tol, dtype=np.float64)
+        _check(lib().ats_frame_warm_to_residual(self.h, mlp.h, int(fallback), float(tol) if tols is None else 0.0,
+                                                None if tols is None else _p(tols, ctypes.c_double), int(check_every),
+                                                int(max_iterations), _p(it, ctypes.c_int), _p(res, ctypes.c_double),
+                                                _p(used, ctypes.c_int), _stream(stream)))
+        return it, res, used
+
+    def record_begin(self, stream=None):
+        _check(lib().ats_record_frame_begin(self.h, _stream(stream)))
+
+    def record_end(self, dataset, stream=None):
+        _check(lib().ats_record_frame_end(self.h, dataset.h, _stream(stream)))
+
+    def frame_to_residual(self, tol, check_every=10, max_iterations=1000, stream=None):
+        """One frame iterated until every instance reaches ||grad G|| <= tol ||grad G(y)||
+        (or max_iterations); tol is a float or one value per instance; returns
+        (iterations per instance, relative residual per instance)."""
+        n = self.info.num_instances
+        it = np.zeros(n, dtype=np.int32)
+        res = np.zeros(n, dtype=np.float64)
+        if np.isscalar(tol):
+            _check(lib().ats_frame_to_residual(self.h, float(tol), int(check_every), int(max_iterations),
+                                               _p(it, ctypes.c_int), _p(res, ctypes.c_double), _stream(stream)))
+        else:
+            t = np.ascontiguousarray(tol, dtype=np.float64)
+            _check(lib().ats_frame_to_residuals(self.h, _p(t, ctypes.c_double), int(check_every), int(max_iterations),
+                                                _p(it, ctypes.c_int), _p(res, ctypes.c_double), _stream(stream)))
+        return it, res
+
     def energy(self, stream=None):
         out = np.zeros(3, dtype=np.float64)
         _check(lib().ats_energy(self.h, _p(out, ctypes.c_double), _stream(stream)))
@@ -354,3 +429,98 @@ class Cloth:
         out = np.zeros(self.info.num_instances, dtype=np.float64)
         _check(lib().ats_residual(self.h, _p(out, ctypes.c_double), _stream(stream)))
         return out
+
+
+class MLP:
+    """The warm-start network (ats_mlp_*): 24 -> 64 -> 64 -> 64 -> 3, BF16 weights."""
+
+    def __init__(self, seed=0):
+        h = _vp()
+        _check(lib().ats_mlp_create(int(seed), ctypes.byref(h)))
+        self.h = h
+        self.nparams = lib().ats_mlp_param_count()
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().ats_mlp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def params(self):
+        out = np.zeros(self.nparams, dtype=np.float32)
+        _check(lib().ats_mlp_get_params(self.h, _p(out, ctypes.c_float)))
+        return out
+
+    def set_params(self, theta):
+        t = np.ascontiguousarray(theta, dtype=np.float32)
+        _check(lib().ats_mlp_set_params(self.h, _p(t, ctypes.c_float)))
+
+    def normalization(self):
+        out = np.zeros(54, dtype=np.float32)
+        _check(lib().ats_mlp_get_normalization(self.h, _p(out, ctypes.c_float)))
+        return out
+
+    def set_normalization(self, norm):
+        n = np.ascontiguousarray(norm, dtype=np.float32)
+        _check(lib().ats_mlp_set_normalization(self.h, _p(n, ctypes.c_float)))
+
+    def fit_normalization(self, dataset, stream=None):
+        _check(lib().ats_mlp_fit_normalization(self.h, dataset.h, _stream(stream)))
+
+    def infer(self, features, stream=None):
+        f = np.ascontiguousarray(features, dtype=np.float32)
+        out = np.zeros((f.shape[0], 3), dtype=np.float32)
+        _check(lib().ats_mlp_infer(self.h, _p(f, ctypes.c_float), f.shape[0], _p(out, ctypes.c_float), _stream(stream)))
+        return out
+
+    def gradient(self, features, targets, stream=None):
+        f = np.ascontiguousarray(features, dtype=np.float32)
+        t = np.ascontiguousarray(targets, dtype=np.float32)
+        g = np.zeros(self.nparams, dtype=np.float32)
+        loss = ctypes.c_float(0.0)
+        _check(lib().ats_mlp_gradient(self.h, _p(f, ctypes.c_float), _p(t, ctypes.c_float), f.shape[0],
+                                      _p(g, ctypes.c_float), ctypes.byref(loss), _stream(stream)))
+        return float(loss.value), g
+
+    def train(self, dataset, steps, batch=4096, lr=1e-3, seed=0, stream=None):
+        loss = ctypes.c_float(0.0)
+        _check(lib().ats_mlp_train(self.h, dataset.h, int(steps), int(batch), float(lr), int(seed), ctypes.byref(loss),
+                                   _stream(stream)))
+        return float(loss.value)
+
+
+class Dataset:
+    """Recorded (features, target) samples on the device (ats_dataset_*)."""
+
+    def __init__(self, capacity):
+        h = _vp()
+        _check(lib().ats_dataset_create(int(capacity), ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().ats_dataset_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __len__(self):
+        n = ctypes.c_longlong(0)
+        _check(lib().ats_dataset_size(self.h, ctypes.byref(n)))
+        return int(n.value)
+
+    def read(self, first=0, count=None):
+        count = len(self) - first if count is None else count
+        f = np.zeros((count, 24), dtype=np.float32)
+        t = np.zeros((count, 3), dtype=np.float32)
+        _check(lib().ats_dataset_read(self.h, int(first), int(count), _p(f, ctypes.c_float), _p(t, ctypes.c_float)))
+        return f, t

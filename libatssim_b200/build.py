@@ -23,7 +23,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"] + ARCH
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-I/usr/local/cuda/include"]
 
-CU_SOURCES = ["ats_cloth.cu", "ats_noalloc.cu"]
+CU_SOURCES = ["ats_cloth.cu", "ats_learn.cu", "ats_noalloc.cu"]
 CXX_SOURCES = ["ats_topology.cpp", "ats_launcher.cpp"]
 
 

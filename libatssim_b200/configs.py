@@ -64,6 +64,20 @@ def c2(num_instances=256, seed=0, side_range=(16, 256)):
     return insts, dict(implicit_dt=1.0 / 60.0, num_substep=1, iterations=50, damping=2.0)
 
 
+def wind_accel(rng, total_mass, gravity=(0.0, -9.8, 0.0), max_force=2.0):
+    """Gravity plus a random wind force: direction uniform on the sphere, magnitude
+    U[0, max_force] N, spread over the instance mass."""
+    d = rng.standard_normal(3)
+    d /= np.linalg.norm(d)
+    f = rng.uniform(0.0, max_force) * d
+    return np.asarray(gravity, dtype=np.float64) + f / float(total_mass)
+
+
+def c3():
+    """128 x 128 cloth of the c0 material, random wind per frame, 200 iterations."""
+    return [grid_instance(128)], dict(implicit_dt=1.0 / 60.0, num_substep=1, iterations=200, damping=2.0)
+
+
 def reference_square(positions, faces):
     """libAtsSim Example 2 material on a given mesh (0.01 kg per vertex)."""
     mass = np.full(positions.shape[0], 0.01, dtype=np.float32)

@@ -7,16 +7,18 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
 #include <memory>
+#include <thread>
 #include <string>
 #include <vector>
 
-#include "../../include/ats_cloth.h"
+#include "ats_internal.cuh"
 #include "ats_kernels.cuh"
-#include "ats_topology.hpp"
 
 namespace ats {
 
@@ -24,30 +26,6 @@ static thread_local std::string g_last_error;
 void set_error(const std::string& msg) { g_last_error = msg; }
 
 namespace {
-
-#define ATS_CUDA(call)                                                                          \
-    do {                                                                                        \
-        cudaError_t _e = (call);                                                                \
-        if (_e != cudaSuccess) {                                                                \
-            set_error(std::string(#call) + ": " + cudaGetErrorString(_e));                      \
-            return ATS_ERR_CUDA;                                                                \
-        }                                                                                       \
-    } while (0)
-
-template <typename T>
-struct DevBuf {
-    T* p = nullptr;
-    size_t n = 0;
-    ~DevBuf() {
-        if (p) cudaFree(p);
-    }
-    cudaError_t alloc(size_t count) {
-        n = count;
-        if (count == 0) return cudaSuccess;
-        return cudaMalloc((void**)&p, count * sizeof(T));
-    }
-    size_t bytes() const { return n * sizeof(T); }
-};
 
 // ---------------------------------------------------------------- kernels
 
@@ -384,62 +362,42 @@ __global__ void __launch_bounds__(kSegChunks) segment_final_kernel(const double*
     if (threadIdx.x == 0) out[blockIdx.x] = sqrt(s);
 }
 
+// Residual bookkeeping of ats_frame_to_residual, one block: the first call after
+// predict stores ||grad G(y)|| per instance; later calls deactivate an instance once
+// ||grad G(x)|| <= tol ||grad G(y)|| or its iteration cap is reached; n_active
+// receives the number of instances still iterating.
+__global__ void __launch_bounds__(256) residual_check_kernel(const double* norm, double* norm0, int* active, int* iters,
+                                                            int* n_active, int ninst, int first, int step,
+                                                            int max_iters, double tol, const double* tols) {
+    __shared__ int count[256];
+    int c = 0;
+    for (int i = threadIdx.x; i < ninst; i += blockDim.x) {
+        if (first) {
+            norm0[i] = norm[i];
+            active[i] = norm[i] > 0.0 && max_iters > 0 ? 1 : 0;
+            iters[i] = 0;
+        } else if (active[i]) {
+            iters[i] += step;
+            const double ti = tols ? tols[i] : tol;
+            if (norm[i] <= ti * norm0[i] || iters[i] >= max_iters) active[i] = 0;
+        }
+        c += active[i];
+    }
+    count[threadIdx.x] = c;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) count[threadIdx.x] += count[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *n_active = count[0];
+}
+
 }  // namespace
 }  // namespace ats
 
 using namespace ats;
 
-struct ats_cloth {
-    Layout L;
-    ats_solver_params prm{};
-    int device = 0;
-    int block = 128;
-    float h = 0.f, h2inv = 0.f, damp = 1.f;
-    // device arrays
-    DevBuf<float4> x, x0, vel, vm, inst;
-    DevBuf<int2> st_iw;
-    DevBuf<float> st_rest;
-    DevBuf<int4> slices;
-    DevBuf<int2> xs_edge;
-    DevBuf<float> xs_rest, xs_k, xs_lambda;
-    DevBuf<int4> xb_idx;
-    DevBuf<float4> xb_q;
-    DevBuf<float> xb_lambda;
-    DevBuf<int2> en_edge;
-    DevBuf<float> en_rest, en_k, en_q, en_kb;
-    DevBuf<int4> en_bend;
-    DevBuf<int> inst_seg;
-    DevBuf<int> to_caller;
-    DevBuf<float> io_x, io_v;  // caller-order staging of the state
-    // scratch of the FP64 reductions
-    DevBuf<double> partial, seg_partial, red_out, g2;
-    cudaStream_t capture_stream = nullptr;
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};
-
-    void drop_graphs() {
-        for (auto& g : graph)
-            if (g) {
-                cudaGraphExecDestroy(g);
-                g = nullptr;
-            }
-    }
-    ~ats_cloth() {
-        drop_graphs();
-        if (capture_stream) cudaStreamDestroy(capture_stream);
-    }
-    size_t device_bytes() const {
-        return x.bytes() + x0.bytes() + vel.bytes() + vm.bytes() + inst.bytes() + st_iw.bytes() + st_rest.bytes() +
-               slices.bytes() + xs_edge.bytes() + xs_rest.bytes() + xs_k.bytes() + xs_lambda.bytes() +
-               xb_idx.bytes() + xb_q.bytes() + xb_lambda.bytes() + en_edge.bytes() + en_rest.bytes() + en_k.bytes() +
-               en_q.bytes() + en_kb.bytes() + en_bend.bytes() + inst_seg.bytes() + to_caller.bytes() + io_x.bytes() +
-               io_v.bytes() + partial.bytes() +
-               seg_partial.bytes() + red_out.bytes() + g2.bytes();
-    }
-};
-
-namespace {
-
-inline cudaStream_t S(ats_stream s) { return (cudaStream_t)s; }
+namespace ats {
 
 template <typename T, typename U>
 int upload(DevBuf<T>& d, const std::vector<U>& h, size_t count) {
@@ -486,7 +444,7 @@ cudaError_t sweep_launch(dim3 grid, dim3 block, cudaStream_t st, const SweepArgs
     return cudaLaunchKernelEx(&cfg, vbd_sweep_kernel<TPV, RE, RB>, a);
 }
 
-int launch_sweep(ats_cloth* c, int color, cudaStream_t st) {
+int launch_sweep(ats_cloth* c, int color, cudaStream_t st, const int* active) {
     const int sb = c->L.color_slices[color], se = c->L.color_slices[color + 1];
     if (se <= sb) return ATS_OK;
     SweepArgs a;
@@ -498,6 +456,7 @@ int launch_sweep(ats_cloth* c, int color, cudaStream_t st) {
     a.st_rest = c->st_rest.p;
     a.slices = c->slices.p;
     a.inst = c->inst.p;
+    a.active = active;
     a.slice_begin = sb;
     a.slice_end = se;
     a.h = c->h;
@@ -556,12 +515,12 @@ int launch_xpbd_bending(ats_cloth* c, int color, cudaStream_t st) {
     return ATS_OK;
 }
 
-int enqueue_iterations(ats_cloth* c, int solver, int iterations, cudaStream_t st) {
+int enqueue_iterations(ats_cloth* c, int solver, int iterations, cudaStream_t st, const int* active) {
     int r;
     for (int it = 0; it < iterations; ++it) {
         if (solver == ATS_SOLVER_VBD) {
             for (int col = 0; col < c->L.n_vcolors; ++col)
-                if ((r = launch_sweep(c, col, st))) return r;
+                if ((r = launch_sweep(c, col, st, active))) return r;
         } else {
             for (int col = 0; col < c->L.n_scolors; ++col)
                 if ((r = launch_xpbd_stretch(c, col, st))) return r;
@@ -583,7 +542,85 @@ int enqueue_frame(ats_cloth* c, int solver, cudaStream_t st) {
     return ATS_OK;
 }
 
-}  // namespace
+int enqueue_residual_norms(ats_cloth* c, cudaStream_t st) {
+    GradArgs a;
+    a.x = c->x.p;
+    a.x0 = c->x0.p;
+    a.vel = c->vel.p;
+    a.vm = c->vm.p;
+    a.inst = c->inst.p;
+    a.st_iw = c->st_iw.p;
+    a.st_rest = c->st_rest.p;
+    a.slices = c->slices.p;
+    a.nslices = (int)c->slices.n;
+    a.tpv = c->L.tpv;
+    a.h = (double)c->h;
+    a.g2 = c->g2.p;
+    const int blocks = (a.nslices * 32 + 127) / 128;
+    grad_kernel<<<blocks, 128, 0, st>>>(a);
+    ATS_CUDA(cudaGetLastError());
+    segment_partial_kernel<<<dim3(kSegChunks, c->L.ninst), kRedThreads, 0, st>>>(c->g2.p, c->inst_seg.p,
+                                                                                   c->seg_partial.p);
+    ATS_CUDA(cudaGetLastError());
+    segment_final_kernel<<<c->L.ninst, kSegChunks, 0, st>>>(c->seg_partial.p, c->red_out.p);
+    ATS_CUDA(cudaGetLastError());
+    return ATS_OK;
+}
+
+int frame_to_residual_impl(ats_cloth* c, double tol, const double* tols, int check_every, int max_iterations,
+                           int* iterations, double* residual, cudaStream_t st,
+                           const std::function<int(cudaStream_t)>& after_predict) {
+    if (!c || !(tol >= 0.0) || check_every <= 0 || max_iterations < 0) {
+        set_error("frame to residual: need a handle, tol >= 0, check_every > 0, max_iterations >= 0");
+        return ATS_ERR_INVALID;
+    }
+    const int ni = c->L.ninst;
+    int r;
+    const double* dtols = nullptr;
+    if (tols) {
+        if (!c->tols.p) ATS_CUDA(c->tols.alloc(ni));
+        ATS_CUDA(cudaMemcpyAsync(c->tols.p, tols, ni * sizeof(double), cudaMemcpyHostToDevice, st));
+        dtols = c->tols.p;
+    }
+    for (int sub = 0; sub < c->prm.num_substep; ++sub) {
+        if ((r = launch_predict(c, st)) || (r = enqueue_residual_norms(c, st))) return r;
+        residual_check_kernel<<<1, 256, 0, st>>>(c->red_out.p, c->norm0.p, c->active.p, c->iters.p, c->n_active.p, ni,
+                                                  1, 0, max_iterations, tol, dtols);
+        ATS_CUDA(cudaGetLastError());
+        if (after_predict && (r = after_predict(st))) return r;
+        for (int done = 0; done < max_iterations;) {
+            ATS_CUDA(cudaMemcpyAsync(c->host_flag, c->n_active.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+            ATS_CUDA(cudaStreamSynchronize(st));
+            if (*c->host_flag == 0) break;
+            const int step = std::min(check_every, max_iterations - done);
+            if ((r = enqueue_iterations(c, ATS_SOLVER_VBD, step, st, c->active.p)) || (r = enqueue_residual_norms(c, st)))
+                return r;
+            done += step;
+            residual_check_kernel<<<1, 256, 0, st>>>(c->red_out.p, c->norm0.p, c->active.p, c->iters.p, c->n_active.p,
+                                                      ni, 0, step, max_iterations, tol, dtols);
+            ATS_CUDA(cudaGetLastError());
+        }
+        if (sub + 1 == c->prm.num_substep && (iterations || residual)) {
+            // report against the last substep: residual relative to ||grad G(y)||
+            if (residual) {
+                std::vector<double> nrm(ni), n0(ni);
+                ATS_CUDA(cudaMemcpyAsync(nrm.data(), c->red_out.p, ni * sizeof(double), cudaMemcpyDeviceToHost, st));
+                ATS_CUDA(cudaMemcpyAsync(n0.data(), c->norm0.p, ni * sizeof(double), cudaMemcpyDeviceToHost, st));
+                ATS_CUDA(cudaStreamSynchronize(st));
+                for (int i = 0; i < ni; ++i) residual[i] = n0[i] > 0.0 ? nrm[i] / n0[i] : 0.0;
+            }
+            if (iterations) {
+                ATS_CUDA(cudaMemcpyAsync(iterations, c->iters.p, ni * sizeof(int), cudaMemcpyDeviceToHost, st));
+                ATS_CUDA(cudaStreamSynchronize(st));
+            }
+        }
+        if ((r = launch_update(c, st))) return r;
+    }
+    ATS_CUDA(cudaStreamSynchronize(st));
+    return ATS_OK;
+}
+
+}  // namespace ats
 
 extern "C" {
 
@@ -614,11 +651,25 @@ int ats_cloth_create(const ats_instance_desc* inst, int ninst, const ats_solver_
     std::vector<Topology> topos(ninst);
     std::vector<ats_instance_desc> descs(inst, inst + ninst);
     std::string err;
-    for (int i = 0; i < ninst; ++i)
-        if (!build_topology(inst[i], topos[i], err)) {
-            set_error("ats_cloth_create: instance " + std::to_string(i) + ": " + err);
-            return ATS_ERR_INVALID;
-        }
+    {
+        // instances are independent: build their topologies on a few host threads
+        std::vector<std::string> errs(ninst);
+        std::vector<char> ok(ninst, 1);
+        const int nthreads = std::max(1, std::min(ninst, (int)std::thread::hardware_concurrency()));
+        std::atomic<int> next{0};
+        auto work = [&] {
+            for (int i = next++; i < ninst; i = next++) ok[i] = build_topology(inst[i], topos[i], errs[i]);
+        };
+        std::vector<std::thread> pool;
+        for (int t = 1; t < nthreads; ++t) pool.emplace_back(work);
+        work();
+        for (auto& t : pool) t.join();
+        for (int i = 0; i < ninst; ++i)
+            if (!ok[i]) {
+                set_error("ats_cloth_create: instance " + std::to_string(i) + ": " + errs[i]);
+                return ATS_ERR_INVALID;
+            }
+    }
     std::unique_ptr<ats_cloth> c(new (std::nothrow) ats_cloth());
     if (!c) {
         set_error("ats_cloth_create: out of memory");
@@ -656,12 +707,21 @@ int ats_cloth_create(const ats_instance_desc* inst, int ninst, const ats_solver_
         return r;
     if ((r = upload(c->inst_seg, L.inst_vbegin, L.inst_vbegin.size()))) return r;
     if ((r = upload(c->to_caller, L.to_caller, nv))) return r;
+    if ((r = upload(c->feat_nb, L.feat_nb, L.feat_nb.size())) || (r = upload(c->feat_len, L.feat_len, L.feat_len.size())) ||
+        (r = upload(c->inst_eseg, L.inst_eseg, L.inst_eseg.size())) ||
+        (r = upload(c->inst_bseg, L.inst_bseg, L.inst_bseg.size())))
+        return r;
     ATS_CUDA(c->io_x.alloc(3 * nv));
     ATS_CUDA(c->io_v.alloc(3 * nv));
     ATS_CUDA(c->partial.alloc(3 * (size_t)kRedBlocks));
     ATS_CUDA(c->seg_partial.alloc((size_t)kSegChunks * L.ninst));
     ATS_CUDA(c->red_out.alloc(std::max(3, L.ninst)));
     ATS_CUDA(c->g2.alloc(nv));
+    ATS_CUDA(c->norm0.alloc(L.ninst));
+    ATS_CUDA(c->active.alloc(L.ninst));
+    ATS_CUDA(c->iters.alloc(L.ninst));
+    ATS_CUDA(c->n_active.alloc(1));
+    ATS_CUDA(cudaHostAlloc((void**)&c->host_flag, sizeof(int), cudaHostAllocDefault));
     ATS_CUDA(cudaStreamCreateWithFlags(&c->capture_stream, cudaStreamNonBlocking));
     ATS_CUDA(cudaDeviceSynchronize());
     *out = c.release();
@@ -691,6 +751,15 @@ int ats_cloth_query(const ats_cloth* c, ats_cloth_info* info) {
     info->block_size = c->block;
     info->stencil_slots = (int)c->L.st_rest.size();
     info->device_bytes = (long long)c->device_bytes();
+    return ATS_OK;
+}
+
+int ats_cloth_vertex_order(const ats_cloth* c, int* layout_of_caller) {
+    if (!c || !layout_of_caller) {
+        set_error("ats_cloth_vertex_order: null argument");
+        return ATS_ERR_INVALID;
+    }
+    std::memcpy(layout_of_caller, c->L.to_layout.data(), c->L.nv * sizeof(int));
     return ATS_OK;
 }
 
@@ -941,33 +1010,32 @@ int ats_energy(ats_cloth* c, double* out3, ats_stream stream) {
     return ATS_OK;
 }
 
+int ats_frame_to_residual(ats_cloth* c, double tol, int check_every, int max_iterations, int* iterations,
+                          double* residual, ats_stream stream) {
+    if (!c) {
+        set_error("ats_frame_to_residual: null handle");
+        return ATS_ERR_INVALID;
+    }
+    return frame_to_residual_impl(c, tol, nullptr, check_every, max_iterations, iterations, residual, S(stream), nullptr);
+}
+
+int ats_frame_to_residuals(ats_cloth* c, const double* tols, int check_every, int max_iterations, int* iterations,
+                           double* residual, ats_stream stream) {
+    if (!c || !tols) {
+        set_error("ats_frame_to_residuals: need a handle and one tolerance per instance");
+        return ATS_ERR_INVALID;
+    }
+    return frame_to_residual_impl(c, 0.0, tols, check_every, max_iterations, iterations, residual, S(stream), nullptr);
+}
+
 int ats_residual(ats_cloth* c, double* out, ats_stream stream) {
     if (!c || !out) {
         set_error("ats_residual: null argument");
         return ATS_ERR_INVALID;
     }
     cudaStream_t st = S(stream);
-    GradArgs a;
-    a.x = c->x.p;
-    a.x0 = c->x0.p;
-    a.vel = c->vel.p;
-    a.vm = c->vm.p;
-    a.inst = c->inst.p;
-    a.st_iw = c->st_iw.p;
-    a.st_rest = c->st_rest.p;
-    a.slices = c->slices.p;
-    a.nslices = (int)c->slices.n;
-    a.tpv = c->L.tpv;
-    a.h = (double)c->h;
-    a.g2 = c->g2.p;
-    const int blocks = (a.nslices * 32 + 127) / 128;
-    grad_kernel<<<blocks, 128, 0, st>>>(a);
-    ATS_CUDA(cudaGetLastError());
-    segment_partial_kernel<<<dim3(kSegChunks, c->L.ninst), kRedThreads, 0, st>>>(c->g2.p, c->inst_seg.p,
-                                                                                   c->seg_partial.p);
-    ATS_CUDA(cudaGetLastError());
-    segment_final_kernel<<<c->L.ninst, kSegChunks, 0, st>>>(c->seg_partial.p, c->red_out.p);
-    ATS_CUDA(cudaGetLastError());
+    int r = enqueue_residual_norms(c, st);
+    if (r) return r;
     ATS_CUDA(cudaMemcpyAsync(out, c->red_out.p, c->L.ninst * sizeof(double), cudaMemcpyDeviceToHost, st));
     ATS_CUDA(cudaStreamSynchronize(st));
     return ATS_OK;

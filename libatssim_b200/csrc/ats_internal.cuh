@@ -1,0 +1,122 @@
+// ats_internal.cuh -- handle layout and helpers shared by the library's .cu files.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <functional>
+#include <string>
+#include <vector>
+
+#include "../../include/ats_cloth.h"
+#include "ats_topology.hpp"
+
+namespace ats {
+
+void set_error(const std::string& msg);
+
+#define ATS_CUDA(call)                                                                          \
+    do {                                                                                        \
+        cudaError_t _e = (call);                                                                \
+        if (_e != cudaSuccess) {                                                                \
+            set_error(std::string(#call) + ": " + cudaGetErrorString(_e));                      \
+            return ATS_ERR_CUDA;                                                                \
+        }                                                                                       \
+    } while (0)
+
+template <typename T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+    cudaError_t alloc(size_t count) {
+        n = count;
+        if (count == 0) return cudaSuccess;
+        return cudaMalloc((void**)&p, count * sizeof(T));
+    }
+    size_t bytes() const { return n * sizeof(T); }
+};
+
+inline cudaStream_t S(ats_stream s) { return (cudaStream_t)s; }
+
+}  // namespace ats
+
+struct ats_cloth {
+    using Layout = ats::Layout;
+    template <typename T>
+    using DevBuf = ats::DevBuf<T>;
+    Layout L;
+    ats_solver_params prm{};
+    int device = 0;
+    int block = 128;
+    float h = 0.f, h2inv = 0.f, damp = 1.f;
+    // device arrays
+    DevBuf<float4> x, x0, vel, vm, inst;
+    DevBuf<int2> st_iw;
+    DevBuf<float> st_rest;
+    DevBuf<int4> slices;
+    DevBuf<int2> xs_edge;
+    DevBuf<float> xs_rest, xs_k, xs_lambda;
+    DevBuf<int4> xb_idx;
+    DevBuf<float4> xb_q;
+    DevBuf<float> xb_lambda;
+    DevBuf<int2> en_edge;
+    DevBuf<float> en_rest, en_k, en_q, en_kb;
+    DevBuf<int4> en_bend;
+    DevBuf<int> inst_seg;
+    DevBuf<int> to_caller;
+    DevBuf<float> io_x, io_v;  // caller-order staging of the state
+    // scratch of the FP64 reductions
+    DevBuf<double> partial, seg_partial, red_out, g2, norm0, tols;
+    DevBuf<int> active, iters, n_active;  // ats_frame_to_residual bookkeeping
+    int* host_flag = nullptr;             // pinned copy of n_active
+    // learned warm start (uploaded at create; the rest allocated on first use)
+    DevBuf<int> feat_nb, inst_eseg, inst_bseg, free_list;
+    DevBuf<float> feat_len, feat_stage;
+    DevBuf<float4> y_buf;
+    DevBuf<double> pot_partial, pot_y, pot_guess;
+    DevBuf<int> guess_used;
+    cudaStream_t capture_stream = nullptr;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+
+    void drop_graphs() {
+        for (auto& g : graph)
+            if (g) {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
+    }
+    ~ats_cloth() {
+        drop_graphs();
+        if (capture_stream) cudaStreamDestroy(capture_stream);
+        if (host_flag) cudaFreeHost(host_flag);
+    }
+    size_t device_bytes() const {
+        return x.bytes() + x0.bytes() + vel.bytes() + vm.bytes() + inst.bytes() + st_iw.bytes() + st_rest.bytes() +
+               slices.bytes() + xs_edge.bytes() + xs_rest.bytes() + xs_k.bytes() + xs_lambda.bytes() +
+               xb_idx.bytes() + xb_q.bytes() + xb_lambda.bytes() + en_edge.bytes() + en_rest.bytes() + en_k.bytes() +
+               en_q.bytes() + en_kb.bytes() + en_bend.bytes() + inst_seg.bytes() + to_caller.bytes() + io_x.bytes() +
+               io_v.bytes() + partial.bytes() +
+               seg_partial.bytes() + red_out.bytes() + g2.bytes() + norm0.bytes() + active.bytes() + iters.bytes() +
+               n_active.bytes();
+    }
+};
+
+
+namespace ats {
+
+// Kernel launches of one handle (ats_cloth.cu); each returns an ATS_* status.
+int launch_predict(ats_cloth* c, cudaStream_t st);
+int launch_update(ats_cloth* c, cudaStream_t st);
+int launch_sweep(ats_cloth* c, int color, cudaStream_t st, const int* active = nullptr);
+int enqueue_iterations(ats_cloth* c, int solver, int iterations, cudaStream_t st, const int* active = nullptr);
+// FP64 ||grad G|| per instance into c->red_out.p
+int enqueue_residual_norms(ats_cloth* c, cudaStream_t st);
+// ats_frame_to_residual with an optional hook run after ||grad G(y)|| is taken and
+// before the first iteration (the learned warm start replaces y there).
+int frame_to_residual_impl(ats_cloth* c, double tol, const double* tols, int check_every, int max_iterations,
+                           int* iterations, double* residual, cudaStream_t st,
+                           const std::function<int(cudaStream_t)>& after_predict);
+
+}  // namespace ats

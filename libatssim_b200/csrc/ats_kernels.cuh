@@ -34,6 +34,7 @@ struct SweepArgs {
     const float* __restrict__ st_rest;
     const int4* __restrict__ slices;
     const float4* __restrict__ inst;
+    const int* __restrict__ active;  // per instance, null = all active
     int slice_begin, slice_end;
     float h, h2inv;
 };
@@ -143,6 +144,8 @@ __global__ void __launch_bounds__(256) vbd_sweep_kernel(SweepArgs a) {
 
     grid_dependency_wait();
     allow_dependent_launch();
+    // a slice belongs to one instance: instances that have converged are skipped
+    if (a.active && !a.active[__float_as_int(mv.w)]) return;
 
     // positions and frame-start state (ordered behind the previous kernel); the
     // neighbours belong to other colours, which this launch does not write

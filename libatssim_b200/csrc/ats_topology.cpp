@@ -195,54 +195,60 @@ bool build_slices(Layout& L, int tpv, std::string& err) {
     }
     L.tpv = tpv;
     const int vps = 32 / tpv;  // vertices per slice (one warp)
-    L.st_iw.clear();
-    L.st_rest.clear();
-    L.slices.clear();
-    L.color_slices.assign(1, 0);
-    // Per vertex: edge neighbours first (rest >= 0), then bending-only neighbours.
-    // The neighbour lists are sorted by layout id inside each group.
-    auto n_edges = [&](int v) {
-        int c = 0;
-        for (int q = L.nb_off[v]; q < L.nb_off[v + 1]; ++q) c += L.nb_rest[q] >= 0.f;
-        return c;
+    // size the arrays first
+    size_t total = 0;
+    size_t nslices = 0;
+    auto slice_rows = [&](int s, int n, int& erows, int& brows) {
+        int max_e = 0, max_b = 0;
+        for (int k = 0; k < n; ++k) {
+            const int ne = L.nb_nedge[s + k];
+            max_e = std::max(max_e, ne);
+            max_b = std::max(max_b, L.nb_off[s + k + 1] - L.nb_off[s + k] - ne);
+        }
+        erows = (max_e + tpv - 1) / tpv;
+        brows = (max_b + tpv - 1) / tpv;
     };
-    std::vector<int> order;
+    for (int c = 0; c < L.n_vcolors; ++c)
+        for (int ri = L.run_off[c]; ri < L.run_off[c + 1]; ++ri)
+            for (int s = L.runs[2 * ri]; s < L.runs[2 * ri + 1]; s += vps) {
+                int er, br;
+                slice_rows(s, std::min(vps, L.runs[2 * ri + 1] - s), er, br);
+                total += 32 * (size_t)(er + br);
+                ++nslices;
+            }
+    L.st_iw.assign(2 * total, 0);
+    L.st_rest.assign(total, -1.f);
+    L.slices.clear();
+    L.slices.reserve(4 * nslices);
+    L.color_slices.assign(1, 0);
+    size_t off = 0;
+    // entry (row, thread th) of a slice = vertex th / tpv, slot row * tpv + th % tpv
+    // within the edge rows (first erows rows) or the bending-only rows
     for (int c = 0; c < L.n_vcolors; ++c) {
         for (int ri = L.run_off[c]; ri < L.run_off[c + 1]; ++ri) {
             const int b = L.runs[2 * ri], e = L.runs[2 * ri + 1];
             for (int s = b; s < e; s += vps) {
                 const int n = std::min(vps, e - s);
-                int max_e = 0, max_b = 0;
-                for (int k = 0; k < n; ++k) {
-                    const int ne = n_edges(s + k);
-                    max_e = std::max(max_e, ne);
-                    max_b = std::max(max_b, L.nb_off[s + k + 1] - L.nb_off[s + k] - ne);
-                }
-                const int erows = (max_e + tpv - 1) / tpv, brows = (max_b + tpv - 1) / tpv;
+                int erows, brows;
+                slice_rows(s, n, erows, brows);
                 const int rows = erows + brows;
-                const size_t off = L.st_rest.size();
-                L.st_iw.resize(2 * (off + 32 * (size_t)rows));
-                L.st_rest.resize(off + 32 * (size_t)rows);
                 for (int th = 0; th < 32; ++th) {
                     const int k = th / tpv;
                     const int self = s + std::min(k, n - 1);
-                    // this vertex's neighbours split into edge / bending-only slots
-                    std::vector<int> eq, bq;
-                    if (k < n)
-                        for (int q = L.nb_off[s + k]; q < L.nb_off[s + k + 1]; ++q)
-                            (L.nb_rest[q] >= 0.f ? eq : bq).push_back(q);
+                    const int lo = k < n ? L.nb_off[s + k] : 0;
+                    const int ne = k < n ? L.nb_nedge[s + k] : 0;
+                    const int nb = k < n ? L.nb_off[s + k + 1] - lo - ne : 0;
                     for (int row = 0; row < rows; ++row) {
                         const bool edge_row = row < erows;
                         const int slot = (edge_row ? row : row - erows) * tpv + th % tpv;
-                        const std::vector<int>& src = edge_row ? eq : bq;
                         const size_t at = off + 32 * (size_t)row + th;
                         int idx = self;
                         float w = 0.f, rest = -1.f;
-                        if (slot < (int)src.size()) {
-                            const int q = src[slot];
+                        if (edge_row ? slot < ne : slot < nb) {
+                            const int q = lo + (edge_row ? slot : ne + slot);
                             idx = L.nb_u[q];
                             w = L.nb_w[q];
-                            rest = L.nb_rest[q];
+                            rest = edge_row ? L.nb_rest[q] : -1.f;
                         }
                         L.st_iw[2 * at] = idx;
                         std::memcpy(&L.st_iw[2 * at + 1], &w, 4);
@@ -253,6 +259,7 @@ bool build_slices(Layout& L, int tpv, std::string& err) {
                 L.slices.push_back(n);
                 L.slices.push_back((int)off);
                 L.slices.push_back(rows | (erows << 16));
+                off += 32 * (size_t)rows;
             }
         }
         L.color_slices.push_back((int)L.slices.size() / 4);
@@ -318,46 +325,55 @@ bool build_layout(const std::vector<Topology>& topos, const std::vector<ats_inst
         L.run_off.push_back((int)L.runs.size() / 2);
     }
 
-    // per-vertex data and neighbour lists (in layout ids, sorted by neighbour id)
+    // per-vertex data and neighbour lists (in layout ids): edge neighbours first,
+    // then bending-only neighbours, each sorted by id; bending weights summed in FP64
     struct Nb {
         int u;
         float rest;
         double w;
     };
     std::vector<std::vector<Nb>> sten(L.nv);
+    std::vector<int> nedge(L.nv, 0);
     for (int i = 0; i < L.ninst; ++i) {
         const Topology& t = topos[i];
         const ats_instance_desc& d = descs[i];
         const int ob = L.inst_vbegin[i];
+        std::vector<Nb> cand;
         for (int v = 0; v < t.nv; ++v) {
-            int lv = L.to_layout[ob + v];
-            std::map<int, Nb> m;
+            const int lv = L.to_layout[ob + v];
+            cand.clear();
             for (int k = t.ve_off[v]; k < t.ve_off[v + 1]; ++k) {
-                int e = t.ve[k];
-                int u = t.edges[2 * e] == v ? t.edges[2 * e + 1] : t.edges[2 * e];
-                int lu = L.to_layout[ob + u];
-                m[lu] = Nb{lu, t.rest[e], 0.0};
+                const int e = t.ve[k];
+                const int u = t.edges[2 * e] == v ? t.edges[2 * e + 1] : t.edges[2 * e];
+                cand.push_back(Nb{L.to_layout[ob + u], t.rest[e], 0.0});
             }
             double hdiag = 0.0;
             for (int k = t.vb_off[v]; k < t.vb_off[v + 1]; ++k) {
-                int e = t.vb[k];
+                const int e = t.vb[k];
                 const int* be = &t.bending[4 * e];
-                int o = be[0] == v ? 0 : be[1] == v ? 1 : be[2] == v ? 2 : 3;
+                const int o = be[0] == v ? 0 : be[1] == v ? 1 : be[2] == v ? 2 : 3;
                 const float* Q = &t.q[16 * (size_t)e];  // Q[col][row], symmetric
                 hdiag += (double)Q[4 * o + o];
-                for (int j = 0; j < 4; ++j) {
-                    if (j == o) continue;
-                    int lu = L.to_layout[ob + be[j]];
-                    auto it = m.find(lu);
-                    if (it == m.end()) it = m.emplace(lu, Nb{lu, -1.f, 0.0}).first;
-                    it->second.w += (double)Q[4 * o + j];
+                for (int j = 0; j < 4; ++j)
+                    if (j != o) cand.push_back(Nb{L.to_layout[ob + be[j]], -2.f, (double)Q[4 * o + j]});
+            }
+            // merge by neighbour id: the edge entry carries the rest length
+            std::sort(cand.begin(), cand.end(), [](const Nb& x, const Nb& y) { return x.u < y.u; });
+            std::vector<Nb>& out = sten[lv];
+            for (size_t k = 0; k < cand.size();) {
+                Nb m{cand[k].u, -1.f, 0.0};
+                size_t j = k;
+                for (; j < cand.size() && cand[j].u == m.u; ++j) {
+                    if (cand[j].rest > -2.f) m.rest = cand[j].rest;
+                    m.w += cand[j].w;
                 }
+                out.push_back(m);
+                k = j;
             }
+            std::stable_partition(out.begin(), out.end(), [](const Nb& x) { return x.rest >= 0.f; });
+            for (const Nb& x : out) nedge[lv] += x.rest >= 0.f;
             const double kb = d.k_bend;
-            for (auto& kv : m) {
-                kv.second.w *= kb;
-                sten[lv].push_back(kv.second);
-            }
+            for (Nb& x : out) x.w *= kb;
             const float mass = d.mass[v];
             const bool fixed = d.fixed[v] != 0;
             L.x0[4 * (size_t)lv + 0] = t.pos[3 * v];
@@ -372,6 +388,7 @@ bool build_layout(const std::vector<Topology>& topos, const std::vector<ats_inst
         }
     }
     L.nb_off.assign(1, 0);
+    L.nb_nedge = nedge;
     for (int lv = 0; lv < L.nv; ++lv) {
         for (const Nb& nb : sten[lv]) {
             L.nb_u.push_back(nb.u);
@@ -419,7 +436,9 @@ bool build_layout(const std::vector<Topology>& topos, const std::vector<ats_inst
         L.xb_color.push_back((int)L.xb_idx.size() / 4);
     }
 
-    // energy terms in original element order
+    // energy terms in original element order, instance by instance
+    L.inst_eseg.assign(1, 0);
+    L.inst_bseg.assign(1, 0);
     for (int i = 0; i < L.ninst; ++i) {
         const Topology& t = topos[i];
         const int ob = L.inst_vbegin[i];
@@ -433,6 +452,45 @@ bool build_layout(const std::vector<Topology>& topos, const std::vector<ats_inst
             for (int j = 0; j < 4; ++j) L.en_bend.push_back(L.to_layout[ob + t.bending[4 * e + j]]);
             for (int j = 0; j < 16; ++j) L.en_q.push_back(t.q[16 * (size_t)e + j]);
             L.en_kb.push_back(descs[i].k_bend);
+        }
+        L.inst_eseg.push_back((int)L.en_rest.size());
+        L.inst_bseg.push_back((int)L.en_kb.size());
+    }
+
+    // direction slots of the edge neighbours (rest plane x-z): the six neighbour
+    // directions of a uniform-diagonal grid vertex, nearest angle wins
+    static const double kSlotDeg[6] = {0.0, 45.0, 90.0, 180.0, 225.0, 270.0};
+    L.feat_nb.assign(6 * (size_t)L.nv, -1);
+    L.feat_len.assign(6 * (size_t)L.nv, 0.f);
+    std::vector<double> best(6);
+    for (int i = 0; i < L.ninst; ++i) {
+        const Topology& t = topos[i];
+        const int ob = L.inst_vbegin[i];
+        for (int v = 0; v < t.nv; ++v) {
+            const int lv = L.to_layout[ob + v];
+            std::fill(best.begin(), best.end(), 1e30);
+            for (int k = t.ve_off[v]; k < t.ve_off[v + 1]; ++k) {
+                const int e = t.ve[k];
+                const int u = t.edges[2 * e] == v ? t.edges[2 * e + 1] : t.edges[2 * e];
+                const double dx = (double)t.pos[3 * u] - t.pos[3 * v], dz = (double)t.pos[3 * u + 2] - t.pos[3 * v + 2];
+                double deg = std::atan2(dz, dx) * 57.29577951308232;
+                if (deg < 0) deg += 360.0;
+                int slot = 0;
+                double dist = 1e30;
+                for (int q = 0; q < 6; ++q) {
+                    double d = std::fabs(deg - kSlotDeg[q]);
+                    d = std::min(d, 360.0 - d);
+                    if (d < dist) {
+                        dist = d;
+                        slot = q;
+                    }
+                }
+                if (dist < best[slot]) {
+                    best[slot] = dist;
+                    L.feat_nb[6 * (size_t)lv + slot] = L.to_layout[ob + u];
+                    L.feat_len[6 * (size_t)lv + slot] = t.rest[e];
+                }
+            }
         }
     }
     return true;

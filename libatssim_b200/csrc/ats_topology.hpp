@@ -57,8 +57,9 @@ struct Layout {
     std::vector<float> vm;          // {bending Hessian diagonal k_b sum Q_oo, pin boost (0 / 1e9), inv mass, instance id bits}
     std::vector<float> inst;        // per instance {gravity xyz, k_stretch}
     // neighbour lists (CSR, layout order): neighbour id, rest length (-1 = not an
-    // edge), bending weight k_b sum_b Q_b[o_v][o_u]
-    std::vector<int> nb_off, nb_u;
+    // edge), bending weight k_b sum_b Q_b[o_v][o_u]; per vertex the edge neighbours
+    // come first (nb_nedge of them), then the bending-only ones, each group sorted by id
+    std::vector<int> nb_off, nb_u, nb_nedge;
     std::vector<float> nb_rest, nb_w;
     std::vector<int> runs;          // per colour c: runs[c] .. runs of (begin, end) layout ranges
     std::vector<int> run_off;       // n_vcolors + 1 offsets into runs (pairs)
@@ -82,6 +83,11 @@ struct Layout {
     std::vector<int> en_bend;       // 4 per bending edge
     std::vector<float> en_q;        // 16 per bending edge (column-major)
     std::vector<float> en_kb;
+    std::vector<int> inst_eseg, inst_bseg;  // ninst + 1 offsets into en_edge / en_bend pairs
+    // learned warm start: per vertex the edge neighbours in 6 rest-direction slots
+    // (+x, +x+z, +z, -x, -x-z, -z in the rest plane; -1 = none) and their rest lengths
+    std::vector<int> feat_nb;       // 6 per vertex, layout ids
+    std::vector<float> feat_len;    // 6 per vertex
 };
 
 bool build_layout(const std::vector<Topology>& topos, const std::vector<ats_instance_desc>& descs, const float* gravity,

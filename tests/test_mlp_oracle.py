@@ -1,0 +1,28 @@
+"""The warm-start MLP oracle checks itself: analytic gradients against central
+finite differences of the exact FP64 network (no GPU)."""
+import numpy as np
+
+from oracle import mlp_oracle as M
+
+
+def test_oracle_gradient_matches_finite_differences():
+    rng = np.random.RandomState(0)
+    theta = rng.uniform(-0.3, 0.3, M.NPARAMS)
+    x = rng.standard_normal((7, M.IN))
+    t = rng.standard_normal((7, M.OUT))
+    _, g = M.loss_and_grad(theta, x, t, quantize=False)
+    idx = rng.choice(M.NPARAMS, 40, replace=False)
+    idx = np.concatenate([idx, [0, 1535, 1536, 10111, 10112, 10114]])
+    fd = M.finite_difference(theta, x, t, idx)
+    assert np.allclose(g[idx], fd, rtol=1e-5, atol=1e-9)
+
+
+def test_bf16_rounding():
+    v = np.array([1.0, 1.00390625, 1.01171875, 1.001953125, -3.14159], dtype=np.float32)
+    r = M.bf16(v)
+    assert r[0] == 1.0
+    assert r[1] == 1.0          # 1 + 2^-8: a tie, rounds to the even mantissa
+    assert r[2] == 1.015625     # 1 + 3 * 2^-8: a tie, rounds up to the even mantissa
+    assert r[3] == 1.0          # below half a BF16 ulp
+    assert r[4] == -3.140625
+    assert M.NPARAMS == 10115

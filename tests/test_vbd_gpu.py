@@ -220,3 +220,48 @@ def test_bad_color_is_rejected(ats):
         cloth.vbd_color_sweep(cloth.info.num_vertex_colors)
     with pytest.raises(ats.AtsError):
         cloth.xpbd_stretch_color(-1)
+
+
+def test_frame_to_residual_matches_explicit_iterations(ats):
+    insts, prm = configs.c0()
+    a = ats.Cloth(insts, **prm)
+    b = ats.Cloth(insts, **prm)
+    for _ in range(5):
+        a.frame(graph=True)
+        b.frame(graph=True)
+    its, res = a.frame_to_residual(tol=0.25, check_every=5, max_iterations=400)
+    assert its[0] % 5 == 0 and 0 < its[0] <= 400
+    assert res[0] <= 0.25 or its[0] == 400
+    # the same frame by hand: predict, the same number of iterations, residual, update
+    b.predict()
+    r0 = b.residual()[0]
+    b.vbd_iterations(int(its[0]))
+    r1 = b.residual()[0]
+    b.update_velocity()
+    assert abs(r1 / r0 - res[0]) <= 1e-12 * max(1.0, res[0])
+    xa, va = a.state()
+    xb, vb = b.state()
+    assert np.array_equal(xa, xb) and np.array_equal(va, vb)
+
+
+def test_batched_early_exit_per_instance(ats):
+    insts, prm = configs.c2(num_instances=6, seed=5, side_range=(8, 48))
+    batch = ats.Cloth(insts, **prm)
+    for _ in range(2):
+        batch.frame(graph=True)
+    x_start, v_start = batch.state()
+    its, res = batch.frame_to_residual(tol=0.05, check_every=4, max_iterations=300)
+    assert len(set(its.tolist())) > 1  # instances stop at different iteration counts
+    xb, vb = batch.state()
+    off = 0
+    for i, inst in enumerate(insts):
+        n = inst.num_verts
+        one = ats.Cloth([inst], **prm)
+        one.set_state(x_start[off:off + n], v_start[off:off + n])
+        one.predict()
+        one.vbd_iterations(int(its[i]))
+        one.update_velocity()
+        x1, v1 = one.state()
+        assert np.array_equal(xb[off:off + n], x1), i
+        assert np.array_equal(vb[off:off + n], v1), i
+        off += n
