@@ -150,6 +150,8 @@ int ats_set_state(ats_cloth* cloth, const float* x, const float* v, ats_stream s
 int ats_get_state(ats_cloth* cloth, float* x, float* v, ats_stream stream);
 /* Current iterate x (mid-frame), same layout. Synchronises `stream`. */
 int ats_get_positions(ats_cloth* cloth, float* x, ats_stream stream);
+/* Replaces the current iterate x only (the frame start x0 and v stay). */
+int ats_set_positions(ats_cloth* cloth, const float* x, ats_stream stream);
 
 /* Per-instance external acceleration (gravity plus wind force / instance mass),
  * 3 floats per instance, read by the device at every predict / sweep; enqueued on
@@ -281,8 +283,12 @@ int ats_mlp_train(ats_mlp* mlp, const ats_dataset* data, int steps, int batch, f
  * y when its FP64 incremental potential G(guess) > G(y); used (host, one per instance,
  * nullable) receives 1 where the guess was kept (synchronises `stream` then). */
 int ats_warm_start(ats_cloth* cloth, const ats_mlp* mlp, int fallback, int* used, ats_stream stream);
-/* ats_frame with the learned guess between predict and the iterations. */
-int ats_frame_warm(ats_cloth* cloth, const ats_mlp* mlp, int fallback, ats_stream stream);
+/* ats_frame with the learned guess between predict and the iterations; `iterations`
+ * < 0 uses the handle's count. With use_graph != 0 the frame is replayed from a CUDA
+ * graph captured on first use (re-captured when the model, count or fallback change;
+ * the model's parameters may change between replays). */
+int ats_frame_warm(ats_cloth* cloth, const ats_mlp* mlp, int fallback, int iterations, int use_graph,
+                   ats_stream stream);
 /* ats_frame_to_residual with the learned guess; the residual stays relative to
  * ||grad G(y)|| of the inertial prediction. tols (host, one per instance) overrides
  * tol when not null. */

@@ -95,6 +95,7 @@ _SIGNATURES = {
     "ats_set_state": [_vp, _fp, _fp, _vp],
     "ats_get_state": [_vp, _fp, _fp, _vp],
     "ats_get_positions": [_vp, _fp, _vp],
+    "ats_set_positions": [_vp, _fp, _vp],
     "ats_set_accel": [_vp, _fp, _vp],
     "ats_predict_position": [_vp, _vp],
     "ats_vbd_color_sweep": [_vp, ctypes.c_int, _vp],
@@ -126,7 +127,7 @@ _SIGNATURES = {
     "ats_record_frame_end": [_vp, _vp, _vp],
     "ats_mlp_train": [_vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_ulonglong, _fp, _vp],
     "ats_warm_start": [_vp, _vp, ctypes.c_int, _ip, _vp],
-    "ats_frame_warm": [_vp, _vp, ctypes.c_int, _vp],
+    "ats_frame_warm": [_vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp],
     "ats_frame_warm_to_residual": [_vp, _vp, ctypes.c_int, ctypes.c_double, _dp, ctypes.c_int, ctypes.c_int, _ip, _dp,
                                    _ip, _vp],
     "ats_frame_to_residuals": [_vp, _dp, ctypes.c_int, ctypes.c_int, _ip, _dp, _vp],
@@ -337,6 +338,10 @@ class Cloth:
         _check(lib().ats_get_positions(self.h, _p(x, ctypes.c_float), _stream(stream)))
         return x
 
+    def set_positions(self, x, stream=None):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        _check(lib().ats_set_positions(self.h, _p(x, ctypes.c_float), _stream(stream)))
+
     def set_accel(self, accel, stream=None):
         a = np.ascontiguousarray(np.broadcast_to(np.asarray(accel, dtype=np.float32), (self.info.num_instances, 3)))
         _check(lib().ats_set_accel(self.h, _p(a, ctypes.c_float), _stream(stream)))
@@ -376,8 +381,8 @@ class Cloth:
         fn = lib().ats_frame_graph if graph else lib().ats_frame
         _check(fn(self.h, solver, _stream(stream)))
 
-    def frame_warm(self, mlp, fallback=True, stream=None):
-        _check(lib().ats_frame_warm(self.h, mlp.h, int(fallback), _stream(stream)))
+    def frame_warm(self, mlp, fallback=True, iterations=-1, graph=False, stream=None):
+        _check(lib().ats_frame_warm(self.h, mlp.h, int(fallback), int(iterations), int(graph), _stream(stream)))
 
     def warm_start(self, mlp, fallback=True, stream=None):
         used = np.zeros(self.info.num_instances, dtype=np.int32)

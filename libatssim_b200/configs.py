@@ -78,6 +78,16 @@ def c3():
     return [grid_instance(128)], dict(implicit_dt=1.0 / 60.0, num_substep=1, iterations=200, damping=2.0)
 
 
+def c4(num_instances=64, seed=0, side_range=(64, 512)):
+    """Batched instances of the c0 material, side U{64..512} from RandomState(seed + i),
+    two top corners pinned; random wind per instance per frame; 50 iterations."""
+    insts = []
+    for i in range(num_instances):
+        rng = np.random.RandomState(seed + i)
+        insts.append(grid_instance(int(rng.randint(side_range[0], side_range[1] + 1))))
+    return insts, dict(implicit_dt=1.0 / 60.0, num_substep=1, iterations=50, damping=2.0)
+
+
 def reference_square(positions, faces):
     """libAtsSim Example 2 material on a given mesh (0.01 kg per vertex)."""
     mass = np.full(positions.shape[0], 0.01, dtype=np.float32)

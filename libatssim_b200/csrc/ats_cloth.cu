@@ -177,6 +177,14 @@ __global__ void gather_state_kernel(const float4* __restrict__ src, const int* _
     dst[o + 2] = p.z;
 }
 
+__global__ void scatter_positions_kernel(const float* __restrict__ xc, const int* __restrict__ to_caller,
+                                         float4* __restrict__ x, int n) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const size_t o = 3 * (size_t)to_caller[i];
+    x[i] = make_float4(xc[o], xc[o + 1], xc[o + 2], 0.f);
+}
+
 // ---- FP64 reductions (deterministic: fixed element -> thread assignment, fixed tree)
 constexpr int kRedThreads = 256;
 constexpr int kRedBlocks = 296;  // 2 x 148 SMs
@@ -290,7 +298,8 @@ struct GradArgs {
     int nslices;
     int tpv;
     double h;
-    double* g2;  // per vertex (layout order)
+    double* g2;          // per vertex (layout order)
+    const int* active;   // per instance; null = all. Frozen instances keep their g2.
 };
 
 __global__ void grad_kernel(GradArgs a) {
@@ -303,7 +312,9 @@ __global__ void grad_kernel(GradArgs a) {
     if (k >= sd.y) return;
     if (lane % a.tpv != 0) return;  // the first lane of a vertex walks all its slots
     const int v = sd.x + k;
-    const float4 xv = a.x[v], p0 = a.x0[v], vv = a.vel[v], mv = a.vm[v];
+    const float4 mv = a.vm[v];
+    if (a.active && !a.active[__float_as_int(mv.w)]) return;  // unchanged since its last probe
+    const float4 xv = a.x[v], p0 = a.x0[v], vv = a.vel[v];
     if (mv.y != 0.f) {
         a.g2[v] = 0.0;
         return;
@@ -542,8 +553,9 @@ int enqueue_frame(ats_cloth* c, int solver, cudaStream_t st) {
     return ATS_OK;
 }
 
-int enqueue_residual_norms(ats_cloth* c, cudaStream_t st) {
+int enqueue_residual_norms(ats_cloth* c, cudaStream_t st, const int* active) {
     GradArgs a;
+    a.active = active;
     a.x = c->x.p;
     a.x0 = c->x0.p;
     a.vel = c->vel.p;
@@ -588,14 +600,23 @@ int frame_to_residual_impl(ats_cloth* c, double tol, const double* tols, int che
                                                   1, 0, max_iterations, tol, dtols);
         ATS_CUDA(cudaGetLastError());
         if (after_predict && (r = after_predict(st))) return r;
+        // probes (residual + deactivation) run on the device every check_every
+        // iterations; the host looks at the number of active instances only every
+        // kProbesPerSync probes, so it rarely waits on the device
+        constexpr int kProbesPerSync = 4;
+        int probes = 0;
         for (int done = 0; done < max_iterations;) {
-            ATS_CUDA(cudaMemcpyAsync(c->host_flag, c->n_active.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-            ATS_CUDA(cudaStreamSynchronize(st));
-            if (*c->host_flag == 0) break;
+            if (probes % kProbesPerSync == 0) {
+                ATS_CUDA(cudaMemcpyAsync(c->host_flag, c->n_active.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+                ATS_CUDA(cudaStreamSynchronize(st));
+                if (*c->host_flag == 0) break;
+            }
             const int step = std::min(check_every, max_iterations - done);
-            if ((r = enqueue_iterations(c, ATS_SOLVER_VBD, step, st, c->active.p)) || (r = enqueue_residual_norms(c, st)))
+            if ((r = enqueue_iterations(c, ATS_SOLVER_VBD, step, st, c->active.p)) ||
+                (r = enqueue_residual_norms(c, st, c->active.p)))
                 return r;
             done += step;
+            ++probes;
             residual_check_kernel<<<1, 256, 0, st>>>(c->red_out.p, c->norm0.p, c->active.p, c->iters.p, c->n_active.p,
                                                       ni, 0, step, max_iterations, tol, dtols);
             ATS_CUDA(cudaGetLastError());
@@ -774,6 +795,20 @@ int ats_set_state(ats_cloth* c, const float* x, const float* v, ats_stream strea
     if (v) ATS_CUDA(cudaMemcpyAsync(c->io_v.p, v, 12 * (size_t)n, cudaMemcpyHostToDevice, st));
     scatter_state_kernel<<<(n + 255) / 256, 256, 0, st>>>(c->io_x.p, c->io_v.p, c->to_caller.p, c->x.p, c->x0.p,
                                                           c->vel.p, n, v ? 1 : 0);
+    ATS_CUDA(cudaGetLastError());
+    ATS_CUDA(cudaStreamSynchronize(st));
+    return ATS_OK;
+}
+
+int ats_set_positions(ats_cloth* c, const float* x, ats_stream stream) {
+    if (!c || !x) {
+        set_error("ats_set_positions: need a handle and positions");
+        return ATS_ERR_INVALID;
+    }
+    cudaStream_t st = S(stream);
+    const int n = c->L.nv;
+    ATS_CUDA(cudaMemcpyAsync(c->io_x.p, x, 12 * (size_t)n, cudaMemcpyHostToDevice, st));
+    scatter_positions_kernel<<<(n + 255) / 256, 256, 0, st>>>(c->io_x.p, c->to_caller.p, c->x.p, n);
     ATS_CUDA(cudaGetLastError());
     ATS_CUDA(cudaStreamSynchronize(st));
     return ATS_OK;

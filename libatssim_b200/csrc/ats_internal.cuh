@@ -77,6 +77,9 @@ struct ats_cloth {
     DevBuf<float4> y_buf;
     DevBuf<double> pot_partial, pot_y, pot_guess;
     DevBuf<int> guess_used;
+    cudaGraphExec_t warm_graph = nullptr;  // captured warm-started frame (ats_frame_warm)
+    const void* warm_key_mlp = nullptr;
+    int warm_key_iters = -1, warm_key_fallback = -1;
     cudaStream_t capture_stream = nullptr;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
 
@@ -86,6 +89,10 @@ struct ats_cloth {
                 cudaGraphExecDestroy(g);
                 g = nullptr;
             }
+        if (warm_graph) {
+            cudaGraphExecDestroy(warm_graph);
+            warm_graph = nullptr;
+        }
     }
     ~ats_cloth() {
         drop_graphs();
@@ -111,8 +118,9 @@ int launch_predict(ats_cloth* c, cudaStream_t st);
 int launch_update(ats_cloth* c, cudaStream_t st);
 int launch_sweep(ats_cloth* c, int color, cudaStream_t st, const int* active = nullptr);
 int enqueue_iterations(ats_cloth* c, int solver, int iterations, cudaStream_t st, const int* active = nullptr);
-// FP64 ||grad G|| per instance into c->red_out.p
-int enqueue_residual_norms(ats_cloth* c, cudaStream_t st);
+// FP64 ||grad G|| per instance into c->red_out.p; with `active`, instances whose flag
+// is 0 keep the per-vertex values of the previous call (their positions are frozen)
+int enqueue_residual_norms(ats_cloth* c, cudaStream_t st, const int* active = nullptr);
 // ats_frame_to_residual with an optional hook run after ||grad G(y)|| is taken and
 // before the first iteration (the learned warm start replaces y there).
 int frame_to_residual_impl(ats_cloth* c, double tol, const double* tols, int check_every, int max_iterations,

@@ -412,6 +412,136 @@ __global__ void __launch_bounds__(kThreads) infer_samples_kernel(const float* __
                 out[(size_t)(base + i) * kOut + k] = S.nrm[kNormOutMean + k] + S.nrm[kNormOutStd + k] * S.y[i][k];
 }
 
+// Inference, one warp per 16 vertices, activations kept in registers: the FP32
+// accumulators of a 64-wide layer (8 n-tiles of m16n8) are exactly the A fragments of
+// the next layer's four k16 steps once rounded to BF16 pairs, so only the features go
+// through shared memory. Persistent CTAs keep the packed weights in shared memory.
+// Same quantisation points and the same mma order as forward(): identical outputs.
+constexpr int kWarpRows = 32;  // two m16 sub-tiles; every lane gathers one vertex's features
+struct WarpScratch {
+    __nv_bfloat16 x[kWarpRows][kInP];
+    float out[kWarpRows][4];
+};
+struct InferSmem {
+    __nv_bfloat16 w[kPacked];
+    float b[3 * kHid + kOutP];
+    float nrm[kNorm];
+    WarpScratch ws[kThreads / 32];
+};
+
+__device__ __forceinline__ uint32_t pack_f2(float lo, float hi) {
+    return pk(__float2bfloat16_rn(lo), __float2bfloat16_rn(hi));
+}
+
+// acc[nt][4] (FP32) of a 64-wide layer -> GELU -> A fragments a[ks][4] of the next layer
+__device__ __forceinline__ void hidden_epilogue(const float acc[8][4], const float* bias, int t, uint32_t a[4][4]) {
+    float h[8][4];
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+        const float b0 = bias[8 * nt + 2 * t], b1 = bias[8 * nt + 2 * t + 1];
+        h[nt][0] = gelu(acc[nt][0] + b0);
+        h[nt][1] = gelu(acc[nt][1] + b1);
+        h[nt][2] = gelu(acc[nt][2] + b0);
+        h[nt][3] = gelu(acc[nt][3] + b1);
+    }
+#pragma unroll
+    for (int ks = 0; ks < 4; ++ks) {
+        a[ks][0] = pack_f2(h[2 * ks][0], h[2 * ks][1]);
+        a[ks][1] = pack_f2(h[2 * ks][2], h[2 * ks][3]);
+        a[ks][2] = pack_f2(h[2 * ks + 1][0], h[2 * ks + 1][1]);
+        a[ks][3] = pack_f2(h[2 * ks + 1][2], h[2 * ks + 1][3]);
+    }
+}
+
+template <int KS, int NT>
+__device__ __forceinline__ void warp_layer(const uint32_t a[][4], const __nv_bfloat16* W, int K, int g, int t,
+                                           float acc[][4]) {
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt) {
+        acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
+        const __nv_bfloat16* wr = W + (8 * nt + g) * K + 2 * t;
+#pragma unroll
+        for (int ks = 0; ks < KS; ++ks) {
+            const uint32_t b0 = *reinterpret_cast<const uint32_t*>(wr + 16 * ks);
+            const uint32_t b1 = *reinterpret_cast<const uint32_t*>(wr + 16 * ks + 8);
+            mma16816(acc[nt], a[ks][0], a[ks][1], a[ks][2], a[ks][3], b0, b1);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) infer_warp_kernel(FeatArgs fa, const __nv_bfloat16* __restrict__ wpack,
+                                                              const float* __restrict__ master,
+                                                              const float* __restrict__ nrm, float4* __restrict__ x,
+                                                              float s) {
+    __shared__ __align__(16) InferSmem S;
+    for (int i = threadIdx.x; i < kNorm; i += kThreads) S.nrm[i] = nrm[i];
+    for (int i = threadIdx.x; i < kPacked / 2; i += kThreads)
+        reinterpret_cast<uint32_t*>(S.w)[i] = reinterpret_cast<const uint32_t*>(wpack)[i];
+    for (int i = threadIdx.x; i < kHid; i += kThreads) {
+        S.b[i] = master[kB1 + i];
+        S.b[kHid + i] = master[kB2 + i];
+        S.b[2 * kHid + i] = master[kB3 + i];
+    }
+    for (int i = threadIdx.x; i < kOutP; i += kThreads) S.b[3 * kHid + i] = i < kOut ? master[kB4 + i] : 0.f;
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    WarpScratch& W = S.ws[warp];
+    const int ntiles = (fa.nv + kWarpRows - 1) / kWarpRows;
+    for (int tile = blockIdx.x * (kThreads / 32) + warp; tile < ntiles; tile += gridDim.x * (kThreads / 32)) {
+        const int v0 = tile * kWarpRows;
+        if (lane < kWarpRows) {
+            const int v = v0 + lane;
+            float f[kIn];
+            if (v < fa.nv) vertex_features(fa, v, f);
+            for (int k = 0; k < kInP; ++k)
+                W.x[lane][k] = __float2bfloat16_rn(
+                    v < fa.nv && k < kIn ? (f[k] - S.nrm[kNormInMean + k]) * S.nrm[kNormInScale + k] : 0.f);
+        }
+        __syncwarp();
+#pragma unroll 1
+        for (int half = 0; half < 2; ++half) {
+            const int r0 = 16 * half;
+            uint32_t a1[2][4];
+#pragma unroll
+            for (int ks = 0; ks < 2; ++ks) {
+                a1[ks][0] = *reinterpret_cast<const uint32_t*>(&W.x[r0 + g][16 * ks + 2 * t]);
+                a1[ks][1] = *reinterpret_cast<const uint32_t*>(&W.x[r0 + g + 8][16 * ks + 2 * t]);
+                a1[ks][2] = *reinterpret_cast<const uint32_t*>(&W.x[r0 + g][16 * ks + 2 * t + 8]);
+                a1[ks][3] = *reinterpret_cast<const uint32_t*>(&W.x[r0 + g + 8][16 * ks + 2 * t + 8]);
+            }
+            float acc[8][4];
+            uint32_t a[4][4];
+            warp_layer<2, 8>(a1, S.w + kP1, kInP, g, t, acc);
+            hidden_epilogue(acc, S.b, t, a);
+            warp_layer<4, 8>(a, S.w + kP2, kHid, g, t, acc);
+            hidden_epilogue(acc, S.b + kHid, t, a);
+            warp_layer<4, 8>(a, S.w + kP3, kHid, g, t, acc);
+            hidden_epilogue(acc, S.b + 2 * kHid, t, a);
+            float o[1][4];
+            warp_layer<4, 1>(a, S.w + kP4, kHid, g, t, o);  // output columns 0..7 (0..2 used)
+            if (t < 2) {
+                const float* b4 = S.b + 3 * kHid;
+                W.out[r0 + g][2 * t] = o[0][0] + b4[2 * t];
+                W.out[r0 + g][2 * t + 1] = o[0][1] + b4[2 * t + 1];
+                W.out[r0 + g + 8][2 * t] = o[0][2] + b4[2 * t];
+                W.out[r0 + g + 8][2 * t + 1] = o[0][3] + b4[2 * t + 1];
+            }
+        }
+        __syncwarp();
+        if (lane < kWarpRows) {
+            const int v = v0 + lane;
+            if (v < fa.nv && fa.vm[v].y == 0.f) {
+                float4 p = x[v];
+                p.x += s * (S.nrm[kNormOutMean + 0] + S.nrm[kNormOutStd + 0] * W.out[lane][0]);
+                p.y += s * (S.nrm[kNormOutMean + 1] + S.nrm[kNormOutStd + 1] * W.out[lane][1]);
+                p.z += s * (S.nrm[kNormOutMean + 2] + S.nrm[kNormOutStd + 2] * W.out[lane][2]);
+                x[v] = p;
+            }
+        }
+        __syncwarp();
+    }
+}
+
 __global__ void copy4_kernel(const float4* __restrict__ src, float4* __restrict__ dst, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) dst[i] = src[i];
@@ -449,57 +579,79 @@ struct PotArgs {
     const float* kb;
     const int* bseg;
     double h;
-    double* partial;  // ninst * kPotChunks
+    double* partial;  // 2 * ninst * kPotChunks
 };
 
-// G(x) = sum m/(2h^2)|x - y|^2 + sum 1/2 k (l - L)^2 + sum 1/2 k_b x^T Q x over one instance
+// Per instance, in one pass over the geometry: G(x) (inertia + springs + bending) and
+// G(y) (springs + bending; its inertia term is 0), y the inertial prediction,
+// G(z) = sum m/(2h^2)|z - y|^2 + sum 1/2 k (l - L)^2 + sum 1/2 k_b z^T Q z.
+__device__ __forceinline__ double spring_energy(float4 p0, float4 p1, float L, float k) {
+    const double dx = (double)p1.x - p0.x, dy = (double)p1.y - p0.y, dz = (double)p1.z - p0.z;
+    const double C = sqrt(dx * dx + dy * dy + dz * dz) - (double)L;
+    return 0.5 * (double)k * C * C;
+}
+__device__ __forceinline__ double bending_energy(const float4* pos, int4 id, const float* Q, float kb) {
+    const int vid[4] = {id.x, id.y, id.z, id.w};
+    double p[4][3];
+    for (int k = 0; k < 4; ++k) {
+        const float4 t = pos[vid[k]];
+        p[k][0] = t.x;
+        p[k][1] = t.y;
+        p[k][2] = t.z;
+    }
+    double s = 0.0;
+    for (int c = 0; c < 4; ++c)
+        for (int r = 0; r < 4; ++r) s += (double)Q[4 * c + r] * (p[c][0] * p[r][0] + p[c][1] * p[r][1] + p[c][2] * p[r][2]);
+    return 0.5 * (double)kb * s;
+}
+
 __global__ void __launch_bounds__(256) potential_kernel(PotArgs a) {
-    __shared__ double sh[256];
+    __shared__ double shx[256], shy[256];
     const int i = blockIdx.y, j = blockIdx.x, stride = kPotChunks * 256;
-    double acc = 0.0;
+    double gx = 0.0, gy = 0.0;
     for (int v = a.vseg[i] + j * 256 + threadIdx.x; v < a.vseg[i + 1]; v += stride) {
         const float4 p = a.x[v], q = a.y[v];
         const double dx = (double)p.x - q.x, dy = (double)p.y - q.y, dz = (double)p.z - q.z;
-        acc += (double)a.x0[v].w / (2.0 * a.h * a.h) * (dx * dx + dy * dy + dz * dz);
+        gx += (double)a.x0[v].w / (2.0 * a.h * a.h) * (dx * dx + dy * dy + dz * dz);
     }
     for (int e = a.eseg[i] + j * 256 + threadIdx.x; e < a.eseg[i + 1]; e += stride) {
         const int2 ed = a.edge[e];
-        const float4 p0 = a.x[ed.x], p1 = a.x[ed.y];
-        const double dx = (double)p1.x - p0.x, dy = (double)p1.y - p0.y, dz = (double)p1.z - p0.z;
-        const double C = sqrt(dx * dx + dy * dy + dz * dz) - (double)a.rest[e];
-        acc += 0.5 * (double)a.kst[e] * C * C;
+        const float L = a.rest[e], k = a.kst[e];
+        gx += spring_energy(a.x[ed.x], a.x[ed.y], L, k);
+        gy += spring_energy(a.y[ed.x], a.y[ed.y], L, k);
     }
     for (int b = a.bseg[i] + j * 256 + threadIdx.x; b < a.bseg[i + 1]; b += stride) {
         const int4 id = a.bend[b];
-        const int vid[4] = {id.x, id.y, id.z, id.w};
-        double p[4][3];
-        for (int k = 0; k < 4; ++k) {
-            const float4 t = a.x[vid[k]];
-            p[k][0] = t.x;
-            p[k][1] = t.y;
-            p[k][2] = t.z;
-        }
         const float* Q = a.q16 + 16 * (size_t)b;
-        double s = 0.0;
-        for (int c = 0; c < 4; ++c)
-            for (int r = 0; r < 4; ++r) s += (double)Q[4 * c + r] * (p[c][0] * p[r][0] + p[c][1] * p[r][1] + p[c][2] * p[r][2]);
-        acc += 0.5 * (double)a.kb[b] * s;
+        gx += bending_energy(a.x, id, Q, a.kb[b]);
+        gy += bending_energy(a.y, id, Q, a.kb[b]);
     }
-    sh[threadIdx.x] = acc;
+    shx[threadIdx.x] = gx;
+    shy[threadIdx.x] = gy;
     __syncthreads();
     for (int s = 128; s > 0; s >>= 1) {
-        if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+        if (threadIdx.x < s) {
+            shx[threadIdx.x] += shx[threadIdx.x + s];
+            shy[threadIdx.x] += shy[threadIdx.x + s];
+        }
         __syncthreads();
     }
-    if (threadIdx.x == 0) a.partial[i * kPotChunks + j] = sh[0];
+    if (threadIdx.x == 0) {
+        a.partial[2 * (i * kPotChunks + j)] = shx[0];
+        a.partial[2 * (i * kPotChunks + j) + 1] = shy[0];
+    }
 }
 
-__global__ void potential_final_kernel(const double* partial, double* out, int ninst) {
+__global__ void potential_final_kernel(const double* partial, double* gx, double* gy, int ninst) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= ninst) return;
-    double s = 0.0;
-    for (int j = 0; j < kPotChunks; ++j) s += partial[i * kPotChunks + j];
-    out[i] = s;
+    double sx = 0.0, sy = 0.0;
+    for (int j = 0; j < kPotChunks; ++j) {
+        sx += partial[2 * (i * kPotChunks + j)];
+        sy += partial[2 * (i * kPotChunks + j) + 1];
+    }
+    gx[i] = sx;
+    gy[i] = sy;
 }
 
 // keep the guess of an instance only if G(guess) <= G(y); otherwise restore y
@@ -600,14 +752,14 @@ FeatArgs feat_args(ats_cloth* c) {
 int ensure_learn_buffers(ats_cloth* c) {
     const size_t nv = c->L.nv;
     if (!c->y_buf.p) ATS_CUDA(c->y_buf.alloc(nv));
-    if (!c->pot_partial.p) ATS_CUDA(c->pot_partial.alloc((size_t)kPotChunks * c->L.ninst));
+    if (!c->pot_partial.p) ATS_CUDA(c->pot_partial.alloc((size_t)2 * kPotChunks * c->L.ninst));
     if (!c->pot_y.p) ATS_CUDA(c->pot_y.alloc(c->L.ninst));
     if (!c->pot_guess.p) ATS_CUDA(c->pot_guess.alloc(c->L.ninst));
     if (!c->guess_used.p) ATS_CUDA(c->guess_used.alloc(c->L.ninst));
     return ATS_OK;
 }
 
-int enqueue_potential(ats_cloth* c, double* out, cudaStream_t st) {
+int enqueue_potential(ats_cloth* c, double* gx, double* gy, cudaStream_t st) {
     PotArgs a;
     a.x = c->x.p;
     a.y = c->y_buf.p;
@@ -626,24 +778,34 @@ int enqueue_potential(ats_cloth* c, double* out, cudaStream_t st) {
     a.partial = c->pot_partial.p;
     potential_kernel<<<dim3(kPotChunks, c->L.ninst), 256, 0, st>>>(a);
     ATS_CUDA(cudaGetLastError());
-    potential_final_kernel<<<(c->L.ninst + 127) / 128, 128, 0, st>>>(c->pot_partial.p, out, c->L.ninst);
+    potential_final_kernel<<<(c->L.ninst + 127) / 128, 128, 0, st>>>(c->pot_partial.p, gx, gy, c->L.ninst);
     ATS_CUDA(cudaGetLastError());
     return ATS_OK;
 }
 
-// after predict: save y, (G(y)), x = guess, (G(guess), fallback)
+// after predict: save y, x = guess, then (G(guess), G(y) and the per-instance fallback)
 int enqueue_warm_start(ats_cloth* c, const ats_mlp* m, int fallback, cudaStream_t st) {
     int r;
     if ((r = set_smem_limits()) || (r = ensure_learn_buffers(c))) return r;
     const int nv = c->L.nv;
     copy4_kernel<<<(nv + 255) / 256, 256, 0, st>>>(c->x.p, c->y_buf.p, nv);
     ATS_CUDA(cudaGetLastError());
-    if (fallback && (r = enqueue_potential(c, c->pot_y.p, st))) return r;
-    infer_kernel<<<(nv + kTile - 1) / kTile, kThreads, kTileSmem, st>>>(feat_args(c), m->wpack.p, m->master.p, m->nrm.p,
-                                                                          c->x.p, 9.8f * c->h * c->h);
+    {
+        static int sm_count = 0;
+        if (!sm_count) {
+            int dev = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, dev);
+            if (sm_count <= 0) sm_count = 148;
+        }
+        const int tiles = (nv + kWarpRows - 1) / kWarpRows;
+        const int grid = std::max(1, std::min((tiles + 3) / 4, sm_count * 8));
+        infer_warp_kernel<<<grid, kThreads, 0, st>>>(feat_args(c), m->wpack.p, m->master.p, m->nrm.p, c->x.p,
+                                                     9.8f * c->h * c->h);
+    }
     ATS_CUDA(cudaGetLastError());
     if (fallback) {
-        if ((r = enqueue_potential(c, c->pot_guess.p, st))) return r;
+        if ((r = enqueue_potential(c, c->pot_guess.p, c->pot_y.p, st))) return r;
         const int n = std::max(nv, c->L.ninst);
         fallback_kernel<<<(n + 255) / 256, 256, 0, st>>>(c->x.p, c->y_buf.p, c->vm.p, c->pot_y.p, c->pot_guess.p,
                                                           c->guess_used.p, nv, c->L.ninst);
@@ -982,18 +1144,54 @@ int ats_warm_start(ats_cloth* c, const ats_mlp* m, int fallback, int* used, ats_
     return ATS_OK;
 }
 
-int ats_frame_warm(ats_cloth* c, const ats_mlp* m, int fallback, ats_stream stream) {
+int ats_frame_warm(ats_cloth* c, const ats_mlp* m, int fallback, int iterations, int use_graph, ats_stream stream) {
     if (!c || !m) {
         set_error("ats_frame_warm: need a handle and a model");
         return ATS_ERR_INVALID;
     }
-    cudaStream_t st = S(stream);
+    const int iters = iterations < 0 ? c->prm.iterations : iterations;
+    auto enqueue = [&](cudaStream_t st) {
+        int r;
+        for (int sub = 0; sub < c->prm.num_substep; ++sub) {
+            if ((r = launch_predict(c, st)) || (r = enqueue_warm_start(c, m, fallback, st)) ||
+                (r = enqueue_iterations(c, ATS_SOLVER_VBD, iters, st)) || (r = launch_update(c, st)))
+                return r;
+        }
+        return (int)ATS_OK;
+    };
+    if (!use_graph) return enqueue(S(stream));
     int r;
-    for (int sub = 0; sub < c->prm.num_substep; ++sub) {
-        if ((r = launch_predict(c, st)) || (r = enqueue_warm_start(c, m, fallback, st)) ||
-            (r = enqueue_iterations(c, ATS_SOLVER_VBD, c->prm.iterations, st)) || (r = launch_update(c, st)))
+    if ((r = set_smem_limits()) || (r = ensure_learn_buffers(c))) return r;
+    // one captured warm frame per handle, re-captured when model, budget or fallback change
+    if (!c->warm_graph || c->warm_key_mlp != (const void*)m || c->warm_key_iters != iters ||
+        c->warm_key_fallback != fallback) {
+        if (c->warm_graph) {
+            cudaGraphExecDestroy(c->warm_graph);
+            c->warm_graph = nullptr;
+        }
+        cudaGraph_t g = nullptr;
+        ATS_CUDA(cudaStreamBeginCapture(c->capture_stream, cudaStreamCaptureModeThreadLocal));
+        r = enqueue(c->capture_stream);
+        cudaError_t e = cudaStreamEndCapture(c->capture_stream, &g);
+        if (r) {
+            if (g) cudaGraphDestroy(g);
             return r;
+        }
+        if (e != cudaSuccess) {
+            set_error(std::string("ats_frame_warm: capture failed: ") + cudaGetErrorString(e));
+            return ATS_ERR_CUDA;
+        }
+        e = cudaGraphInstantiate(&c->warm_graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            set_error(std::string("ats_frame_warm: instantiate failed: ") + cudaGetErrorString(e));
+            return ATS_ERR_CUDA;
+        }
+        c->warm_key_mlp = m;
+        c->warm_key_iters = iters;
+        c->warm_key_fallback = fallback;
     }
+    ATS_CUDA(cudaGraphLaunch(c->warm_graph, S(stream)));
     return ATS_OK;
 }
 

@@ -163,3 +163,44 @@ def test_learned_warm_start_reaches_plain_residual_in_fewer_iterations(ats):
     needed = np.array(needed)
     # the learned guess reaches the plain 100-iteration residual in fewer iterations
     assert np.median(needed) < iters, needed
+
+
+def test_warp_tiled_inference_equals_tile_forward(ats):
+    """The frame's inference kernel (register-resident activations, one warp per 16
+    vertices) against ats_mlp_infer (the shared-memory tile forward checked against
+    the oracle): same BF16 rounding points and mma order, so the same guess."""
+    inst = configs.grid_instance(40)
+    cloth = ats.Cloth([inst], implicit_dt=1.0 / 60.0, num_substep=1, iterations=10, damping=2.0)
+    for _ in range(4):
+        cloth.frame()
+    m = ats.MLP(seed=5)
+    m.set_normalization(_norm_vector(np.random.RandomState(2)))
+    ds = ats.Dataset(inst.num_verts)
+    cloth.predict()
+    y = cloth.positions()
+    cloth.record_begin()
+    cloth.record_end(ds)  # features of the free vertices at this frame start
+    f, _ = ds.read()
+    cloth.warm_start(m, fallback=False)
+    guess = cloth.positions()
+    free = np.nonzero(inst.fixed == 0)[0]
+    order = cloth.vertex_order()
+    rows = np.argsort(order)[np.sort(order[free])]
+    s = 9.8 / 3600.0
+    expect = y[rows] + np.float32(s) * m.infer(f)
+    assert np.allclose(guess[rows], expect, rtol=0, atol=1e-7)
+    pinned = inst.fixed.astype(bool)
+    assert np.array_equal(guess[pinned], y[pinned])
+
+
+def test_warm_frame_graph_equals_eager(ats):
+    insts, prm = configs.c2(num_instances=3, seed=4, side_range=(12, 24))
+    a = ats.Cloth(insts, **prm)
+    b = ats.Cloth(insts, **prm)
+    m = ats.MLP(seed=6)
+    for _ in range(3):
+        a.frame_warm(m, fallback=True, iterations=7, graph=True)
+        b.frame_warm(m, fallback=True, iterations=7, graph=False)
+    xa, va = a.state()
+    xb, vb = b.state()
+    assert np.array_equal(xa, xb) and np.array_equal(va, vb)
