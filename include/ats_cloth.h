@@ -116,6 +116,16 @@ int ats_mass_area_weighted(const float* positions, int num_verts, const int* fac
  * null arrays first to get the counts. */
 int ats_obj_read(const char* path, int* num_verts, float* positions, int* num_faces, int* faces);
 
+/* Writes positions and triangles as an OBJ file ("v x y z", 1-based "f a b c"), as
+ * src/Utils/mesh_reader.cpp:374-462 exports a simulated frame. */
+int ats_obj_write(const char* path, const float* positions, int num_verts, const int* faces, int num_faces);
+/* Cloth state (x, v, 3 floats per vertex) as a versioned little-endian file with an
+ * FNV-1a checksum, for checkpoint / resume (replaces the raw dumps of
+ * src/Utils/mesh_reader.h:323-343). Read with null x / v to get num_verts and frame;
+ * otherwise *num_verts is the capacity on input and the count on output. */
+int ats_state_write(const char* path, const float* x, const float* v, int num_verts, int frame);
+int ats_state_read(const char* path, float* x, float* v, int* num_verts, int* frame);
+
 /* ---------------------------------------------------------------- topology (host only)
  * Replaces SimMesh::extract_edges_from_surface (src/Utils/mesh_reader.h:206-298), the
  * adjacency set-up and greedy colourings of examples/example2_async_iter.cpp:229-304,
@@ -275,6 +285,12 @@ int ats_dataset_read(const ats_dataset* data, long long first, long long count, 
  * ats_record_frame_end before ats_update_velocity (target (x - y)/s of every free vertex). */
 int ats_record_frame_begin(ats_cloth* cloth, ats_stream stream);
 int ats_record_frame_end(ats_cloth* cloth, ats_dataset* data, ats_stream stream);
+/* Data-parallel training pieces: the gradient of one batch drawn from `data` (host
+ * output, parameters unchanged), and one Adam step with a given gradient (for a
+ * gradient averaged over ranks). Both synchronise `stream`. */
+int ats_mlp_batch_gradient(ats_mlp* mlp, const ats_dataset* data, int batch, unsigned long long seed, float* grad,
+                           float* loss, ats_stream stream);
+int ats_mlp_apply_gradient(ats_mlp* mlp, const float* grad, float lr, ats_stream stream);
 /* `steps` Adam steps on batches of `batch` samples drawn from `data` (seeded);
  * mean_loss (nullable) = mean loss of the last 20 steps. Synchronises `stream`. */
 int ats_mlp_train(ats_mlp* mlp, const ats_dataset* data, int steps, int batch, float lr, unsigned long long seed,

@@ -183,6 +183,13 @@ public:
 
     // Depth-first topological order; false (and an empty order) if the graph has a cycle.
     bool topological_sort();
+    // Measured costs: `repeats` launches of one representative task per distinct
+    // (function id, cluster) on every processor 0..nprocs-1 that implements it, each
+    // followed by the device drain, host-timed in milliseconds; processors without an
+    // implementation get `inf`. The result feeds profile_from (the reference refits
+    // its matrix from command-buffer timestamps, launcher.cpp:711-793).
+    void profile_costs(const std::function<LaunchParam(const Task&)>& task_to_param, int repeats, uint nprocs,
+                       std::vector<std::pair<FunctionID, uint>>& keys, std::vector<std::vector<double>>& costs);
     // Costs per (function id, cluster) -> per-processor cost (launcher.cpp:645-704).
     void profile_from(const std::vector<std::pair<FunctionID, uint>>& map_tasks,
                       const std::vector<std::vector<double>>& map_costs, std::vector<double>& cost_total);

@@ -82,6 +82,9 @@ _SIGNATURES = {
     "ats_reference_pins": [_fp, ctypes.c_int, _u8p],
     "ats_mass_area_weighted": [_fp, ctypes.c_int, _ip, ctypes.c_int, ctypes.c_float, _fp],
     "ats_obj_read": [ctypes.c_char_p, _ip, _fp, _ip, _ip],
+    "ats_obj_write": [ctypes.c_char_p, _fp, ctypes.c_int, _ip, ctypes.c_int],
+    "ats_state_write": [ctypes.c_char_p, _fp, _fp, ctypes.c_int, ctypes.c_int],
+    "ats_state_read": [ctypes.c_char_p, _fp, _fp, _ip, _ip],
     "ats_topology_build": [ctypes.POINTER(InstanceDesc), ctypes.POINTER(_vp)],
     "ats_topology_destroy": [_vp],
     "ats_topology_counts": [_vp, _ip],
@@ -119,6 +122,8 @@ _SIGNATURES = {
     "ats_mlp_set_normalization": [_vp, _fp],
     "ats_mlp_fit_normalization": [_vp, _vp, _vp],
     "ats_mlp_gradient": [_vp, _fp, _fp, ctypes.c_int, _fp, _fp, _vp],
+    "ats_mlp_batch_gradient": [_vp, _vp, ctypes.c_int, ctypes.c_ulonglong, _fp, _fp, _vp],
+    "ats_mlp_apply_gradient": [_vp, _fp, ctypes.c_float, _vp],
     "ats_dataset_create": [ctypes.c_longlong, ctypes.POINTER(_vp)],
     "ats_dataset_destroy": [_vp],
     "ats_dataset_size": [_vp, ctypes.POINTER(ctypes.c_longlong)],
@@ -217,6 +222,29 @@ def obj_read(path):
     _check(lib().ats_obj_read(path.encode(), ctypes.byref(nv), _p(pos, ctypes.c_float), ctypes.byref(nf),
                               _p(faces, ctypes.c_int)))
     return pos, faces
+
+
+def obj_write(path, positions, faces):
+    pos = np.ascontiguousarray(positions, dtype=np.float32)
+    f = np.ascontiguousarray(faces, dtype=np.int32)
+    _check(lib().ats_obj_write(path.encode(), _p(pos, ctypes.c_float), pos.shape[0], _p(f, ctypes.c_int), f.shape[0]))
+
+
+def state_write(path, x, v, frame=0):
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    v = np.ascontiguousarray(v, dtype=np.float32)
+    _check(lib().ats_state_write(path.encode(), _p(x, ctypes.c_float), _p(v, ctypes.c_float), x.shape[0], int(frame)))
+
+
+def state_read(path):
+    """-> (x, v, frame)"""
+    n, fr = ctypes.c_int(0), ctypes.c_int(0)
+    _check(lib().ats_state_read(path.encode(), None, None, ctypes.byref(n), ctypes.byref(fr)))
+    x = np.zeros((n.value, 3), dtype=np.float32)
+    v = np.zeros((n.value, 3), dtype=np.float32)
+    _check(lib().ats_state_read(path.encode(), _p(x, ctypes.c_float), _p(v, ctypes.c_float), ctypes.byref(n),
+                                ctypes.byref(fr)))
+    return x, v, fr.value
 
 
 class Instance:
@@ -491,6 +519,17 @@ class MLP:
         _check(lib().ats_mlp_gradient(self.h, _p(f, ctypes.c_float), _p(t, ctypes.c_float), f.shape[0],
                                       _p(g, ctypes.c_float), ctypes.byref(loss), _stream(stream)))
         return float(loss.value), g
+
+    def batch_gradient(self, dataset, batch=4096, seed=0, stream=None):
+        g = np.zeros(self.nparams, dtype=np.float32)
+        loss = ctypes.c_float(0.0)
+        _check(lib().ats_mlp_batch_gradient(self.h, dataset.h, int(batch), int(seed), _p(g, ctypes.c_float),
+                                            ctypes.byref(loss), _stream(stream)))
+        return float(loss.value), g
+
+    def apply_gradient(self, grad, lr=1e-3, stream=None):
+        g = np.ascontiguousarray(grad, dtype=np.float32)
+        _check(lib().ats_mlp_apply_gradient(self.h, _p(g, ctypes.c_float), float(lr), _stream(stream)))
 
     def train(self, dataset, steps, batch=4096, lr=1e-3, seed=0, stream=None):
         loss = ctypes.c_float(0.0)

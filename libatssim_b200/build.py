@@ -24,7 +24,7 @@ NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-r
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-I/usr/local/cuda/include"]
 
 CU_SOURCES = ["ats_cloth.cu", "ats_learn.cu", "ats_noalloc.cu"]
-CXX_SOURCES = ["ats_topology.cpp", "ats_launcher.cpp"]
+CXX_SOURCES = ["ats_topology.cpp", "ats_launcher.cpp", "ats_io.cpp"]
 
 
 def _run(cmd):

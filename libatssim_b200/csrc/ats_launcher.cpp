@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstdio>
 #include <functional>
 #include <stack>
@@ -172,6 +173,36 @@ void Scheduler::profile_from(const std::vector<std::pair<FunctionID, uint>>& map
     }
     if (cost_total.empty()) cost_total = sum;
     summary_of_costs_each_device = cost_total;
+}
+
+void Scheduler::profile_costs(const std::function<LaunchParam(const Task&)>& task_to_param, int repeats, uint nprocs,
+                              std::vector<std::pair<FunctionID, uint>>& keys, std::vector<std::vector<double>>& costs) {
+    keys.clear();
+    costs.clear();
+    std::map<std::pair<uint, uint>, uint> seen;  // (func, cluster) -> representative task
+    for (uint t = 0; t < list_task.size(); ++t) {
+        const auto key = std::make_pair((uint)list_task[t].func_id, list_task[t].cluster_idx);
+        if (!seen.count(key)) seen[key] = t;
+    }
+    for (const auto& kv : seen) {
+        const Task& task = list_task[kv.second];
+        std::vector<double> row(nprocs, (double)inf);
+        for (uint p = 0; p < nprocs; ++p) {
+            bool found = false;
+            const Implementation& imp = task.get_implementation(p, found);
+            if (!found) continue;
+            drain(p);
+            imp.launch_task(task_to_param(task));  // warm-up
+            drain(p);
+            const auto t0 = std::chrono::steady_clock::now();
+            for (int r = 0; r < repeats; ++r) imp.launch_task(task_to_param(task));
+            drain(p);
+            const auto t1 = std::chrono::steady_clock::now();
+            row[p] = std::chrono::duration<double, std::milli>(t1 - t0).count() / std::max(1, repeats);
+        }
+        keys.push_back({task.func_id, task.cluster_idx});
+        costs.push_back(row);
+    }
 }
 
 void Scheduler::standardizing_dag(const std::vector<std::function<void(const LaunchParam&)>>& empty_fns) {

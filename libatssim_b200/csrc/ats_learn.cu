@@ -1095,6 +1095,50 @@ int ats_mlp_train(ats_mlp* m, const ats_dataset* d, int steps, int batch, float 
     return ATS_OK;
 }
 
+int ats_mlp_batch_gradient(ats_mlp* m, const ats_dataset* d, int batch, unsigned long long seed, float* grad,
+                           float* loss, ats_stream stream) {
+    if (!m || !d || batch <= 0 || d->size <= 0 || !grad) {
+        set_error("ats_mlp_batch_gradient: need a model, a non-empty dataset, batch > 0 and a gradient output");
+        return ATS_ERR_INVALID;
+    }
+    int r;
+    const int ctas = (batch + kTile - 1) / kTile;
+    if ((r = set_smem_limits()) || (r = ensure_partials(m, ctas))) return r;
+    cudaStream_t st = S(stream);
+    train_tile_kernel<<<ctas, kThreads, kTileSmem, st>>>(d->feat.p, d->targ.p, d->size, batch, 1,
+                                                          seed * 0x9E3779B97F4A7C15ull + 0x5851F42D4C957F2Dull,
+                                                          m->wpack.p, m->master.p, m->nrm.p, m->partial.p,
+                                                          m->loss_partial.p);
+    ATS_CUDA(cudaGetLastError());
+    reduce_adam_kernel<<<(kParams + 255) / 256, 256, 0, st>>>(m->partial.p, ctas, m->master.p, m->m1.p, m->m2.p,
+                                                              m->grad.p, m->wpack.p, 0.f, 0.9f, 0.999f, 1e-8f, 1, 0);
+    ATS_CUDA(cudaGetLastError());
+    sum_loss_kernel<<<1, 32, 0, st>>>(m->loss_partial.p, ctas, m->loss.p);
+    ATS_CUDA(cudaMemcpyAsync(grad, m->grad.p, kParams * sizeof(float), cudaMemcpyDeviceToHost, st));
+    float l = 0.f;
+    ATS_CUDA(cudaMemcpyAsync(&l, m->loss.p, sizeof(float), cudaMemcpyDeviceToHost, st));
+    ATS_CUDA(cudaStreamSynchronize(st));
+    if (loss) *loss = l / (float)(batch * kOut);
+    return ATS_OK;
+}
+
+int ats_mlp_apply_gradient(ats_mlp* m, const float* grad, float lr, ats_stream stream) {
+    if (!m || !grad) {
+        set_error("ats_mlp_apply_gradient: need a model and a gradient");
+        return ATS_ERR_INVALID;
+    }
+    int r = ensure_partials(m, 1);
+    if (r) return r;
+    cudaStream_t st = S(stream);
+    ATS_CUDA(cudaMemcpyAsync(m->partial.p, grad, kParams * sizeof(float), cudaMemcpyHostToDevice, st));
+    ++m->step;
+    reduce_adam_kernel<<<(kParams + 255) / 256, 256, 0, st>>>(m->partial.p, 1, m->master.p, m->m1.p, m->m2.p, nullptr,
+                                                              m->wpack.p, lr, 0.9f, 0.999f, 1e-8f, m->step, 1);
+    ATS_CUDA(cudaGetLastError());
+    ATS_CUDA(cudaStreamSynchronize(st));
+    return ATS_OK;
+}
+
 int ats_mlp_gradient(ats_mlp* m, const float* features, const float* targets, int n, float* grad, float* loss,
                      ats_stream stream) {
     if (!m || !features || !targets || n <= 0 || !grad) {

@@ -5,7 +5,8 @@
 // scheduler in the requested mode and the same frames through ats_frame on a second
 // handle, and prints the largest position difference as JSON (0 = bit-identical).
 //
-// usage: vbd_dag <grid n> <iterations> <frames> <mode: gpu | hetero | fake>
+// usage: vbd_dag <grid n> <iterations> <frames> <mode: gpu | hetero | fake | profiled>
+// (profiled: costs measured with Scheduler::profile_costs, then the Hetero launch)
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -83,12 +84,33 @@ int main(int argc, char** argv) {
     for (unsigned t : per_iter.back()) s.set_connect(t, t_last);
     s.set_connect(t_last, t_update);
 
-    // computation matrix: the GPU is ten times faster, as a profiled B200 would be
-    std::vector<std::pair<Launcher::FunctionID, unsigned>> keys = {{Launcher::id_xpbd_predict_position, 0},
-                                                                   {Launcher::id_xpbd_update_velocity, 0},
-                                                                   {Launcher::id_xpbd_constraint_last_node, 0}};
-    for (unsigned c = 0; c < ncol; ++c) keys.push_back({Launcher::id_vbd_all_in_one, c});
-    std::vector<std::vector<double>> costs(keys.size(), std::vector<double>{1.0, 0.1});
+    auto to_param = [](const Launcher::Task& t) {
+        Launcher::LaunchParam p;
+        p.function_id = t.func_id;
+        p.iter_idx = t.iter_idx;
+        p.cluster_idx = t.cluster_idx;
+        p.is_allocated_to_main_device = t.is_allocated_to_main_device;
+        return p;
+    };
+    std::vector<std::pair<Launcher::FunctionID, unsigned>> keys;
+    std::vector<std::vector<double>> costs;
+    if (!std::strcmp(mode, "profiled")) {
+        // measured costs on this B200 (host implementation = device work + wait)
+        s.profile_costs(to_param, 5, 2, keys, costs);
+        check(ats_set_state(a, pos.data(), nullptr, nullptr), "restore");
+        std::printf("{\"profiled\": [");
+        for (size_t i = 0; i < keys.size(); ++i)
+            std::printf("%s[\"%s\", %u, %.5f, %.5f]", i ? ", " : "", Launcher::taskNames.at(keys[i].first).c_str(),
+                        keys[i].second, costs[i][0], costs[i][1]);
+        std::printf("]}\n");
+    } else {
+        // computation matrix: the GPU is ten times faster, as a profiled B200 would be
+        keys = {{Launcher::id_xpbd_predict_position, 0},
+                {Launcher::id_xpbd_update_velocity, 0},
+                {Launcher::id_xpbd_constraint_last_node, 0}};
+        for (unsigned c = 0; c < ncol; ++c) keys.push_back({Launcher::id_vbd_all_in_one, c});
+        costs.assign(keys.size(), std::vector<double>{1.0, 0.1});
+    }
     std::vector<double> total;
     s.profile_from(keys, costs, total);
     s.communication_cost_matrix_uma = {{0.0f, 0.1f}, {0.1f, 0.0f}};
@@ -100,16 +122,8 @@ int main(int argc, char** argv) {
     s.make_wait_events();
 
     Launcher::Scheduler::LaunchMode m = Launcher::Scheduler::LaunchModeGpu;
-    if (!std::strcmp(mode, "hetero")) m = Launcher::Scheduler::LaunchModeHetero;
+    if (!std::strcmp(mode, "hetero") || !std::strcmp(mode, "profiled")) m = Launcher::Scheduler::LaunchModeHetero;
     if (!std::strcmp(mode, "fake")) m = Launcher::Scheduler::LaunchModeFakeHetero;
-    auto to_param = [](const Launcher::Task& t) {
-        Launcher::LaunchParam p;
-        p.function_id = t.func_id;
-        p.iter_idx = t.iter_idx;
-        p.cluster_idx = t.cluster_idx;
-        p.is_allocated_to_main_device = t.is_allocated_to_main_device;
-        return p;
-    };
     const unsigned on_gpu = s.get_proc_schedules().size() > 1 ? (unsigned)s.get_proc_schedules()[1].size() : 0u;
     for (int f = 0; f < frames; ++f) {
         s.launch(m, to_param, false);

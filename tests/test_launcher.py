@@ -51,11 +51,16 @@ def test_heft_rejects_cycles(programs):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("mode", ["gpu", "hetero", "fake"])
+@pytest.mark.parametrize("mode", ["gpu", "hetero", "fake", "profiled"])
 def test_vbd_task_graph_through_scheduler(programs, mode):
     r = subprocess.run([programs["vbd_dag"], "32", "8", "4", mode], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr
-    out = json.loads(r.stdout)
+    lines = r.stdout.strip().splitlines()
+    if mode == "profiled":
+        prof = json.loads(lines[0])["profiled"]
+        # one measured row per distinct (function id, colour); both devices implement every task
+        assert len(prof) == 3 + 4 and all(c > 0 for row in prof for c in row[2:])
+    out = json.loads(lines[-1])
     assert out["max_abs_diff"] == 0.0
     assert out["max_displacement"] > 1e-3
     # predict + 8 x 4 colours + last node + update + root + terminal, all on the B200
