@@ -204,3 +204,38 @@ def test_warm_frame_graph_equals_eager(ats):
     xa, va = a.state()
     xb, vb = b.state()
     assert np.array_equal(xa, xb) and np.array_equal(va, vb)
+
+
+def test_batch_gradient_and_adam_step(ats):
+    # a 3 x 3 grid with only the centre free records one sample per frame, so every
+    # batch drawn from the dataset holds copies of that sample
+    fixed = np.ones(9, dtype=np.uint8)
+    fixed[4] = 0
+    inst = configs.grid_instance(3, fixed=fixed)
+    cloth = ats.Cloth([inst], implicit_dt=1.0 / 60.0, num_substep=1, iterations=10, damping=2.0)
+    ds = ats.Dataset(4)
+    cloth.set_accel(np.array([[0.3, -9.8, 0.5]]))
+    cloth.predict()
+    cloth.record_begin()
+    cloth.vbd_iterations(10)
+    cloth.record_end(ds)
+    assert len(ds) == 1
+    rng = np.random.RandomState(6)
+    m = ats.MLP(seed=5)
+    m.set_normalization(_norm_vector(rng))
+    theta0 = m.params()
+    f, t = ds.read()
+    l1, g1 = m.gradient(f, t)
+    # batch 256: the output gradient 2e/(3n) differs from the single sample's by a power
+    # of two, so its BF16 rounding is the same and only FP32 summation order remains
+    lb, gb = m.batch_gradient(ds, batch=256, seed=7)
+    assert np.array_equal(m.params(), theta0)  # a gradient leaves the parameters alone
+    assert abs(lb - l1) <= 1e-5 * l1
+    assert np.linalg.norm(gb - g1) <= 1e-4 * np.linalg.norm(g1)
+    lb2, gb2 = m.batch_gradient(ds, batch=256, seed=7)
+    assert lb2 == lb and np.array_equal(gb2, gb)  # deterministic
+    # the first Adam step from zero moments moves every parameter by lr * g / (|g| + eps)
+    g = rng.standard_normal(theta0.size).astype(np.float32)
+    m.apply_gradient(g, lr=1e-3)
+    expected = theta0.astype(np.float64) - 1e-3 * g / (np.abs(g) + 1e-8)
+    assert np.max(np.abs(m.params() - expected)) < 1e-6
