@@ -219,6 +219,11 @@ int ats_energy(ats_cloth* cloth, double* out3, ats_stream stream);
  * instance, of the current iterate (grad = m/h^2 (x - y) - f_stretch - f_bending,
  * y = x0 + h v + h^2 a). Synchronises `stream`. */
 int ats_residual(ats_cloth* cloth, double* out_per_instance, ats_stream stream);
+/* FP64 incremental potential G(x) per instance of the current iterate against the
+ * current frame start: the three ats_energy terms of the instance, summed per vertex
+ * over the merged neighbour stencil (the quantity the learned warm start's fallback
+ * compares). Synchronises `stream`. */
+int ats_potential(ats_cloth* cloth, double* out_per_instance, ats_stream stream);
 
 /* FP64 energy of one cloth state given as plain device arrays, with no device
  * allocation. It has no counterpart in the reference. It is for callers that cannot

@@ -113,6 +113,7 @@ _SIGNATURES = {
     "ats_energy": [_vp, _dp, _vp],
     "ats_frame_to_residual": [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, _ip, _dp, _vp],
     "ats_residual": [_vp, _dp, _vp],
+    "ats_potential": [_vp, _dp, _vp],
     "ats_mlp_create": [ctypes.c_ulonglong, ctypes.POINTER(_vp)],
     "ats_mlp_destroy": [_vp],
     "ats_mlp_get_params": [_vp, _fp],
@@ -461,6 +462,12 @@ class Cloth:
     def residual(self, stream=None):
         out = np.zeros(self.info.num_instances, dtype=np.float64)
         _check(lib().ats_residual(self.h, _p(out, ctypes.c_double), _stream(stream)))
+        return out
+
+    def potential(self, stream=None):
+        """Per-instance FP64 incremental potential G(x) of the current iterate."""
+        out = np.zeros(self.info.num_instances, dtype=np.float64)
+        _check(lib().ats_potential(self.h, _p(out, ctypes.c_double), _stream(stream)))
         return out
 
 

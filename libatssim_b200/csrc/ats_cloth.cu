@@ -284,10 +284,26 @@ __global__ void __launch_bounds__(kRedThreads) sum_partials3_kernel(const double
     }
 }
 
-// Squared FP64 gradient of the incremental potential at every free vertex:
-// grad = m/h^2 (x - y) - f_stretch - f_bending, y = x0 + h v + h^2 a.
-struct GradArgs {
+// Per-vertex FP64 evaluation of the incremental potential
+//   G(z) = sum m/(2h^2)|z - y|^2 + sum 1/2 k (l - L)^2 + 1/2 sum_b k_b z^T Q_b z
+// over the sliced-ELL stencil of the sweep, its rows loaded up front (all stencil
+// entries, then all gathers) as in vbd_sweep_kernel:
+//   kEvalGrad     out0[v] = |grad_v G(x)|^2 at free vertices (0 when pinned), with
+//                 grad = m/h^2 (x - y) - f_stretch + sum_u W_vu (x_u - x_v),
+//                 y = x0 + h v + h^2 a;
+//   kEvalPot      out0[v] = the vertex's share of G(x): its inertia term against
+//                 y = x0 + h v + h^2 a (a = 0 at pinned vertices, as
+//                 Energy::compute_energy_inertia, xpbd_constraints.h:2079-2098), a
+//                 quarter k (l - L)^2 per incident spring (each spring is seen from both
+//                 ends) and -1/4 sum_u W_vu |x_u - x_v|^2, which sums to the bending
+//                 energy because the merged stencil W is symmetric with zero row sums
+//                 (x^T W x = -1/2 sum_{v,u} W_vu |x_u - x_v|^2);
+//   kEvalPotPair  out0[v], out1[v] = the shares of G(x) and G(y) with y the saved
+//                 inertial prediction (the inertia term of G(y) is 0).
+constexpr int kEvalGrad = 0, kEvalPot = 1, kEvalPotPair = 2;
+struct EvalArgs {
     const float4* x;
+    const float4* y;  // kEvalPotPair only
     const float4* x0;
     const float4* vel;
     const float4* vm;
@@ -296,61 +312,161 @@ struct GradArgs {
     const float* st_rest;
     const int4* slices;
     int nslices;
-    int tpv;
     double h;
-    double* g2;          // per vertex (layout order)
-    const int* active;   // per instance; null = all. Frozen instances keep their g2.
+    double* out0;
+    double* out1;
+    const int* active;  // per instance; null = all. Frozen instances keep their values.
 };
 
-__global__ void grad_kernel(GradArgs a) {
-    // one thread per (vertex, lane-group) entry: walk the slice rows of its vertex
-    const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-    const int lane = threadIdx.x & 31;
-    if (warp >= a.nslices) return;
-    const int4 sd = a.slices[warp];
-    const int k = lane / a.tpv;
-    if (k >= sd.y) return;
-    if (lane % a.tpv != 0) return;  // the first lane of a vertex walks all its slots
-    const int v = sd.x + k;
-    const float4 mv = a.vm[v];
-    if (a.active && !a.active[__float_as_int(mv.w)]) return;  // unchanged since its last probe
-    const float4 xv = a.x[v], p0 = a.x0[v], vv = a.vel[v];
-    if (mv.y != 0.f) {
-        a.g2[v] = 0.0;
-        return;
-    }
-    const float4 acc = a.inst[__float_as_int(mv.w)];
-    const double h = a.h, m = p0.w;
-    double gx = m / (h * h) * ((double)xv.x - ((double)p0.x + h * vv.x + h * h * acc.x));
-    double gy = m / (h * h) * ((double)xv.y - ((double)p0.y + h * vv.y + h * h * acc.y));
-    double gz = m / (h * h) * ((double)xv.z - ((double)p0.z + h * vv.z + h * h * acc.z));
-    const double ks = acc.w;
-    const int rows = sd.w & 0xffff, erows = sd.w >> 16;
-    for (int row = 0; row < rows; ++row) {
-        for (int r = 0; r < a.tpv; ++r) {
-            const int e = sd.z + row * 32 + k * a.tpv + r;
-            const int2 iw = a.st_iw[e];
-            const int u = iw.x;
-            if (u == v) continue;
-            const float4 xu = a.x[u];
-            const double dx = (double)xu.x - xv.x, dy = (double)xu.y - xv.y, dz = (double)xu.z - xv.z;
-            const double w = __int_as_float(iw.y);
-            gx += w * dx;
-            gy += w * dy;
-            gz += w * dz;
-            const double L = row < erows ? a.st_rest[e] : -1.0;
-            if (L >= 0.0) {
-                const double l = sqrt(dx * dx + dy * dy + dz * dz);
-                if (l > 0.0) {
-                    const double s = ks * (l - L) / l;
-                    gx -= s * dx;
-                    gy -= s * dy;
-                    gz -= s * dz;
-                }
+template <int MODE>
+__device__ __forceinline__ void eval_row(float4 xv, float4 xu, float4 yv, float4 yu, float L, float w, double ks,
+                                         double& a0, double& a1, double& a2) {
+    const double dx = (double)xu.x - xv.x, dy = (double)xu.y - xv.y, dz = (double)xu.z - xv.z;
+    const double dd = dx * dx + dy * dy + dz * dz;
+    if (MODE == kEvalGrad) {
+        a0 += w * dx;
+        a1 += w * dy;
+        a2 += w * dz;
+        if (L >= 0.f && dd > 0.0) {
+            const double l = sqrt(dd);
+            const double s = ks * (l - L) / l;
+            a0 -= s * dx;
+            a1 -= s * dy;
+            a2 -= s * dz;
+        }
+    } else {
+        a0 -= 0.25 * w * dd;
+        if (L >= 0.f) {
+            const double cx = sqrt(dd) - L;
+            a0 += 0.25 * ks * cx * cx;
+        }
+        if (MODE == kEvalPotPair) {
+            const double ex = (double)yu.x - yv.x, ey = (double)yu.y - yv.y, ez = (double)yu.z - yv.z;
+            const double ee = ex * ex + ey * ey + ez * ez;
+            a1 -= 0.25 * w * ee;
+            if (L >= 0.f) {
+                const double cy = sqrt(ee) - L;
+                a1 += 0.25 * ks * cy * cy;
             }
         }
     }
-    a.g2[v] = gx * gx + gy * gy + gz * gz;
+}
+
+template <int TPV, int RE, int RB, int MODE>
+__global__ void __launch_bounds__(128) stencil_eval_kernel(EvalArgs a) {
+    const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (warp >= a.nslices) return;
+    const int lane = threadIdx.x & 31;
+    const int4 sd = __ldg(&a.slices[warp]);
+    const int rows = sd.w & 0xffff, erows = sd.w >> 16, brows = rows - erows;
+    const int k = lane / TPV;
+    const bool leader = k < sd.y && (lane % TPV) == 0;
+    const int v = sd.x + min(k, sd.y - 1);
+    const int base = sd.z + lane;
+    const int bbase = base + erows * 32;
+    const float4 mv = __ldg(&a.vm[v]);
+    // a slice belongs to one instance, so this exit is warp-uniform
+    if (a.active && !a.active[__float_as_int(mv.w)]) return;
+    int ue[RE], ub[RB];
+    float we[RE], le[RE], wb[RB];
+#pragma unroll
+    for (int r = 0; r < RE; ++r) {
+        ue[r] = v;
+        we[r] = 0.f;
+        le[r] = -1.f;
+        if (r < erows) {
+            const int2 iw = __ldg(&a.st_iw[base + r * 32]);
+            ue[r] = iw.x;
+            we[r] = __int_as_float(iw.y);
+            le[r] = __ldg(&a.st_rest[base + r * 32]);
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < RB; ++r) {
+        ub[r] = v;
+        wb[r] = 0.f;
+        if (r < brows) {
+            const int2 iw = __ldg(&a.st_iw[bbase + r * 32]);
+            ub[r] = iw.x;
+            wb[r] = __int_as_float(iw.y);
+        }
+    }
+    const float4 ip = __ldg(&a.inst[__float_as_int(mv.w)]);
+    const double ks = ip.w;
+    const float4 xv = a.x[v];
+    const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 yv = MODE == kEvalPotPair ? a.y[v] : zero;
+    float4 xe[RE], xb[RB], ye[RE], yb[RB];
+#pragma unroll
+    for (int r = 0; r < RE; ++r) {
+        xe[r] = a.x[ue[r]];
+        ye[r] = MODE == kEvalPotPair ? a.y[ue[r]] : zero;
+    }
+#pragma unroll
+    for (int r = 0; r < RB; ++r) {
+        xb[r] = a.x[ub[r]];
+        yb[r] = MODE == kEvalPotPair ? a.y[ub[r]] : zero;
+    }
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+#pragma unroll
+    for (int r = 0; r < RE; ++r) eval_row<MODE>(xv, xe[r], yv, ye[r], le[r], we[r], ks, a0, a1, a2);
+    for (int r = RE; r < erows; ++r) {
+        const int2 iw = __ldg(&a.st_iw[base + r * 32]);
+        eval_row<MODE>(xv, a.x[iw.x], yv, MODE == kEvalPotPair ? a.y[iw.x] : zero, __ldg(&a.st_rest[base + r * 32]),
+                       __int_as_float(iw.y), ks, a0, a1, a2);
+    }
+#pragma unroll
+    for (int r = 0; r < RB; ++r) eval_row<MODE>(xv, xb[r], yv, yb[r], -1.f, wb[r], ks, a0, a1, a2);
+    for (int r = RB; r < brows; ++r) {
+        const int2 iw = __ldg(&a.st_iw[bbase + r * 32]);
+        eval_row<MODE>(xv, a.x[iw.x], yv, MODE == kEvalPotPair ? a.y[iw.x] : zero, -1.f, __int_as_float(iw.y), ks, a0,
+                       a1, a2);
+    }
+#pragma unroll
+    for (int o = TPV / 2; o > 0; o >>= 1) {
+        a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+        a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+        a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+    }
+    if (!leader) return;
+    const float4 p0 = a.x0[v];
+    const double h = a.h, m = p0.w;
+    if (MODE == kEvalGrad) {
+        if (mv.y != 0.f) {
+            a.out0[v] = 0.0;
+            return;
+        }
+        const float4 vv = a.vel[v];
+        a0 += m / (h * h) * ((double)xv.x - ((double)p0.x + h * vv.x + h * h * ip.x));
+        a1 += m / (h * h) * ((double)xv.y - ((double)p0.y + h * vv.y + h * h * ip.y));
+        a2 += m / (h * h) * ((double)xv.z - ((double)p0.z + h * vv.z + h * h * ip.z));
+        a.out0[v] = a0 * a0 + a1 * a1 + a2 * a2;
+    } else if (MODE == kEvalPot) {
+        const float4 vv = a.vel[v];
+        const bool pinned = mv.y != 0.f;
+        const double ax = pinned ? 0.0 : ip.x, ay = pinned ? 0.0 : ip.y, az = pinned ? 0.0 : ip.z;
+        const double dx = (double)xv.x - ((double)p0.x + h * vv.x + h * h * ax);
+        const double dy = (double)xv.y - ((double)p0.y + h * vv.y + h * h * ay);
+        const double dz = (double)xv.z - ((double)p0.z + h * vv.z + h * h * az);
+        a.out0[v] = a0 + m / (2.0 * h * h) * (dx * dx + dy * dy + dz * dz);
+    } else {
+        const double dx = (double)xv.x - yv.x, dy = (double)xv.y - yv.y, dz = (double)xv.z - yv.z;
+        a.out0[v] = a0 + m / (2.0 * h * h) * (dx * dx + dy * dy + dz * dz);
+        a.out1[v] = a1;
+    }
+}
+
+template <int MODE>
+cudaError_t stencil_eval_launch(int tpv, const EvalArgs& a, cudaStream_t st) {
+    const int blocks = (a.nslices * 32 + 127) / 128;
+    if (blocks == 0) return cudaSuccess;
+    switch (tpv) {
+        case 1: stencil_eval_kernel<1, 6, 6, MODE><<<blocks, 128, 0, st>>>(a); break;
+        case 2: stencil_eval_kernel<2, 3, 3, MODE><<<blocks, 128, 0, st>>>(a); break;
+        case 4: stencil_eval_kernel<4, 2, 2, MODE><<<blocks, 128, 0, st>>>(a); break;
+        default: stencil_eval_kernel<8, 1, 1, MODE><<<blocks, 128, 0, st>>>(a); break;
+    }
+    return cudaGetLastError();
 }
 
 // Deterministic per-instance sum of g2 over the instance's layout range, two levels:
@@ -367,10 +483,10 @@ __global__ void __launch_bounds__(kRedThreads) segment_partial_kernel(const doub
     if (threadIdx.x == 0) partial[i * kSegChunks + j] = s;
 }
 
-__global__ void __launch_bounds__(kSegChunks) segment_final_kernel(const double* partial, double* out) {
+__global__ void __launch_bounds__(kSegChunks) segment_final_kernel(const double* partial, double* out, int take_sqrt) {
     __shared__ double sh[kSegChunks];
     double s = block_sum(partial[blockIdx.x * kSegChunks + threadIdx.x], sh);
-    if (threadIdx.x == 0) out[blockIdx.x] = sqrt(s);
+    if (threadIdx.x == 0) out[blockIdx.x] = take_sqrt ? sqrt(s) : s;
 }
 
 // Residual bookkeeping of ats_frame_to_residual, one block: the first call after
@@ -553,10 +669,10 @@ int enqueue_frame(ats_cloth* c, int solver, cudaStream_t st) {
     return ATS_OK;
 }
 
-int enqueue_residual_norms(ats_cloth* c, cudaStream_t st, const int* active) {
-    GradArgs a;
-    a.active = active;
+EvalArgs eval_args(ats_cloth* c) {
+    EvalArgs a;
     a.x = c->x.p;
+    a.y = nullptr;
     a.x0 = c->x0.p;
     a.vel = c->vel.p;
     a.vm = c->vm.p;
@@ -565,18 +681,49 @@ int enqueue_residual_norms(ats_cloth* c, cudaStream_t st, const int* active) {
     a.st_rest = c->st_rest.p;
     a.slices = c->slices.p;
     a.nslices = (int)c->slices.n;
-    a.tpv = c->L.tpv;
     a.h = (double)c->h;
-    a.g2 = c->g2.p;
-    const int blocks = (a.nslices * 32 + 127) / 128;
-    grad_kernel<<<blocks, 128, 0, st>>>(a);
-    ATS_CUDA(cudaGetLastError());
-    segment_partial_kernel<<<dim3(kSegChunks, c->L.ninst), kRedThreads, 0, st>>>(c->g2.p, c->inst_seg.p,
+    a.out0 = a.out1 = nullptr;
+    a.active = nullptr;
+    return a;
+}
+
+int segment_sum(ats_cloth* c, const double* per_vertex, double* out, int take_sqrt, cudaStream_t st) {
+    segment_partial_kernel<<<dim3(kSegChunks, c->L.ninst), kRedThreads, 0, st>>>(per_vertex, c->inst_seg.p,
                                                                                    c->seg_partial.p);
     ATS_CUDA(cudaGetLastError());
-    segment_final_kernel<<<c->L.ninst, kSegChunks, 0, st>>>(c->seg_partial.p, c->red_out.p);
+    segment_final_kernel<<<c->L.ninst, kSegChunks, 0, st>>>(c->seg_partial.p, out, take_sqrt);
     ATS_CUDA(cudaGetLastError());
     return ATS_OK;
+}
+
+int enqueue_residual_norms(ats_cloth* c, cudaStream_t st, const int* active) {
+    EvalArgs a = eval_args(c);
+    a.active = active;
+    a.out0 = c->g2.p;
+    ATS_CUDA(stencil_eval_launch<kEvalGrad>(c->L.tpv, a, st));
+    return segment_sum(c, c->g2.p, c->red_out.p, 1, st);
+}
+
+int enqueue_potential_pair(ats_cloth* c, const float4* y, double* gx, double* gy, cudaStream_t st) {
+    const size_t nv = c->L.nv;
+    if (!c->pot_vx.p) ATS_CUDA(c->pot_vx.alloc(nv));
+    if (!c->pot_vy.p) ATS_CUDA(c->pot_vy.alloc(nv));
+    EvalArgs a = eval_args(c);
+    a.y = y;
+    a.out0 = c->pot_vx.p;
+    a.out1 = c->pot_vy.p;
+    ATS_CUDA(stencil_eval_launch<kEvalPotPair>(c->L.tpv, a, st));
+    int r;
+    if ((r = segment_sum(c, c->pot_vx.p, gx, 0, st))) return r;
+    return segment_sum(c, c->pot_vy.p, gy, 0, st);
+}
+
+int enqueue_potential(ats_cloth* c, double* g, cudaStream_t st) {
+    if (!c->pot_vx.p) ATS_CUDA(c->pot_vx.alloc(c->L.nv));
+    EvalArgs a = eval_args(c);
+    a.out0 = c->pot_vx.p;
+    ATS_CUDA(stencil_eval_launch<kEvalPot>(c->L.tpv, a, st));
+    return segment_sum(c, c->pot_vx.p, g, 0, st);
 }
 
 int frame_to_residual_impl(ats_cloth* c, double tol, const double* tols, int check_every, int max_iterations,
@@ -1010,6 +1157,19 @@ int ats_autotune(ats_cloth* c, int iterations, ats_stream stream, int* out_tpv, 
     if (r) return r;
     if (out_tpv) *out_tpv = c->L.tpv;
     if (out_block) *out_block = c->block;
+    return ATS_OK;
+}
+
+int ats_potential(ats_cloth* c, double* out, ats_stream stream) {
+    if (!c || !out) {
+        set_error("ats_potential: null argument");
+        return ATS_ERR_INVALID;
+    }
+    cudaStream_t st = S(stream);
+    int r = enqueue_potential(c, c->red_out.p, st);
+    if (r) return r;
+    ATS_CUDA(cudaMemcpyAsync(out, c->red_out.p, c->L.ninst * sizeof(double), cudaMemcpyDeviceToHost, st));
+    ATS_CUDA(cudaStreamSynchronize(st));
     return ATS_OK;
 }
 

@@ -75,7 +75,7 @@ struct ats_cloth {
     DevBuf<int> feat_nb, inst_eseg, inst_bseg, free_list;
     DevBuf<float> feat_len, feat_stage;
     DevBuf<float4> y_buf;
-    DevBuf<double> pot_partial, pot_y, pot_guess;
+    DevBuf<double> pot_y, pot_guess, pot_vx, pot_vy;
     DevBuf<int> guess_used;
     cudaGraphExec_t warm_graph = nullptr;  // captured warm-started frame (ats_frame_warm)
     const void* warm_key_mlp = nullptr;
@@ -121,6 +121,11 @@ int enqueue_iterations(ats_cloth* c, int solver, int iterations, cudaStream_t st
 // FP64 ||grad G|| per instance into c->red_out.p; with `active`, instances whose flag
 // is 0 keep the per-vertex values of the previous call (their positions are frozen)
 int enqueue_residual_norms(ats_cloth* c, cudaStream_t st, const int* active = nullptr);
+// Per instance, the FP64 incremental potential G of the current positions (gx) and of
+// y (gy), both against the inertial prediction y (ninst values each, device pointers).
+int enqueue_potential_pair(ats_cloth* c, const float4* y, double* gx, double* gy, cudaStream_t st);
+// Per instance, G(x) against the inertial prediction of the current frame start.
+int enqueue_potential(ats_cloth* c, double* g, cudaStream_t st);
 // ats_frame_to_residual with an optional hook run after ||grad G(y)|| is taken and
 // before the first iteration (the learned warm start replaces y there).
 int frame_to_residual_impl(ats_cloth* c, double tol, const double* tols, int check_every, int max_iterations,

@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstddef>
 #include <cstring>
 #include <memory>
 #include <vector>
@@ -412,131 +413,166 @@ __global__ void __launch_bounds__(kThreads) infer_samples_kernel(const float* __
                 out[(size_t)(base + i) * kOut + k] = S.nrm[kNormOutMean + k] + S.nrm[kNormOutStd + k] * S.y[i][k];
 }
 
-// Inference, one warp per 16 vertices, activations kept in registers: the FP32
+// Inference, one warp per 32 vertices, activations kept in registers: the FP32
 // accumulators of a 64-wide layer (8 n-tiles of m16n8) are exactly the A fragments of
 // the next layer's four k16 steps once rounded to BF16 pairs, so only the features go
-// through shared memory. Persistent CTAs keep the packed weights in shared memory.
-// Same quantisation points and the same mma order as forward(): identical outputs.
-constexpr int kWarpRows = 32;  // two m16 sub-tiles; every lane gathers one vertex's features
-struct WarpScratch {
-    __nv_bfloat16 x[kWarpRows][kInP];
+// through shared memory. The warp's two m16 halves share every B fragment. Weights sit
+// in shared memory in padded rows (80 B / 144 B): the 8 row addresses of an ldmatrix
+// land in 8 different 16-byte bank groups, so fragment loads are conflict-free.
+// Persistent CTAs, as many as are resident. Same quantisation points and the same mma
+// order as forward(): identical outputs.
+constexpr int kWarpRows = 32;       // two m16 halves; every lane gathers one vertex's features
+constexpr int kRowX = kInP + 8;     // 40 bf16 = 80 B
+constexpr int kRowH = kHid + 8;     // 72 bf16 = 144 B
+struct __align__(16) WarpScratch {
+    __nv_bfloat16 x[kWarpRows][kRowX];
     float out[kWarpRows][4];
 };
-struct InferSmem {
-    __nv_bfloat16 w[kPacked];
-    float b[3 * kHid + kOutP];
+struct __align__(16) InferSmem {
+    __nv_bfloat16 w1[kHid][kRowX];
+    __nv_bfloat16 w2[kHid][kRowH];
+    __nv_bfloat16 w3[kHid][kRowH];
+    __nv_bfloat16 w4[8][kRowH];  // output rows 0..2 used, 3..7 zero
+    float b[3 * kHid + 8];
     float nrm[kNorm];
     WarpScratch ws[kThreads / 32];
 };
+static_assert(sizeof(InferSmem) <= 48 * 1024, "static shared memory");
+static_assert(offsetof(InferSmem, w2) % 16 == 0 && offsetof(InferSmem, w3) % 16 == 0 &&
+                  offsetof(InferSmem, w4) % 16 == 0 && offsetof(InferSmem, ws) % 16 == 0,
+              "ldmatrix rows must be 16-byte aligned");
 
 __device__ __forceinline__ uint32_t pack_f2(float lo, float hi) {
-    return pk(__float2bfloat16_rn(lo), __float2bfloat16_rn(hi));
+    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t*>(&v);
+}
+
+// four 8x8 BF16 matrices; lanes 8i..8i+7 give the row addresses of matrix i
+__device__ __forceinline__ void ldsm_x4(uint32_t r[4], const __nv_bfloat16* p) {
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(p);
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(a)
+                 : "memory");
 }
 
 // acc[nt][4] (FP32) of a 64-wide layer -> GELU -> A fragments a[ks][4] of the next layer
 __device__ __forceinline__ void hidden_epilogue(const float acc[8][4], const float* bias, int t, uint32_t a[4][4]) {
-    float h[8][4];
-#pragma unroll
-    for (int nt = 0; nt < 8; ++nt) {
-        const float b0 = bias[8 * nt + 2 * t], b1 = bias[8 * nt + 2 * t + 1];
-        h[nt][0] = gelu(acc[nt][0] + b0);
-        h[nt][1] = gelu(acc[nt][1] + b1);
-        h[nt][2] = gelu(acc[nt][2] + b0);
-        h[nt][3] = gelu(acc[nt][3] + b1);
-    }
 #pragma unroll
     for (int ks = 0; ks < 4; ++ks) {
-        a[ks][0] = pack_f2(h[2 * ks][0], h[2 * ks][1]);
-        a[ks][1] = pack_f2(h[2 * ks][2], h[2 * ks][3]);
-        a[ks][2] = pack_f2(h[2 * ks + 1][0], h[2 * ks + 1][1]);
-        a[ks][3] = pack_f2(h[2 * ks + 1][2], h[2 * ks + 1][3]);
+        const int n0 = 16 * ks + 2 * t, n1 = n0 + 8;
+        a[ks][0] = pack_f2(gelu(acc[2 * ks][0] + bias[n0]), gelu(acc[2 * ks][1] + bias[n0 + 1]));
+        a[ks][1] = pack_f2(gelu(acc[2 * ks][2] + bias[n0]), gelu(acc[2 * ks][3] + bias[n0 + 1]));
+        a[ks][2] = pack_f2(gelu(acc[2 * ks + 1][0] + bias[n1]), gelu(acc[2 * ks + 1][1] + bias[n1 + 1]));
+        a[ks][3] = pack_f2(gelu(acc[2 * ks + 1][2] + bias[n1]), gelu(acc[2 * ks + 1][3] + bias[n1 + 1]));
     }
 }
 
-template <int KS, int NT>
-__device__ __forceinline__ void warp_layer(const uint32_t a[][4], const __nv_bfloat16* W, int K, int g, int t,
-                                           float acc[][4]) {
+// acc[h][nt] = A_h (16 x 16 KS) * W^T for n-tiles 0..NT-1; W rows [n][k] with stride ROW
+template <int KS, int NT, int ROW>
+__device__ __forceinline__ void warp_layer2(const uint32_t a[2][4][4], const __nv_bfloat16* W, int lane,
+                                            float acc[2][NT][4]) {
 #pragma unroll
     for (int nt = 0; nt < NT; ++nt) {
-        acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
-        const __nv_bfloat16* wr = W + (8 * nt + g) * K + 2 * t;
+        uint32_t b[KS][2];
 #pragma unroll
-        for (int ks = 0; ks < KS; ++ks) {
-            const uint32_t b0 = *reinterpret_cast<const uint32_t*>(wr + 16 * ks);
-            const uint32_t b1 = *reinterpret_cast<const uint32_t*>(wr + 16 * ks + 8);
-            mma16816(acc[nt], a[ks][0], a[ks][1], a[ks][2], a[ks][3], b0, b1);
+        for (int p = 0; p < KS / 2; ++p) {
+            uint32_t r[4];
+            ldsm_x4(r, W + (8 * nt + (lane & 7)) * ROW + 32 * p + (lane >> 3) * 8);
+            b[2 * p][0] = r[0];
+            b[2 * p][1] = r[1];
+            b[2 * p + 1][0] = r[2];
+            b[2 * p + 1][1] = r[3];
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            acc[h][nt][0] = acc[h][nt][1] = acc[h][nt][2] = acc[h][nt][3] = 0.f;
+#pragma unroll
+            for (int ks = 0; ks < KS; ++ks)
+                mma16816(acc[h][nt], a[h][ks][0], a[h][ks][1], a[h][ks][2], a[h][ks][3], b[ks][0], b[ks][1]);
         }
     }
 }
 
-__global__ void __launch_bounds__(kThreads) infer_warp_kernel(FeatArgs fa, const __nv_bfloat16* __restrict__ wpack,
-                                                              const float* __restrict__ master,
-                                                              const float* __restrict__ nrm, float4* __restrict__ x,
-                                                              float s) {
-    __shared__ __align__(16) InferSmem S;
+__global__ void __launch_bounds__(kThreads, 3) infer_warp_kernel(FeatArgs fa, const __nv_bfloat16* __restrict__ wpack,
+                                                                 const float* __restrict__ master,
+                                                                 const float* __restrict__ nrm, float4* __restrict__ x,
+                                                                 float s) {
+    __shared__ InferSmem S;
     for (int i = threadIdx.x; i < kNorm; i += kThreads) S.nrm[i] = nrm[i];
-    for (int i = threadIdx.x; i < kPacked / 2; i += kThreads)
-        reinterpret_cast<uint32_t*>(S.w)[i] = reinterpret_cast<const uint32_t*>(wpack)[i];
+    const uint32_t* wp = reinterpret_cast<const uint32_t*>(wpack);
+    for (int i = threadIdx.x; i < kHid * (kInP / 2); i += kThreads)
+        reinterpret_cast<uint32_t*>(&S.w1[i / (kInP / 2)][0])[i % (kInP / 2)] = wp[kP1 / 2 + i];
+    for (int i = threadIdx.x; i < kHid * (kHid / 2); i += kThreads) {
+        reinterpret_cast<uint32_t*>(&S.w2[i / (kHid / 2)][0])[i % (kHid / 2)] = wp[kP2 / 2 + i];
+        reinterpret_cast<uint32_t*>(&S.w3[i / (kHid / 2)][0])[i % (kHid / 2)] = wp[kP3 / 2 + i];
+    }
+    for (int i = threadIdx.x; i < 8 * (kHid / 2); i += kThreads)
+        reinterpret_cast<uint32_t*>(&S.w4[i / (kHid / 2)][0])[i % (kHid / 2)] = wp[kP4 / 2 + i];
     for (int i = threadIdx.x; i < kHid; i += kThreads) {
         S.b[i] = master[kB1 + i];
         S.b[kHid + i] = master[kB2 + i];
         S.b[2 * kHid + i] = master[kB3 + i];
     }
-    for (int i = threadIdx.x; i < kOutP; i += kThreads) S.b[3 * kHid + i] = i < kOut ? master[kB4 + i] : 0.f;
+    for (int i = threadIdx.x; i < 8; i += kThreads) S.b[3 * kHid + i] = i < kOut ? master[kB4 + i] : 0.f;
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
     WarpScratch& W = S.ws[warp];
     const int ntiles = (fa.nv + kWarpRows - 1) / kWarpRows;
     for (int tile = blockIdx.x * (kThreads / 32) + warp; tile < ntiles; tile += gridDim.x * (kThreads / 32)) {
-        const int v0 = tile * kWarpRows;
-        if (lane < kWarpRows) {
-            const int v = v0 + lane;
+        const int v = tile * kWarpRows + lane;
+        {
             float f[kIn];
             if (v < fa.nv) vertex_features(fa, v, f);
-            for (int k = 0; k < kInP; ++k)
-                W.x[lane][k] = __float2bfloat16_rn(
-                    v < fa.nv && k < kIn ? (f[k] - S.nrm[kNormInMean + k]) * S.nrm[kNormInScale + k] : 0.f);
-        }
-        __syncwarp();
-#pragma unroll 1
-        for (int half = 0; half < 2; ++half) {
-            const int r0 = 16 * half;
-            uint32_t a1[2][4];
+            uint32_t q[kInP / 2];
 #pragma unroll
-            for (int ks = 0; ks < 2; ++ks) {
-                a1[ks][0] = *reinterpret_cast<const uint32_t*>(&W.x[r0 + g][16 * ks + 2 * t]);
-                a1[ks][1] = *reinterpret_cast<const uint32_t*>(&W.x[r0 + g + 8][16 * ks + 2 * t]);
-                a1[ks][2] = *reinterpret_cast<const uint32_t*>(&W.x[r0 + g][16 * ks + 2 * t + 8]);
-                a1[ks][3] = *reinterpret_cast<const uint32_t*>(&W.x[r0 + g + 8][16 * ks + 2 * t + 8]);
-            }
-            float acc[8][4];
-            uint32_t a[4][4];
-            warp_layer<2, 8>(a1, S.w + kP1, kInP, g, t, acc);
-            hidden_epilogue(acc, S.b, t, a);
-            warp_layer<4, 8>(a, S.w + kP2, kHid, g, t, acc);
-            hidden_epilogue(acc, S.b + kHid, t, a);
-            warp_layer<4, 8>(a, S.w + kP3, kHid, g, t, acc);
-            hidden_epilogue(acc, S.b + 2 * kHid, t, a);
-            float o[1][4];
-            warp_layer<4, 1>(a, S.w + kP4, kHid, g, t, o);  // output columns 0..7 (0..2 used)
-            if (t < 2) {
-                const float* b4 = S.b + 3 * kHid;
-                W.out[r0 + g][2 * t] = o[0][0] + b4[2 * t];
-                W.out[r0 + g][2 * t + 1] = o[0][1] + b4[2 * t + 1];
-                W.out[r0 + g + 8][2 * t] = o[0][2] + b4[2 * t];
-                W.out[r0 + g + 8][2 * t + 1] = o[0][3] + b4[2 * t + 1];
+            for (int k = 0; k < kIn / 2; ++k)
+                q[k] = v < fa.nv ? pack_f2((f[2 * k] - S.nrm[kNormInMean + 2 * k]) * S.nrm[kNormInScale + 2 * k],
+                                           (f[2 * k + 1] - S.nrm[kNormInMean + 2 * k + 1]) *
+                                               S.nrm[kNormInScale + 2 * k + 1])
+                                 : 0u;
+#pragma unroll
+            for (int k = kIn / 2; k < kInP / 2; ++k) q[k] = 0u;
+            uint4* row = reinterpret_cast<uint4*>(&W.x[lane][0]);
+#pragma unroll
+            for (int j = 0; j < kInP / 8; ++j) row[j] = make_uint4(q[4 * j], q[4 * j + 1], q[4 * j + 2], q[4 * j + 3]);
+        }
+        __syncwarp();
+        uint32_t a[2][4][4];
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int ks = 0; ks < 2; ++ks)
+                ldsm_x4(a[h][ks], &W.x[16 * h + (lane & 8) + (lane & 7)][16 * ks + ((lane >> 4) << 3)]);
+        float acc[2][8][4];
+        warp_layer2<2, 8, kRowX>(a, &S.w1[0][0], lane, acc);
+        hidden_epilogue(acc[0], S.b, t, a[0]);
+        hidden_epilogue(acc[1], S.b, t, a[1]);
+        warp_layer2<4, 8, kRowH>(a, &S.w2[0][0], lane, acc);
+        hidden_epilogue(acc[0], S.b + kHid, t, a[0]);
+        hidden_epilogue(acc[1], S.b + kHid, t, a[1]);
+        warp_layer2<4, 8, kRowH>(a, &S.w3[0][0], lane, acc);
+        hidden_epilogue(acc[0], S.b + 2 * kHid, t, a[0]);
+        hidden_epilogue(acc[1], S.b + 2 * kHid, t, a[1]);
+        float o[2][1][4];
+        warp_layer2<4, 1, kRowH>(a, &S.w4[0][0], lane, o);  // output columns 0..7 (0..2 used)
+        if (t < 2) {
+            const float* b4 = S.b + 3 * kHid;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                W.out[16 * h + g][2 * t] = o[h][0][0] + b4[2 * t];
+                W.out[16 * h + g][2 * t + 1] = o[h][0][1] + b4[2 * t + 1];
+                W.out[16 * h + g + 8][2 * t] = o[h][0][2] + b4[2 * t];
+                W.out[16 * h + g + 8][2 * t + 1] = o[h][0][3] + b4[2 * t + 1];
             }
         }
         __syncwarp();
-        if (lane < kWarpRows) {
-            const int v = v0 + lane;
-            if (v < fa.nv && fa.vm[v].y == 0.f) {
-                float4 p = x[v];
-                p.x += s * (S.nrm[kNormOutMean + 0] + S.nrm[kNormOutStd + 0] * W.out[lane][0]);
-                p.y += s * (S.nrm[kNormOutMean + 1] + S.nrm[kNormOutStd + 1] * W.out[lane][1]);
-                p.z += s * (S.nrm[kNormOutMean + 2] + S.nrm[kNormOutStd + 2] * W.out[lane][2]);
-                x[v] = p;
-            }
+        if (v < fa.nv && fa.vm[v].y == 0.f) {
+            float4 p = x[v];
+            p.x += s * (S.nrm[kNormOutMean + 0] + S.nrm[kNormOutStd + 0] * W.out[lane][0]);
+            p.y += s * (S.nrm[kNormOutMean + 1] + S.nrm[kNormOutStd + 1] * W.out[lane][1]);
+            p.z += s * (S.nrm[kNormOutMean + 2] + S.nrm[kNormOutStd + 2] * W.out[lane][2]);
+            x[v] = p;
         }
         __syncwarp();
     }
@@ -560,98 +596,6 @@ __global__ void append_kernel(const float* __restrict__ stage, const float4* __r
     targ[o * kOut + 0] = (p.x - q.x) * inv_s;
     targ[o * kOut + 1] = (p.y - q.y) * inv_s;
     targ[o * kOut + 2] = (p.z - q.z) * inv_s;
-}
-
-// ---------------------------------------------------------------- per-instance FP64 potential
-constexpr int kPotChunks = 32;
-struct PotArgs {
-    const float4* x;
-    const float4* y;
-    const float4* x0;
-    const float4* vm;
-    const int* vseg;
-    const int2* edge;
-    const float* rest;
-    const float* kst;
-    const int* eseg;
-    const int4* bend;
-    const float* q16;
-    const float* kb;
-    const int* bseg;
-    double h;
-    double* partial;  // 2 * ninst * kPotChunks
-};
-
-// Per instance, in one pass over the geometry: G(x) (inertia + springs + bending) and
-// G(y) (springs + bending; its inertia term is 0), y the inertial prediction,
-// G(z) = sum m/(2h^2)|z - y|^2 + sum 1/2 k (l - L)^2 + sum 1/2 k_b z^T Q z.
-__device__ __forceinline__ double spring_energy(float4 p0, float4 p1, float L, float k) {
-    const double dx = (double)p1.x - p0.x, dy = (double)p1.y - p0.y, dz = (double)p1.z - p0.z;
-    const double C = sqrt(dx * dx + dy * dy + dz * dz) - (double)L;
-    return 0.5 * (double)k * C * C;
-}
-__device__ __forceinline__ double bending_energy(const float4* pos, int4 id, const float* Q, float kb) {
-    const int vid[4] = {id.x, id.y, id.z, id.w};
-    double p[4][3];
-    for (int k = 0; k < 4; ++k) {
-        const float4 t = pos[vid[k]];
-        p[k][0] = t.x;
-        p[k][1] = t.y;
-        p[k][2] = t.z;
-    }
-    double s = 0.0;
-    for (int c = 0; c < 4; ++c)
-        for (int r = 0; r < 4; ++r) s += (double)Q[4 * c + r] * (p[c][0] * p[r][0] + p[c][1] * p[r][1] + p[c][2] * p[r][2]);
-    return 0.5 * (double)kb * s;
-}
-
-__global__ void __launch_bounds__(256) potential_kernel(PotArgs a) {
-    __shared__ double shx[256], shy[256];
-    const int i = blockIdx.y, j = blockIdx.x, stride = kPotChunks * 256;
-    double gx = 0.0, gy = 0.0;
-    for (int v = a.vseg[i] + j * 256 + threadIdx.x; v < a.vseg[i + 1]; v += stride) {
-        const float4 p = a.x[v], q = a.y[v];
-        const double dx = (double)p.x - q.x, dy = (double)p.y - q.y, dz = (double)p.z - q.z;
-        gx += (double)a.x0[v].w / (2.0 * a.h * a.h) * (dx * dx + dy * dy + dz * dz);
-    }
-    for (int e = a.eseg[i] + j * 256 + threadIdx.x; e < a.eseg[i + 1]; e += stride) {
-        const int2 ed = a.edge[e];
-        const float L = a.rest[e], k = a.kst[e];
-        gx += spring_energy(a.x[ed.x], a.x[ed.y], L, k);
-        gy += spring_energy(a.y[ed.x], a.y[ed.y], L, k);
-    }
-    for (int b = a.bseg[i] + j * 256 + threadIdx.x; b < a.bseg[i + 1]; b += stride) {
-        const int4 id = a.bend[b];
-        const float* Q = a.q16 + 16 * (size_t)b;
-        gx += bending_energy(a.x, id, Q, a.kb[b]);
-        gy += bending_energy(a.y, id, Q, a.kb[b]);
-    }
-    shx[threadIdx.x] = gx;
-    shy[threadIdx.x] = gy;
-    __syncthreads();
-    for (int s = 128; s > 0; s >>= 1) {
-        if (threadIdx.x < s) {
-            shx[threadIdx.x] += shx[threadIdx.x + s];
-            shy[threadIdx.x] += shy[threadIdx.x + s];
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        a.partial[2 * (i * kPotChunks + j)] = shx[0];
-        a.partial[2 * (i * kPotChunks + j) + 1] = shy[0];
-    }
-}
-
-__global__ void potential_final_kernel(const double* partial, double* gx, double* gy, int ninst) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= ninst) return;
-    double sx = 0.0, sy = 0.0;
-    for (int j = 0; j < kPotChunks; ++j) {
-        sx += partial[2 * (i * kPotChunks + j)];
-        sy += partial[2 * (i * kPotChunks + j) + 1];
-    }
-    gx[i] = sx;
-    gy[i] = sy;
 }
 
 // keep the guess of an instance only if G(guess) <= G(y); otherwise restore y
@@ -701,9 +645,19 @@ int ensure_partials(ats_mlp* m, int ctas) {
     return ATS_OK;
 }
 
+int g_infer_ctas = 148;  // resident CTAs of infer_warp_kernel on the device (set_smem_limits)
+
+// Kernel attributes and launch shapes, set once before any launch or capture.
 int set_smem_limits() {
     static bool done = false;
     if (done) return ATS_OK;
+    {
+        int dev = 0, sms = 0, resident = 0;
+        ATS_CUDA(cudaGetDevice(&dev));
+        ATS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        ATS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, infer_warp_kernel, kThreads, 0));
+        g_infer_ctas = std::max(1, sms) * std::max(1, resident);
+    }
     ATS_CUDA(cudaFuncSetAttribute(train_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmem));
     ATS_CUDA(cudaFuncSetAttribute(infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmem));
     ATS_CUDA(cudaFuncSetAttribute(infer_samples_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmem));
@@ -752,34 +706,11 @@ FeatArgs feat_args(ats_cloth* c) {
 int ensure_learn_buffers(ats_cloth* c) {
     const size_t nv = c->L.nv;
     if (!c->y_buf.p) ATS_CUDA(c->y_buf.alloc(nv));
-    if (!c->pot_partial.p) ATS_CUDA(c->pot_partial.alloc((size_t)2 * kPotChunks * c->L.ninst));
     if (!c->pot_y.p) ATS_CUDA(c->pot_y.alloc(c->L.ninst));
+    if (!c->pot_vx.p) ATS_CUDA(c->pot_vx.alloc(nv));  // per-vertex shares of G(guess), G(y)
+    if (!c->pot_vy.p) ATS_CUDA(c->pot_vy.alloc(nv));
     if (!c->pot_guess.p) ATS_CUDA(c->pot_guess.alloc(c->L.ninst));
     if (!c->guess_used.p) ATS_CUDA(c->guess_used.alloc(c->L.ninst));
-    return ATS_OK;
-}
-
-int enqueue_potential(ats_cloth* c, double* gx, double* gy, cudaStream_t st) {
-    PotArgs a;
-    a.x = c->x.p;
-    a.y = c->y_buf.p;
-    a.x0 = c->x0.p;
-    a.vm = c->vm.p;
-    a.vseg = c->inst_seg.p;
-    a.edge = c->en_edge.p;
-    a.rest = c->en_rest.p;
-    a.kst = c->en_k.p;
-    a.eseg = c->inst_eseg.p;
-    a.bend = c->en_bend.p;
-    a.q16 = c->en_q.p;
-    a.kb = c->en_kb.p;
-    a.bseg = c->inst_bseg.p;
-    a.h = c->h;
-    a.partial = c->pot_partial.p;
-    potential_kernel<<<dim3(kPotChunks, c->L.ninst), 256, 0, st>>>(a);
-    ATS_CUDA(cudaGetLastError());
-    potential_final_kernel<<<(c->L.ninst + 127) / 128, 128, 0, st>>>(c->pot_partial.p, gx, gy, c->L.ninst);
-    ATS_CUDA(cudaGetLastError());
     return ATS_OK;
 }
 
@@ -791,21 +722,14 @@ int enqueue_warm_start(ats_cloth* c, const ats_mlp* m, int fallback, cudaStream_
     copy4_kernel<<<(nv + 255) / 256, 256, 0, st>>>(c->x.p, c->y_buf.p, nv);
     ATS_CUDA(cudaGetLastError());
     {
-        static int sm_count = 0;
-        if (!sm_count) {
-            int dev = 0;
-            cudaGetDevice(&dev);
-            cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, dev);
-            if (sm_count <= 0) sm_count = 148;
-        }
         const int tiles = (nv + kWarpRows - 1) / kWarpRows;
-        const int grid = std::max(1, std::min((tiles + 3) / 4, sm_count * 8));
+        const int grid = std::max(1, std::min((tiles + 3) / 4, g_infer_ctas));
         infer_warp_kernel<<<grid, kThreads, 0, st>>>(feat_args(c), m->wpack.p, m->master.p, m->nrm.p, c->x.p,
                                                      9.8f * c->h * c->h);
     }
     ATS_CUDA(cudaGetLastError());
     if (fallback) {
-        if ((r = enqueue_potential(c, c->pot_guess.p, c->pot_y.p, st))) return r;
+        if ((r = enqueue_potential_pair(c, c->y_buf.p, c->pot_guess.p, c->pot_y.p, st))) return r;
         const int n = std::max(nv, c->L.ninst);
         fallback_kernel<<<(n + 255) / 256, 256, 0, st>>>(c->x.p, c->y_buf.p, c->vm.p, c->pot_y.p, c->pot_guess.p,
                                                           c->guess_used.p, nv, c->L.ninst);

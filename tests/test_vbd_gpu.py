@@ -265,3 +265,55 @@ def test_batched_early_exit_per_instance(ats):
         assert np.array_equal(xb[off:off + n], x1), i
         assert np.array_equal(vb[off:off + n], v1), i
         off += n
+
+
+def _potential_fp64(ats, inst, x, x0, v0, h, accel):
+    """G(x) of one instance in FP64 from its own topology: inertia against
+    y = x0 + h v0 + h^2 a (a = 0 at pins), springs 1/2 k (l - L)^2, bending
+    1/2 k_b sum_b x^T Q_b x."""
+    topo = ats.Topology(inst)
+    e, b = topo.edges()
+    L, Q = topo.rest()
+    x, x0, v0 = (np.asarray(a, dtype=np.float64) for a in (x, x0, v0))
+    # material and acceleration as the handle stores them (FP32)
+    ks, kb = float(np.float32(inst.k_stretch)), float(np.float32(inst.k_bend))
+    acc = np.asarray(accel, dtype=np.float32).astype(np.float64)
+    a = np.where(inst.fixed[:, None] != 0, 0.0, acc[None, :])
+    d = x - (x0 + h * v0 + h * h * a)
+    gi = np.sum(inst.mass.astype(np.float64) / (2 * h * h) * np.sum(d * d, axis=1))
+    l = np.linalg.norm(x[e[:, 1]] - x[e[:, 0]], axis=1)
+    gs = np.sum(0.5 * ks * (l - L.astype(np.float64)) ** 2)
+    P = x[b]  # (B, 4, 3)
+    Qd = Q.astype(np.float64)
+    gb = 0.5 * kb * np.einsum("bij,bik,bjk->", Qd, P, P)
+    # size of the terms the per-vertex form adds: sum |k_b Q_ij| |x_i - x_j|^2
+    D = np.sum((P[:, :, None, :] - P[:, None, :, :]) ** 2, axis=3)
+    scale = kb * np.sum(np.abs(Qd) * D)
+    return gi + gs + gb, scale
+
+
+@pytest.mark.parametrize("bending", [True, False])
+def test_potential_matches_fp64_evaluation(ats, bending):
+    insts, prm = configs.c2(num_instances=3, seed=5, side_range=(10, 24))
+    if not bending:
+        insts = [ats.Instance(i.positions, i.faces, i.mass, i.fixed, i.k_stretch, 0.0) for i in insts]
+    cloth = ats.Cloth(insts, **prm)
+    for _ in range(3):
+        cloth.frame()
+    x0, v0 = cloth.state()
+    cloth.predict()
+    cloth.vbd_iterations(7)
+    x = cloth.positions()
+    cloth.set_state(x0, v0)
+    cloth.set_positions(x)
+    g = cloth.potential()
+    h = float(np.float32(prm["implicit_dt"]))  # the handle keeps h in FP32
+    o = 0
+    for i, inst in enumerate(insts):
+        n = inst.num_verts
+        ref, scale = _potential_fp64(ats, inst, x[o:o + n], x0[o:o + n], v0[o:o + n], h, (0.0, -9.8, 0.0))
+        # the kernel sums -1/4 W_vu |x_u - x_v|^2 with the solver's merged weights W,
+        # FP32 sums of k_b Q (~1e-7 relative rounding per term, random in sign); the
+        # terms are large and cancel, so the bending part carries ~1e-9 of their size
+        assert abs(g[i] - ref) <= 5e-9 * scale + 1e-9 * abs(ref), (i, g[i], ref, scale)
+        o += n
