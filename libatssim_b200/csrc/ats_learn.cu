@@ -6,7 +6,7 @@
 //   features (24): h v / s, (y - x0) / s, and for the 6 edge neighbours in rest
 //   directions (+x, +x+z, +z, -x, -x-z, -z) (x0_u - x0_v) / rest length (0 if none)
 //   output (3):    (x* - y) / s,   guess = y + s * output   (pinned vertices keep y)
-// Network 24 -> 64 -> 64 -> 64 -> 3, exact GELU, BF16 weights and activations, FP32
+// Network 24 -> 64 -> 64 -> 64 -> 3, GELU (polynomial form, ats_gelu.cuh), BF16 weights and activations, FP32
 // accumulation on the tensor cores (mma.sync m16n8k16 bf16). Training: MSE on the
 // solved positions of recorded frames, Adam, deterministic per-CTA gradient partials.
 // Fallback: per instance, the guess is kept only if the FP64 incremental potential
@@ -23,6 +23,7 @@
 #include <memory>
 #include <vector>
 
+#include "ats_gelu.cuh"
 #include "ats_internal.cuh"
 
 namespace ats {
@@ -62,13 +63,15 @@ __device__ __forceinline__ void mma16816(float d[4], uint32_t a0, uint32_t a1, u
 // mma chain; A and B return BF16 elements (any layout), epi(m, n, value) consumes
 // the FP32 result. Fragment layout of m16n8k16 (PTX ISA): group g = lane/4, thread
 // t = lane%4; A rows g / g+8, columns 2t.. / 2t+8..; B columns g, rows 2t.. / 2t+8...
-template <int M, int N, int K, typename FA, typename FB, typename FE>
-__device__ __forceinline__ void cta_gemm(FA A, FB B, FE epi) {
+// The accumulators start at init(n) (a bias, or 0).
+template <int M, int N, int K, typename FA, typename FB, typename FI, typename FE>
+__device__ __forceinline__ void cta_gemm_init(FA A, FB B, FI init, FE epi) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
     constexpr int MT = M / 16, NT = N / 8;
     for (int tile = warp; tile < MT * NT; tile += kThreads / 32) {
         const int m0 = (tile / NT) * 16, n0 = (tile % NT) * 8;
-        float d[4] = {0.f, 0.f, 0.f, 0.f};
+        const float i0 = init(n0 + 2 * t), i1 = init(n0 + 2 * t + 1);
+        float d[4] = {i0, i1, i0, i1};
 #pragma unroll
         for (int k0 = 0; k0 < K; k0 += 16) {
             const uint32_t a0 = pk(A(m0 + g, k0 + 2 * t), A(m0 + g, k0 + 2 * t + 1));
@@ -86,9 +89,9 @@ __device__ __forceinline__ void cta_gemm(FA A, FB B, FE epi) {
     }
 }
 
-__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.f + erff(z * 0.70710678118654752f)); }
-__device__ __forceinline__ float gelu_grad(float z) {
-    return 0.5f * (1.f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
+template <int M, int N, int K, typename FA, typename FB, typename FE>
+__device__ __forceinline__ void cta_gemm(FA A, FB B, FE epi) {
+    cta_gemm_init<M, N, K>(A, B, [](int) { return 0.f; }, epi);
 }
 
 // Shared memory of one 64-sample tile.
@@ -124,29 +127,34 @@ __device__ void forward(Tile& S) {
     const __nv_bfloat16* W2 = S.w + kP2;
     const __nv_bfloat16* W3 = S.w + kP3;
     const __nv_bfloat16* W4 = S.w + kP4;
-    cta_gemm<kTile, kHid, kInP>([&](int m, int k) { return S.x[m][k]; }, [&](int k, int n) { return W1[n * kInP + k]; },
-                                [&](int m, int n, float v) {
-                                    const float a = v + S.b[n];
-                                    S.z[0][m][n] = a;
-                                    S.h[0][m][n] = __float2bfloat16_rn(gelu(a));
-                                });
+    // the accumulators start at the bias: z = b + sum_k a_k w_k
+    cta_gemm_init<kTile, kHid, kInP>([&](int m, int k) { return S.x[m][k]; },
+                                     [&](int k, int n) { return W1[n * kInP + k]; }, [&](int n) { return S.b[n]; },
+                                     [&](int m, int n, float v) {
+                                         S.z[0][m][n] = v;
+                                         S.h[0][m][n] = __float2bfloat16_rn(gelu(v));
+                                     });
     __syncthreads();
-    cta_gemm<kTile, kHid, kHid>([&](int m, int k) { return S.h[0][m][k]; }, [&](int k, int n) { return W2[n * kHid + k]; },
-                                [&](int m, int n, float v) {
-                                    const float a = v + S.b[kHid + n];
-                                    S.z[1][m][n] = a;
-                                    S.h[1][m][n] = __float2bfloat16_rn(gelu(a));
-                                });
+    cta_gemm_init<kTile, kHid, kHid>([&](int m, int k) { return S.h[0][m][k]; },
+                                     [&](int k, int n) { return W2[n * kHid + k]; },
+                                     [&](int n) { return S.b[kHid + n]; },
+                                     [&](int m, int n, float v) {
+                                         S.z[1][m][n] = v;
+                                         S.h[1][m][n] = __float2bfloat16_rn(gelu(v));
+                                     });
     __syncthreads();
-    cta_gemm<kTile, kHid, kHid>([&](int m, int k) { return S.h[1][m][k]; }, [&](int k, int n) { return W3[n * kHid + k]; },
-                                [&](int m, int n, float v) {
-                                    const float a = v + S.b[2 * kHid + n];
-                                    S.z[2][m][n] = a;
-                                    S.h[2][m][n] = __float2bfloat16_rn(gelu(a));
-                                });
+    cta_gemm_init<kTile, kHid, kHid>([&](int m, int k) { return S.h[1][m][k]; },
+                                     [&](int k, int n) { return W3[n * kHid + k]; },
+                                     [&](int n) { return S.b[2 * kHid + n]; },
+                                     [&](int m, int n, float v) {
+                                         S.z[2][m][n] = v;
+                                         S.h[2][m][n] = __float2bfloat16_rn(gelu(v));
+                                     });
     __syncthreads();
-    cta_gemm<kTile, kOutP, kHid>([&](int m, int k) { return S.h[2][m][k]; }, [&](int k, int n) { return W4[n * kHid + k]; },
-                                 [&](int m, int n, float v) { S.y[m][n] = v + S.b[3 * kHid + n]; });
+    cta_gemm_init<kTile, kOutP, kHid>([&](int m, int k) { return S.h[2][m][k]; },
+                                      [&](int k, int n) { return W4[n * kHid + k]; },
+                                      [&](int n) { return S.b[3 * kHid + n]; },
+                                      [&](int m, int n, float v) { S.y[m][n] = v; });
     __syncthreads();
 }
 
@@ -456,22 +464,27 @@ __device__ __forceinline__ void ldsm_x4(uint32_t r[4], const __nv_bfloat16* p) {
                  : "memory");
 }
 
-// acc[nt][4] (FP32) of a 64-wide layer -> GELU -> A fragments a[ks][4] of the next layer
-__device__ __forceinline__ void hidden_epilogue(const float acc[8][4], const float* bias, int t, uint32_t a[4][4]) {
+// acc[nt][4] (FP32, bias included) of a 64-wide layer -> GELU -> A fragments a[ks][4]
+// of the next layer; adjacent columns (2t, 2t+1) go through one packed GELU
+__device__ __forceinline__ void hidden_epilogue(const float acc[8][4], uint32_t a[4][4]) {
 #pragma unroll
     for (int ks = 0; ks < 4; ++ks) {
-        const int n0 = 16 * ks + 2 * t, n1 = n0 + 8;
-        a[ks][0] = pack_f2(gelu(acc[2 * ks][0] + bias[n0]), gelu(acc[2 * ks][1] + bias[n0 + 1]));
-        a[ks][1] = pack_f2(gelu(acc[2 * ks][2] + bias[n0]), gelu(acc[2 * ks][3] + bias[n0 + 1]));
-        a[ks][2] = pack_f2(gelu(acc[2 * ks + 1][0] + bias[n1]), gelu(acc[2 * ks + 1][1] + bias[n1 + 1]));
-        a[ks][3] = pack_f2(gelu(acc[2 * ks + 1][2] + bias[n1]), gelu(acc[2 * ks + 1][3] + bias[n1 + 1]));
+        const float2 h0 = gelu2(make_float2(acc[2 * ks][0], acc[2 * ks][1]));
+        const float2 h1 = gelu2(make_float2(acc[2 * ks][2], acc[2 * ks][3]));
+        const float2 h2 = gelu2(make_float2(acc[2 * ks + 1][0], acc[2 * ks + 1][1]));
+        const float2 h3 = gelu2(make_float2(acc[2 * ks + 1][2], acc[2 * ks + 1][3]));
+        a[ks][0] = pack_f2(h0.x, h0.y);
+        a[ks][1] = pack_f2(h1.x, h1.y);
+        a[ks][2] = pack_f2(h2.x, h2.y);
+        a[ks][3] = pack_f2(h3.x, h3.y);
     }
 }
 
-// acc[h][nt] = A_h (16 x 16 KS) * W^T for n-tiles 0..NT-1; W rows [n][k] with stride ROW
+// acc[h][nt] = bias + A_h (16 x 16 KS) * W^T for n-tiles 0..NT-1; W rows [n][k] with
+// stride ROW
 template <int KS, int NT, int ROW>
-__device__ __forceinline__ void warp_layer2(const uint32_t a[2][4][4], const __nv_bfloat16* W, int lane,
-                                            float acc[2][NT][4]) {
+__device__ __forceinline__ void warp_layer2(const uint32_t a[2][4][4], const __nv_bfloat16* W, const float* bias,
+                                            int lane, float acc[2][NT][4]) {
 #pragma unroll
     for (int nt = 0; nt < NT; ++nt) {
         uint32_t b[KS][2];
@@ -484,9 +497,11 @@ __device__ __forceinline__ void warp_layer2(const uint32_t a[2][4][4], const __n
             b[2 * p + 1][0] = r[2];
             b[2 * p + 1][1] = r[3];
         }
+        const float b0 = bias[8 * nt + 2 * (lane & 3)], b1 = bias[8 * nt + 2 * (lane & 3) + 1];
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
-            acc[h][nt][0] = acc[h][nt][1] = acc[h][nt][2] = acc[h][nt][3] = 0.f;
+            acc[h][nt][0] = acc[h][nt][2] = b0;
+            acc[h][nt][1] = acc[h][nt][3] = b1;
 #pragma unroll
             for (int ks = 0; ks < KS; ++ks)
                 mma16816(acc[h][nt], a[h][ks][0], a[h][ks][1], a[h][ks][2], a[h][ks][3], b[ks][0], b[ks][1]);
@@ -545,25 +560,24 @@ __global__ void __launch_bounds__(kThreads, 3) infer_warp_kernel(FeatArgs fa, co
             for (int ks = 0; ks < 2; ++ks)
                 ldsm_x4(a[h][ks], &W.x[16 * h + (lane & 8) + (lane & 7)][16 * ks + ((lane >> 4) << 3)]);
         float acc[2][8][4];
-        warp_layer2<2, 8, kRowX>(a, &S.w1[0][0], lane, acc);
-        hidden_epilogue(acc[0], S.b, t, a[0]);
-        hidden_epilogue(acc[1], S.b, t, a[1]);
-        warp_layer2<4, 8, kRowH>(a, &S.w2[0][0], lane, acc);
-        hidden_epilogue(acc[0], S.b + kHid, t, a[0]);
-        hidden_epilogue(acc[1], S.b + kHid, t, a[1]);
-        warp_layer2<4, 8, kRowH>(a, &S.w3[0][0], lane, acc);
-        hidden_epilogue(acc[0], S.b + 2 * kHid, t, a[0]);
-        hidden_epilogue(acc[1], S.b + 2 * kHid, t, a[1]);
+        warp_layer2<2, 8, kRowX>(a, &S.w1[0][0], S.b, lane, acc);
+        hidden_epilogue(acc[0], a[0]);
+        hidden_epilogue(acc[1], a[1]);
+        warp_layer2<4, 8, kRowH>(a, &S.w2[0][0], S.b + kHid, lane, acc);
+        hidden_epilogue(acc[0], a[0]);
+        hidden_epilogue(acc[1], a[1]);
+        warp_layer2<4, 8, kRowH>(a, &S.w3[0][0], S.b + 2 * kHid, lane, acc);
+        hidden_epilogue(acc[0], a[0]);
+        hidden_epilogue(acc[1], a[1]);
         float o[2][1][4];
-        warp_layer2<4, 1, kRowH>(a, &S.w4[0][0], lane, o);  // output columns 0..7 (0..2 used)
+        warp_layer2<4, 1, kRowH>(a, &S.w4[0][0], S.b + 3 * kHid, lane, o);  // output columns 0..7 (0..2 used)
         if (t < 2) {
-            const float* b4 = S.b + 3 * kHid;
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
-                W.out[16 * h + g][2 * t] = o[h][0][0] + b4[2 * t];
-                W.out[16 * h + g][2 * t + 1] = o[h][0][1] + b4[2 * t + 1];
-                W.out[16 * h + g + 8][2 * t] = o[h][0][2] + b4[2 * t];
-                W.out[16 * h + g + 8][2 * t + 1] = o[h][0][3] + b4[2 * t + 1];
+                W.out[16 * h + g][2 * t] = o[h][0][0];
+                W.out[16 * h + g][2 * t + 1] = o[h][0][1];
+                W.out[16 * h + g + 8][2 * t] = o[h][0][2];
+                W.out[16 * h + g + 8][2 * t + 1] = o[h][0][3];
             }
         }
         __syncwarp();

@@ -1,7 +1,10 @@
 """CPU oracle of the warm-start MLP (test infrastructure only).
 
-Forward and backward of the 24 -> 64 -> 64 -> 64 -> 3 network with exact GELU and a
-mean-squared-error loss, in FP64. With quantize=True the values are rounded to
+Forward and backward of the 24 -> 64 -> 64 -> 64 -> 3 network with GELU and a
+mean-squared-error loss, in FP64. The network's GELU is the FMA-only polynomial form
+of the CUDA kernels (libatssim_b200/csrc/ats_gelu.cuh: g(z) = z (1/2 + z S(x)),
+x = 2 z^2 / 4.5^2 - 1 for |z| < 4.5, z or 0 beyond), evaluated here in FP64 from the
+same FP32 coefficients; it is within 1.2e-4 of z Phi(z). With quantize=True the values are rounded to
 BF16 where the CUDA kernels round them (inputs, weights, hidden activations, the
 output gradient and the pre-activation gradients that feed the GEMMs), so the
 CUDA FP32-accumulated results can be compared tightly. With quantize=False it is
@@ -40,15 +43,40 @@ def bf16(a):
     return r.astype(np.uint32).view(np.float32).astype(np.float64)
 
 
+GELU_CUT = 4.5
+GELU_SCALE = float(np.float32(2.0 / 4.5 ** 2))  # 2 / cut^2 as the kernels hold it
+GELU_POLY = np.array([
+    1.569028050e-01, -7.717044652e-02, 5.479086563e-02, -4.057224095e-02, 2.779665403e-02,
+    -1.670240983e-02, 1.189577673e-02, -9.356983006e-03, 3.531820374e-03,
+], dtype=np.float32).astype(np.float64)  # S(x), lowest power first
+
 _erf = np.vectorize(math.erf)
 
 
-def gelu(z):
+def gelu_exact(z):
     return 0.5 * z * (1.0 + _erf(z / math.sqrt(2.0)))
 
 
+def _poly(z):
+    z = np.asarray(z, dtype=np.float64)
+    x = z * z * GELU_SCALE - 1.0
+    s = np.full_like(x, GELU_POLY[-1])
+    d = np.zeros_like(x)
+    for c in GELU_POLY[-2::-1]:
+        d = d * x + s
+        s = s * x + c
+    return z, s, d
+
+
+def gelu(z):
+    z, s, _ = _poly(z)
+    return np.where(z >= GELU_CUT, z, np.where(z <= -GELU_CUT, 0.0, z * (0.5 + z * s)))
+
+
 def gelu_grad(z):
-    return 0.5 * (1.0 + _erf(z / math.sqrt(2.0))) + z * np.exp(-0.5 * z * z) / math.sqrt(2.0 * math.pi)
+    z, s, d = _poly(z)
+    g = 0.5 + 2.0 * z * s + 2.0 * GELU_SCALE * z ** 3 * d
+    return np.where(z >= GELU_CUT, 1.0, np.where(z <= -GELU_CUT, 0.0, g))
 
 
 def normalize_inputs(x, norm):

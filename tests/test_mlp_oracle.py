@@ -26,3 +26,19 @@ def test_bf16_rounding():
     assert r[3] == 1.0          # below half a BF16 ulp
     assert r[4] == -3.140625
     assert M.NPARAMS == 10115
+
+
+def test_gelu_polynomial_is_the_kernels_and_close_to_exact():
+    import os
+    import re
+    hdr = open(os.path.join(os.path.dirname(__file__), "..", "libatssim_b200", "csrc", "ats_gelu.cuh")).read()
+    body = hdr[hdr.index("kGeluPoly[kGeluDeg + 1] = {"):]
+    body = body[body.index("{") + 1:body.index("}")]
+    coefs = np.array([float(v.rstrip("f")) for v in re.findall(r"[-+0-9.e]+f", body)], dtype=np.float32)
+    assert np.array_equal(coefs.astype(np.float64), M.GELU_POLY)
+    z = np.linspace(-8, 8, 16001)
+    assert np.max(np.abs(M.gelu(z) - M.gelu_exact(z))) < 1.2e-4
+    # the derivative is the polynomial's own (central differences away from the cut)
+    zz = np.linspace(-4.4, 4.4, 999)
+    fd = (M.gelu(zz + 1e-6) - M.gelu(zz - 1e-6)) / 2e-6
+    assert np.max(np.abs(fd - M.gelu_grad(zz))) < 1e-7
