@@ -197,13 +197,20 @@ int ats_frame_graph(ats_cloth* cloth, int solver, ats_stream stream);
  * stops (its sweeps are skipped) once ||grad G(x)|| <= tol ||grad G(y)|| or after
  * max_iterations; then the velocity update. iterations / residual (host, one per
  * instance, nullable) receive the iterations used and the final relative residual.
- * The residual is the SURVEY definition: incremental-potential gradient over free
- * vertices, y the inertial prediction. Synchronises `stream` after every chunk. */
+ * The residual is the norm of the incremental-potential gradient over free vertices
+ * relative to its value at y, the inertial prediction (the reference defines none);
+ * the probes evaluate each vertex's gradient with the solver's FP32 force arithmetic
+ * and sum in FP64 (ats_residual is FP64 throughout). The host reads the number of
+ * active instances every fourth probe. */
 int ats_frame_to_residual(ats_cloth* cloth, double tol, int check_every, int max_iterations, int* iterations,
                           double* residual, ats_stream stream);
-/* The same with one tolerance per instance (host array). */
-int ats_frame_to_residuals(ats_cloth* cloth, const double* tols, int check_every, int max_iterations, int* iterations,
-                           double* residual, ats_stream stream);
+/* The same with one tolerance per instance (host array) and, when first_check (host,
+ * one per instance) is not null, a probe schedule per instance: instance i is probed
+ * after first_check[i], first_check[i] + check_every, ... iterations and at
+ * max_iterations (an instance whose iteration count is predictable, e.g. from its
+ * previous frame, is probed once or twice instead of every check_every). */
+int ats_frame_to_residuals(ats_cloth* cloth, const double* tols, const int* first_check, int check_every,
+                           int max_iterations, int* iterations, double* residual, ats_stream stream);
 
 /* Times `iterations` VBD iterations for every lanes-per-vertex (1, 2, 4, 8) and
  * block size (64, 128, 256) on this handle's own mesh, keeps the fastest and
@@ -310,12 +317,12 @@ int ats_warm_start(ats_cloth* cloth, const ats_mlp* mlp, int fallback, int* used
  * the model's parameters may change between replays). */
 int ats_frame_warm(ats_cloth* cloth, const ats_mlp* mlp, int fallback, int iterations, int use_graph,
                    ats_stream stream);
-/* ats_frame_to_residual with the learned guess; the residual stays relative to
- * ||grad G(y)|| of the inertial prediction. tols (host, one per instance) overrides
- * tol when not null. */
+/* ats_frame_to_residuals with the learned guess; the residual stays relative to
+ * ||grad G(y)|| of the inertial prediction. tols (host, one per instance) overrides tol when not null;
+ * first_check (nullable) is the per-instance probe schedule of ats_frame_to_residuals. */
 int ats_frame_warm_to_residual(ats_cloth* cloth, const ats_mlp* mlp, int fallback, double tol, const double* tols,
-                               int check_every, int max_iterations, int* iterations, double* residual, int* used,
-                               ats_stream stream);
+                               const int* first_check, int check_every, int max_iterations, int* iterations,
+                               double* residual, int* used, ats_stream stream);
 
 /* Message of the last failed call on this thread ("" if none). */
 const char* ats_last_error(void);

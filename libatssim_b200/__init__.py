@@ -134,9 +134,9 @@ _SIGNATURES = {
     "ats_mlp_train": [_vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_ulonglong, _fp, _vp],
     "ats_warm_start": [_vp, _vp, ctypes.c_int, _ip, _vp],
     "ats_frame_warm": [_vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp],
-    "ats_frame_warm_to_residual": [_vp, _vp, ctypes.c_int, ctypes.c_double, _dp, ctypes.c_int, ctypes.c_int, _ip, _dp,
-                                   _ip, _vp],
-    "ats_frame_to_residuals": [_vp, _dp, ctypes.c_int, ctypes.c_int, _ip, _dp, _vp],
+    "ats_frame_warm_to_residual": [_vp, _vp, ctypes.c_int, ctypes.c_double, _dp, _ip, ctypes.c_int, ctypes.c_int, _ip,
+                                   _dp, _ip, _vp],
+    "ats_frame_to_residuals": [_vp, _dp, _ip, ctypes.c_int, ctypes.c_int, _ip, _dp, _vp],
     "ats_energy_noalloc": [_vp, _vp, _vp, _vp, _vp, ctypes.c_int, _vp, _vp, ctypes.c_int, _vp, _vp, ctypes.c_int,
                            ctypes.c_float, ctypes.c_float, _fp, ctypes.c_float, _vp, _vp],
 }
@@ -418,16 +418,20 @@ class Cloth:
         _check(lib().ats_warm_start(self.h, mlp.h, int(fallback), _p(used, ctypes.c_int), _stream(stream)))
         return used
 
-    def frame_warm_to_residual(self, mlp, tol, fallback=True, check_every=10, max_iterations=1000, stream=None):
+    def frame_warm_to_residual(self, mlp, tol, fallback=True, check_every=10, max_iterations=1000, first_check=None,
+                               stream=None):
         """frame_to_residual with the learned guess; tol is a float or one value per
-        instance; returns (iterations, residual, used)."""
+        instance, first_check None or one first-probe iteration per instance; returns
+        (iterations, residual, used)."""
         n = self.info.num_instances
         it = np.zeros(n, dtype=np.int32)
         res = np.zeros(n, dtype=np.float64)
         used = np.zeros(n, dtype=np.int32)
         tols = None if np.isscalar(tol) else np.ascontiguousarray(tol, dtype=np.float64)
+        fc = None if first_check is None else np.ascontiguousarray(first_check, dtype=np.int32)
         _check(lib().ats_frame_warm_to_residual(self.h, mlp.h, int(fallback), float(tol) if tols is None else 0.0,
-                                                None if tols is None else _p(tols, ctypes.c_double), int(check_every),
+                                                None if tols is None else _p(tols, ctypes.c_double),
+                                                None if fc is None else _p(fc, ctypes.c_int), int(check_every),
                                                 int(max_iterations), _p(it, ctypes.c_int), _p(res, ctypes.c_double),
                                                 _p(used, ctypes.c_int), _stream(stream)))
         return it, res, used
@@ -438,20 +442,25 @@ class Cloth:
     def record_end(self, dataset, stream=None):
         _check(lib().ats_record_frame_end(self.h, dataset.h, _stream(stream)))
 
-    def frame_to_residual(self, tol, check_every=10, max_iterations=1000, stream=None):
+    def frame_to_residual(self, tol, check_every=10, max_iterations=1000, first_check=None, stream=None):
         """One frame iterated until every instance reaches ||grad G|| <= tol ||grad G(y)||
-        (or max_iterations); tol is a float or one value per instance; returns
-        (iterations per instance, relative residual per instance)."""
+        (or max_iterations); tol is a float or one value per instance, first_check None
+        or one first-probe iteration per instance; returns (iterations per instance,
+        relative residual per instance)."""
         n = self.info.num_instances
         it = np.zeros(n, dtype=np.int32)
         res = np.zeros(n, dtype=np.float64)
+        if first_check is not None and np.isscalar(tol):
+            tol = np.full(n, float(tol))
+        fc = None if first_check is None else np.ascontiguousarray(first_check, dtype=np.int32)
         if np.isscalar(tol):
             _check(lib().ats_frame_to_residual(self.h, float(tol), int(check_every), int(max_iterations),
                                                _p(it, ctypes.c_int), _p(res, ctypes.c_double), _stream(stream)))
         else:
             t = np.ascontiguousarray(tol, dtype=np.float64)
-            _check(lib().ats_frame_to_residuals(self.h, _p(t, ctypes.c_double), int(check_every), int(max_iterations),
-                                                _p(it, ctypes.c_int), _p(res, ctypes.c_double), _stream(stream)))
+            _check(lib().ats_frame_to_residuals(self.h, _p(t, ctypes.c_double), None if fc is None else _p(fc, ctypes.c_int),
+                                                int(check_every), int(max_iterations), _p(it, ctypes.c_int),
+                                                _p(res, ctypes.c_double), _stream(stream)))
         return it, res
 
     def energy(self, stream=None):

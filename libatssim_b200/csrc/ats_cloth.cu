@@ -300,6 +300,8 @@ __global__ void __launch_bounds__(kRedThreads) sum_partials3_kernel(const double
 //                 (x^T W x = -1/2 sum_{v,u} W_vu |x_u - x_v|^2);
 //   kEvalPotPair  out0[v], out1[v] = the shares of G(x) and G(y) with y the saved
 //                 inertial prediction (the inertia term of G(y) is 0).
+// kEvalGradF32 (stencil_grad32_kernel) is kEvalGrad with the per-vertex gradient in
+// the sweep's own FP32 arithmetic; only the sum over vertices is FP64.
 constexpr int kEvalGrad = 0, kEvalPot = 1, kEvalPotPair = 2;
 struct EvalArgs {
     const float4* x;
@@ -311,6 +313,7 @@ struct EvalArgs {
     const int2* st_iw;
     const float* st_rest;
     const int4* slices;
+    const int* slice_inst;
     int nslices;
     double h;
     double* out0;
@@ -357,6 +360,8 @@ __global__ void __launch_bounds__(128) stencil_eval_kernel(EvalArgs a) {
     const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     if (warp >= a.nslices) return;
     const int lane = threadIdx.x & 31;
+    // a slice belongs to one instance, so this exit is warp-uniform
+    if (a.active && !a.active[__ldg(&a.slice_inst[warp])]) return;
     const int4 sd = __ldg(&a.slices[warp]);
     const int rows = sd.w & 0xffff, erows = sd.w >> 16, brows = rows - erows;
     const int k = lane / TPV;
@@ -365,8 +370,6 @@ __global__ void __launch_bounds__(128) stencil_eval_kernel(EvalArgs a) {
     const int base = sd.z + lane;
     const int bbase = base + erows * 32;
     const float4 mv = __ldg(&a.vm[v]);
-    // a slice belongs to one instance, so this exit is warp-uniform
-    if (a.active && !a.active[__float_as_int(mv.w)]) return;
     int ue[RE], ub[RB];
     float we[RE], le[RE], wb[RB];
 #pragma unroll
@@ -473,9 +476,11 @@ cudaError_t stencil_eval_launch(int tpv, const EvalArgs& a, cudaStream_t st) {
 // block (chunk j, instance i) sums a fixed strided subset, then one block per
 // instance adds the kSegChunks partials in order.
 constexpr int kSegChunks = 32;
-__global__ void __launch_bounds__(kRedThreads) segment_partial_kernel(const double* g2, const int* seg, double* partial) {
+__global__ void __launch_bounds__(kRedThreads) segment_partial_kernel(const double* g2, const int* seg, double* partial,
+                                                                      const int* mask) {
     __shared__ double sh[kRedThreads];
     const int i = blockIdx.y, j = blockIdx.x;
+    if (mask && !mask[i]) return;  // block-uniform: the instance keeps its previous value
     const int b = seg[i], e = seg[i + 1];
     double v = 0.0;
     for (int t = b + j * kRedThreads + threadIdx.x; t < e; t += kSegChunks * kRedThreads) v += g2[t];
@@ -483,8 +488,10 @@ __global__ void __launch_bounds__(kRedThreads) segment_partial_kernel(const doub
     if (threadIdx.x == 0) partial[i * kSegChunks + j] = s;
 }
 
-__global__ void __launch_bounds__(kSegChunks) segment_final_kernel(const double* partial, double* out, int take_sqrt) {
+__global__ void __launch_bounds__(kSegChunks) segment_final_kernel(const double* partial, double* out, int take_sqrt,
+                                                                   const int* mask) {
     __shared__ double sh[kSegChunks];
+    if (mask && !mask[blockIdx.x]) return;
     double s = block_sum(partial[blockIdx.x * kSegChunks + threadIdx.x], sh);
     if (threadIdx.x == 0) out[blockIdx.x] = take_sqrt ? sqrt(s) : s;
 }
@@ -493,21 +500,30 @@ __global__ void __launch_bounds__(kSegChunks) segment_final_kernel(const double*
 // predict stores ||grad G(y)|| per instance; later calls deactivate an instance once
 // ||grad G(x)|| <= tol ||grad G(y)|| or its iteration cap is reached; n_active
 // receives the number of instances still iterating.
+// Bookkeeping of the residual-driven frame (one block). init: norm0 = ||grad G(y)||,
+// every instance with a nonzero gradient active. Otherwise, after `done` iterations:
+// every active instance has iters = done; an instance probed now (due) stops when
+// ||grad G|| <= tol ||grad G(y)|| or done >= max_iters. Then due is set for the next
+// probe point `next`: active instances with next == max_iters, or next >= first_i and
+// (next - first_i) a multiple of step (first_i = first[i], or step when first is null).
 __global__ void __launch_bounds__(256) residual_check_kernel(const double* norm, double* norm0, int* active, int* iters,
-                                                            int* n_active, int ninst, int first, int step,
-                                                            int max_iters, double tol, const double* tols) {
+                                                            int* n_active, int* due, int ninst, int init, int done,
+                                                            int next, int step, const int* first, int max_iters,
+                                                            double tol, const double* tols) {
     __shared__ int count[256];
     int c = 0;
     for (int i = threadIdx.x; i < ninst; i += blockDim.x) {
-        if (first) {
+        if (init) {
             norm0[i] = norm[i];
             active[i] = norm[i] > 0.0 && max_iters > 0 ? 1 : 0;
             iters[i] = 0;
         } else if (active[i]) {
-            iters[i] += step;
+            iters[i] = done;
             const double ti = tols ? tols[i] : tol;
-            if (norm[i] <= ti * norm0[i] || iters[i] >= max_iters) active[i] = 0;
+            if (due[i] && (norm[i] <= ti * norm0[i] || done >= max_iters)) active[i] = 0;
         }
+        const int f = first ? first[i] : step;
+        due[i] = active[i] && (next >= max_iters || (next >= f && (next - f) % step == 0)) ? 1 : 0;
         c += active[i];
     }
     count[threadIdx.x] = c;
@@ -553,7 +569,10 @@ int upload_stencil(ats_cloth* c) {
     if ((r = upload(c->st_iw, L.st_iw, L.st_rest.size())) || (r = upload(c->st_rest, L.st_rest, L.st_rest.size())) ||
         (r = upload(c->slices, L.slices, L.slices.size() / 4)))
         return r;
-    return ATS_OK;
+    // a slice lies in one instance: the instance id of its first vertex
+    std::vector<int> si(L.slices.size() / 4);
+    for (size_t k = 0; k < si.size(); ++k) std::memcpy(&si[k], &L.vm[4 * (size_t)L.slices[4 * k] + 3], sizeof(int));
+    return upload(c->slice_inst, si, si.size());
 }
 
 template <int TPV, int RE, int RB>
@@ -582,6 +601,7 @@ int launch_sweep(ats_cloth* c, int color, cudaStream_t st, const int* active) {
     a.st_iw = c->st_iw.p;
     a.st_rest = c->st_rest.p;
     a.slices = c->slices.p;
+    a.slice_inst = c->slice_inst.p;
     a.inst = c->inst.p;
     a.active = active;
     a.slice_begin = sb;
@@ -680,6 +700,7 @@ EvalArgs eval_args(ats_cloth* c) {
     a.st_iw = c->st_iw.p;
     a.st_rest = c->st_rest.p;
     a.slices = c->slices.p;
+    a.slice_inst = c->slice_inst.p;
     a.nslices = (int)c->slices.n;
     a.h = (double)c->h;
     a.out0 = a.out1 = nullptr;
@@ -687,21 +708,120 @@ EvalArgs eval_args(ats_cloth* c) {
     return a;
 }
 
-int segment_sum(ats_cloth* c, const double* per_vertex, double* out, int take_sqrt, cudaStream_t st) {
+int segment_sum(ats_cloth* c, const double* per_vertex, double* out, int take_sqrt, cudaStream_t st,
+                const int* mask = nullptr) {
     segment_partial_kernel<<<dim3(kSegChunks, c->L.ninst), kRedThreads, 0, st>>>(per_vertex, c->inst_seg.p,
-                                                                                   c->seg_partial.p);
+                                                                                   c->seg_partial.p, mask);
     ATS_CUDA(cudaGetLastError());
-    segment_final_kernel<<<c->L.ninst, kSegChunks, 0, st>>>(c->seg_partial.p, out, take_sqrt);
+    segment_final_kernel<<<c->L.ninst, kSegChunks, 0, st>>>(c->seg_partial.p, out, take_sqrt, mask);
     ATS_CUDA(cudaGetLastError());
     return ATS_OK;
 }
 
-int enqueue_residual_norms(ats_cloth* c, cudaStream_t st, const int* active) {
+// |grad_v G(x)|^2 per free vertex with the sweep's FP32 force arithmetic (vbd_edge,
+// vbd_bend and the inertia term of vbd_sweep_kernel: grad = -f); only the squared norm
+// and the sums over vertices are FP64. Used by the residual-driven frames, whose
+// probes run every few iterations: the gradient terms of a vertex are far from
+// cancelling at the residuals those frames stop at, so FP32 terms (as the reference
+// energy's) lose nothing there, and this kernel needs half the registers of the FP64
+// one.
+template <int TPV, int RE, int RB>
+__global__ void __launch_bounds__(128) stencil_grad32_kernel(EvalArgs a, float h, float h2inv) {
+    const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (warp >= a.nslices) return;
+    const int lane = threadIdx.x & 31;
+    if (a.active && !a.active[__ldg(&a.slice_inst[warp])]) return;  // warp-uniform
+    const int4 sd = __ldg(&a.slices[warp]);
+    const int rows = sd.w & 0xffff, erows = sd.w >> 16, brows = rows - erows;
+    const int k = lane / TPV;
+    const bool leader = k < sd.y && (lane % TPV) == 0;
+    const int v = sd.x + min(k, sd.y - 1);
+    const int base = sd.z + lane;
+    const int bbase = base + erows * 32;
+    int ue[RE], ub[RB];
+    float we[RE], le[RE], wb[RB];
+#pragma unroll
+    for (int r = 0; r < RE; ++r) {
+        ue[r] = v;
+        we[r] = 0.f;
+        le[r] = -1.f;
+        if (r < erows) {
+            const int2 iw = __ldg(&a.st_iw[base + r * 32]);
+            ue[r] = iw.x;
+            we[r] = __int_as_float(iw.y);
+            le[r] = __ldg(&a.st_rest[base + r * 32]);
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < RB; ++r) {
+        ub[r] = v;
+        wb[r] = 0.f;
+        if (r < brows) {
+            const int2 iw = __ldg(&a.st_iw[bbase + r * 32]);
+            ub[r] = iw.x;
+            wb[r] = __int_as_float(iw.y);
+        }
+    }
+    const float4 mv = __ldg(&a.vm[v]);
+    const float4 ip = __ldg(&a.inst[__float_as_int(mv.w)]);
+    const float4 xv = a.x[v];
+    float4 xe[RE], xb[RB];
+#pragma unroll
+    for (int r = 0; r < RE; ++r) xe[r] = a.x[ue[r]];
+#pragma unroll
+    for (int r = 0; r < RB; ++r) xb[r] = a.x[ub[r]];
+    float fx = 0.f, fy = 0.f, fz = 0.f, h00 = 0.f, h01 = 0.f, h02 = 0.f, h11 = 0.f, h12 = 0.f, h22 = 0.f;
+#pragma unroll
+    for (int r = 0; r < RE; ++r) vbd_edge(xv, xe[r], le[r], we[r], ip.w, fx, fy, fz, h00, h01, h02, h11, h12, h22);
+    for (int r = RE; r < erows; ++r) {
+        const int2 iw = __ldg(&a.st_iw[base + r * 32]);
+        vbd_edge(xv, a.x[iw.x], __ldg(&a.st_rest[base + r * 32]), __int_as_float(iw.y), ip.w, fx, fy, fz, h00, h01,
+                 h02, h11, h12, h22);
+    }
+#pragma unroll
+    for (int r = 0; r < RB; ++r) vbd_bend(xv, xb[r], wb[r], fx, fy, fz);
+    for (int r = RB; r < brows; ++r) {
+        const int2 iw = __ldg(&a.st_iw[bbase + r * 32]);
+        vbd_bend(xv, a.x[iw.x], __int_as_float(iw.y), fx, fy, fz);
+    }
+#pragma unroll
+    for (int o = TPV / 2; o > 0; o >>= 1) {
+        fx += __shfl_xor_sync(0xffffffffu, fx, o);
+        fy += __shfl_xor_sync(0xffffffffu, fy, o);
+        fz += __shfl_xor_sync(0xffffffffu, fz, o);
+    }
+    if (!leader) return;
+    if (mv.y != 0.f) {
+        a.out0[v] = 0.0;
+        return;
+    }
+    const float4 p0 = a.x0[v], vv = a.vel[v];
+    const float m = p0.w, mh = m * h2inv;
+    fx += -mh * ((xv.x - p0.x) - vv.x * h) + m * ip.x;
+    fy += -mh * ((xv.y - p0.y) - vv.y * h) + m * ip.y;
+    fz += -mh * ((xv.z - p0.z) - vv.z * h) + m * ip.z;
+    a.out0[v] = (double)fx * fx + (double)fy * fy + (double)fz * fz;
+}
+
+int enqueue_residual_norms(ats_cloth* c, cudaStream_t st, const int* active, bool fp32_terms) {
     EvalArgs a = eval_args(c);
     a.active = active;
     a.out0 = c->g2.p;
-    ATS_CUDA(stencil_eval_launch<kEvalGrad>(c->L.tpv, a, st));
-    return segment_sum(c, c->g2.p, c->red_out.p, 1, st);
+    if (fp32_terms) {
+        const int blocks = (a.nslices * 32 + 127) / 128;
+        if (blocks > 0) {
+            switch (c->L.tpv) {
+                case 1: stencil_grad32_kernel<1, 6, 6><<<blocks, 128, 0, st>>>(a, c->h, c->h2inv); break;
+                case 2: stencil_grad32_kernel<2, 3, 3><<<blocks, 128, 0, st>>>(a, c->h, c->h2inv); break;
+                case 4: stencil_grad32_kernel<4, 2, 2><<<blocks, 128, 0, st>>>(a, c->h, c->h2inv); break;
+                default: stencil_grad32_kernel<8, 1, 1><<<blocks, 128, 0, st>>>(a, c->h, c->h2inv); break;
+            }
+            ATS_CUDA(cudaGetLastError());
+        }
+    } else {
+        ATS_CUDA(stencil_eval_launch<kEvalGrad>(c->L.tpv, a, st));
+    }
+    return segment_sum(c, c->g2.p, c->red_out.p, 1, st, active);
 }
 
 int enqueue_potential_pair(ats_cloth* c, const float4* y, double* gx, double* gy, cudaStream_t st) {
@@ -726,8 +846,8 @@ int enqueue_potential(ats_cloth* c, double* g, cudaStream_t st) {
     return segment_sum(c, c->pot_vx.p, g, 0, st);
 }
 
-int frame_to_residual_impl(ats_cloth* c, double tol, const double* tols, int check_every, int max_iterations,
-                           int* iterations, double* residual, cudaStream_t st,
+int frame_to_residual_impl(ats_cloth* c, double tol, const double* tols, const int* first_check, int check_every,
+                           int max_iterations, int* iterations, double* residual, cudaStream_t st,
                            const std::function<int(cudaStream_t)>& after_predict) {
     if (!c || !(tol >= 0.0) || check_every <= 0 || max_iterations < 0) {
         set_error("frame to residual: need a handle, tol >= 0, check_every > 0, max_iterations >= 0");
@@ -741,35 +861,61 @@ int frame_to_residual_impl(ats_cloth* c, double tol, const double* tols, int che
         ATS_CUDA(cudaMemcpyAsync(c->tols.p, tols, ni * sizeof(double), cudaMemcpyHostToDevice, st));
         dtols = c->tols.p;
     }
+    if (!c->due.p) ATS_CUDA(c->due.alloc(ni));
+    // probe points: every iteration count at which some instance is due (the device
+    // skips instances that are not), and the cap
+    std::vector<char> point(max_iterations + 1, 0);
+    const int* dfirst = nullptr;
+    if (first_check) {
+        if (!c->first_check.p) ATS_CUDA(c->first_check.alloc(ni));
+        std::vector<int> f(ni);
+        for (int i = 0; i < ni; ++i) {
+            f[i] = std::max(1, first_check[i]);
+            for (int k = f[i]; k <= max_iterations; k += check_every) point[k] = 1;
+        }
+        ATS_CUDA(cudaMemcpyAsync(c->first_check.p, f.data(), ni * sizeof(int), cudaMemcpyHostToDevice, st));
+        ATS_CUDA(cudaStreamSynchronize(st));  // f leaves scope
+        dfirst = c->first_check.p;
+    } else {
+        for (int k = check_every; k <= max_iterations; k += check_every) point[k] = 1;
+    }
+    if (max_iterations > 0) point[max_iterations] = 1;
+    std::vector<int> points;
+    for (int k = 1; k <= max_iterations; ++k)
+        if (point[k]) points.push_back(k);
+    const int first_point = points.empty() ? 0 : points[0];
     for (int sub = 0; sub < c->prm.num_substep; ++sub) {
-        if ((r = launch_predict(c, st)) || (r = enqueue_residual_norms(c, st))) return r;
-        residual_check_kernel<<<1, 256, 0, st>>>(c->red_out.p, c->norm0.p, c->active.p, c->iters.p, c->n_active.p, ni,
-                                                  1, 0, max_iterations, tol, dtols);
-        ATS_CUDA(cudaGetLastError());
+        if ((r = launch_predict(c, st))) return r;
+        if ((r = enqueue_residual_norms(c, st, nullptr, true))) return r;
         if (after_predict && (r = after_predict(st))) return r;
-        // probes (residual + deactivation) run on the device every check_every
-        // iterations; the host looks at the number of active instances only every
-        // kProbesPerSync probes, so it rarely waits on the device
+        residual_check_kernel<<<1, 256, 0, st>>>(c->red_out.p, c->norm0.p, c->active.p, c->iters.p, c->n_active.p,
+                                                  c->due.p, ni, 1, 0, first_point, check_every, dfirst, max_iterations,
+                                                  tol, dtols);
+        ATS_CUDA(cudaGetLastError());
+        // probes run on the device; the host looks at the number of active instances
+        // only every kProbesPerSync probe points, so it rarely waits on the device
         constexpr int kProbesPerSync = 4;
-        int probes = 0;
-        for (int done = 0; done < max_iterations;) {
-            if (probes % kProbesPerSync == 0) {
+        int done = 0;
+        for (size_t p = 0; p < points.size(); ++p) {
+            if (p % kProbesPerSync == 0) {
                 ATS_CUDA(cudaMemcpyAsync(c->host_flag, c->n_active.p, sizeof(int), cudaMemcpyDeviceToHost, st));
                 ATS_CUDA(cudaStreamSynchronize(st));
                 if (*c->host_flag == 0) break;
             }
-            const int step = std::min(check_every, max_iterations - done);
-            if ((r = enqueue_iterations(c, ATS_SOLVER_VBD, step, st, c->active.p)) ||
-                (r = enqueue_residual_norms(c, st, c->active.p)))
+            const int k = points[p];
+            if ((r = enqueue_iterations(c, ATS_SOLVER_VBD, k - done, st, c->active.p)) ||
+                (r = enqueue_residual_norms(c, st, c->due.p, true)))
                 return r;
-            done += step;
-            ++probes;
-            residual_check_kernel<<<1, 256, 0, st>>>(c->red_out.p, c->norm0.p, c->active.p, c->iters.p, c->n_active.p,
-                                                      ni, 0, step, max_iterations, tol, dtols);
+            done = k;
+            const int next = p + 1 < points.size() ? points[p + 1] : max_iterations;
+            residual_check_kernel<<<1, 256, 0, st>>>(c->red_out.p, c->norm0.p, c->active.p, c->iters.p,
+                                                      c->n_active.p, c->due.p, ni, 0, done, next, check_every, dfirst,
+                                                      max_iterations, tol, dtols);
             ATS_CUDA(cudaGetLastError());
         }
         if (sub + 1 == c->prm.num_substep && (iterations || residual)) {
-            // report against the last substep: residual relative to ||grad G(y)||
+            // report against the last substep: residual relative to ||grad G(y)|| (the
+            // value of an instance's last probe)
             if (residual) {
                 std::vector<double> nrm(ni), n0(ni);
                 ATS_CUDA(cudaMemcpyAsync(nrm.data(), c->red_out.p, ni * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -1211,16 +1357,18 @@ int ats_frame_to_residual(ats_cloth* c, double tol, int check_every, int max_ite
         set_error("ats_frame_to_residual: null handle");
         return ATS_ERR_INVALID;
     }
-    return frame_to_residual_impl(c, tol, nullptr, check_every, max_iterations, iterations, residual, S(stream), nullptr);
+    return frame_to_residual_impl(c, tol, nullptr, nullptr, check_every, max_iterations, iterations, residual,
+                                  S(stream), nullptr);
 }
 
-int ats_frame_to_residuals(ats_cloth* c, const double* tols, int check_every, int max_iterations, int* iterations,
-                           double* residual, ats_stream stream) {
+int ats_frame_to_residuals(ats_cloth* c, const double* tols, const int* first_check, int check_every,
+                           int max_iterations, int* iterations, double* residual, ats_stream stream) {
     if (!c || !tols) {
         set_error("ats_frame_to_residuals: need a handle and one tolerance per instance");
         return ATS_ERR_INVALID;
     }
-    return frame_to_residual_impl(c, 0.0, tols, check_every, max_iterations, iterations, residual, S(stream), nullptr);
+    return frame_to_residual_impl(c, 0.0, tols, first_check, check_every, max_iterations, iterations, residual,
+                                  S(stream), nullptr);
 }
 
 int ats_residual(ats_cloth* c, double* out, ats_stream stream) {

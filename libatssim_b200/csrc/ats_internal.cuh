@@ -56,6 +56,7 @@ struct ats_cloth {
     DevBuf<int2> st_iw;
     DevBuf<float> st_rest;
     DevBuf<int4> slices;
+    DevBuf<int> slice_inst;  // instance of each slice
     DevBuf<int2> xs_edge;
     DevBuf<float> xs_rest, xs_k, xs_lambda;
     DevBuf<int4> xb_idx;
@@ -69,7 +70,7 @@ struct ats_cloth {
     DevBuf<float> io_x, io_v;  // caller-order staging of the state
     // scratch of the FP64 reductions
     DevBuf<double> partial, seg_partial, red_out, g2, norm0, tols;
-    DevBuf<int> active, iters, n_active;  // ats_frame_to_residual bookkeeping
+    DevBuf<int> active, iters, n_active, due, first_check;  // ats_frame_to_residual bookkeeping
     int* host_flag = nullptr;             // pinned copy of n_active
     // learned warm start (uploaded at create; the rest allocated on first use)
     DevBuf<int> feat_nb, inst_eseg, inst_bseg, free_list;
@@ -101,7 +102,7 @@ struct ats_cloth {
     }
     size_t device_bytes() const {
         return x.bytes() + x0.bytes() + vel.bytes() + vm.bytes() + inst.bytes() + st_iw.bytes() + st_rest.bytes() +
-               slices.bytes() + xs_edge.bytes() + xs_rest.bytes() + xs_k.bytes() + xs_lambda.bytes() +
+               slices.bytes() + slice_inst.bytes() + xs_edge.bytes() + xs_rest.bytes() + xs_k.bytes() + xs_lambda.bytes() +
                xb_idx.bytes() + xb_q.bytes() + xb_lambda.bytes() + en_edge.bytes() + en_rest.bytes() + en_k.bytes() +
                en_q.bytes() + en_kb.bytes() + en_bend.bytes() + inst_seg.bytes() + to_caller.bytes() + io_x.bytes() +
                io_v.bytes() + partial.bytes() +
@@ -118,18 +119,20 @@ int launch_predict(ats_cloth* c, cudaStream_t st);
 int launch_update(ats_cloth* c, cudaStream_t st);
 int launch_sweep(ats_cloth* c, int color, cudaStream_t st, const int* active = nullptr);
 int enqueue_iterations(ats_cloth* c, int solver, int iterations, cudaStream_t st, const int* active = nullptr);
-// FP64 ||grad G|| per instance into c->red_out.p; with `active`, instances whose flag
-// is 0 keep the per-vertex values of the previous call (their positions are frozen)
-int enqueue_residual_norms(ats_cloth* c, cudaStream_t st, const int* active = nullptr);
+// ||grad G|| per instance into c->red_out.p (FP64 throughout, or FP32 per-vertex terms
+// with FP64 sums); with `active`, instances whose flag is 0 keep their previous values
+int enqueue_residual_norms(ats_cloth* c, cudaStream_t st, const int* active = nullptr, bool fp32_terms = false);
 // Per instance, the FP64 incremental potential G of the current positions (gx) and of
 // y (gy), both against the inertial prediction y (ninst values each, device pointers).
 int enqueue_potential_pair(ats_cloth* c, const float4* y, double* gx, double* gy, cudaStream_t st);
 // Per instance, G(x) against the inertial prediction of the current frame start.
 int enqueue_potential(ats_cloth* c, double* g, cudaStream_t st);
-// ats_frame_to_residual with an optional hook run after ||grad G(y)|| is taken and
-// before the first iteration (the learned warm start replaces y there).
-int frame_to_residual_impl(ats_cloth* c, double tol, const double* tols, int check_every, int max_iterations,
-                           int* iterations, double* residual, cudaStream_t st,
+// ats_frame_to_residual(s) with an optional hook run after ||grad G(y)|| is taken and
+// before the first iteration (the learned warm start replaces y there). Probes use
+// FP32 per-vertex gradient terms and FP64 sums. first_check (host, per instance,
+// nullable) = iteration of an instance's first probe.
+int frame_to_residual_impl(ats_cloth* c, double tol, const double* tols, const int* first_check, int check_every,
+                           int max_iterations, int* iterations, double* residual, cudaStream_t st,
                            const std::function<int(cudaStream_t)>& after_predict);
 
 }  // namespace ats

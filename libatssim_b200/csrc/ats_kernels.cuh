@@ -33,6 +33,7 @@ struct SweepArgs {
     const int2* __restrict__ st_iw;
     const float* __restrict__ st_rest;
     const int4* __restrict__ slices;
+    const int* __restrict__ slice_inst;  // instance of each slice
     const float4* __restrict__ inst;
     const int* __restrict__ active;  // per instance, null = all active
     int slice_begin, slice_end;
@@ -113,6 +114,14 @@ __global__ void __launch_bounds__(256) vbd_sweep_kernel(SweepArgs a) {
     const int base = sd.z + lane;
     const int bbase = base + erows * 32;
 
+    // With an activity mask (written by the kernel before) the flag is read first,
+    // after the dependency wait, so that a converged instance costs one load per
+    // slice; without one, the constant data below is fetched before the wait.
+    if (a.active) {
+        grid_dependency_wait();
+        allow_dependent_launch();
+        if (!a.active[__ldg(&a.slice_inst[slice])]) return;
+    }
     // constant data: stencil rows, material, instance parameters
     int ue[RE], ub[RB];
     float we[RE], le[RE], wb[RB];
@@ -142,10 +151,10 @@ __global__ void __launch_bounds__(256) vbd_sweep_kernel(SweepArgs a) {
     const float4 ip = __ldg(&a.inst[__float_as_int(mv.w)]);
     const float ks = ip.w;
 
-    grid_dependency_wait();
-    allow_dependent_launch();
-    // a slice belongs to one instance: instances that have converged are skipped
-    if (a.active && !a.active[__float_as_int(mv.w)]) return;
+    if (!a.active) {
+        grid_dependency_wait();
+        allow_dependent_launch();
+    }
 
     // positions and frame-start state (ordered behind the previous kernel); the
     // neighbours belong to other colours, which this launch does not write

@@ -1178,14 +1178,14 @@ int ats_frame_warm(ats_cloth* c, const ats_mlp* m, int fallback, int iterations,
 }
 
 int ats_frame_warm_to_residual(ats_cloth* c, const ats_mlp* m, int fallback, double tol, const double* tols,
-                               int check_every, int max_iterations, int* iterations, double* residual, int* used,
-                               ats_stream stream) {
+                               const int* first_check, int check_every, int max_iterations, int* iterations,
+                               double* residual, int* used, ats_stream stream) {
     if (!c || !m) {
         set_error("ats_frame_warm_to_residual: need a handle and a model");
         return ATS_ERR_INVALID;
     }
     cudaStream_t st = S(stream);
-    int r = frame_to_residual_impl(c, tol, tols, check_every, max_iterations, iterations, residual, st,
+    int r = frame_to_residual_impl(c, tol, tols, first_check, check_every, max_iterations, iterations, residual, st,
                                    [&](cudaStream_t s) { return enqueue_warm_start(c, m, fallback, s); });
     if (r) return r;
     if (used) {

@@ -11,8 +11,10 @@ Everything runs through the C ABI; this module only sequences the calls.
                     its per-instance residual r_plain = ||grad G(x)|| / ||grad G(y)||
                     (the same sweeps replayed untimed) is the target;
            learned  predict, learned guess (potential fallback per instance), then
-                    iterations until each instance reaches its r_plain (checked every
-                    `check_every`), at most `iters`; converged instances are skipped.
+                    iterations until each instance reaches its r_plain, at most `iters`;
+                    converged instances are skipped. An instance is first probed at
+                    its previous frame's iteration count minus `lead` (with `schedule`),
+                    then every `check_every`.
            Frame times are CUDA-event times of each whole frame (host checks included).
 """
 import time
@@ -49,7 +51,8 @@ def train(dataset, steps=3000, batch=8192, seed=0):
     return m, loss, time.perf_counter() - t
 
 
-def evaluate(cloth, insts, model, iters, seed0, trajectories=2, frames=40, skip=15, check_every=5, stream=None):
+def evaluate(cloth, insts, model, iters, seed0, trajectories=2, frames=40, skip=15, check_every=5, schedule=True,
+             lead=0, stream=None):
     """Per evaluated frame: plain and learned frame times, iterations, residuals,
     and the FP64 incremental potential reached by both."""
     import torch
@@ -58,6 +61,7 @@ def evaluate(cloth, insts, model, iters, seed0, trajectories=2, frames=40, skip=
     st = stream if stream is not None else torch.cuda.current_stream()
     out = {"plain_ms": [], "learned_ms": [], "learned_iters": [], "used": [], "g_plain": [], "g_learned": [],
            "r_plain": [], "r_learned": []}
+    prev = None  # iterations of the previous learned frame, per instance
     for t in range(trajectories):
         cloth.set_state(x_rest, np.zeros_like(x_rest))
         for f in range(frames):
@@ -80,8 +84,10 @@ def evaluate(cloth, insts, model, iters, seed0, trajectories=2, frames=40, skip=
                 # learned: guess, then iterations until every instance reaches r_plain
                 torch.cuda.synchronize()
                 e0.record(st)
+                first = None if (prev is None or not schedule) else np.maximum(1, prev - lead)
                 its, r_l, used = cloth.frame_warm_to_residual(model, r_plain, check_every=check_every,
-                                                              max_iterations=iters, stream=st)
+                                                              max_iterations=iters, first_check=first, stream=st)
+                prev = its.copy()
                 e1.record(st)
                 torch.cuda.synchronize()
                 out["learned_ms"].append(e0.elapsed_time(e1))
