@@ -336,9 +336,9 @@ def run_learned(args):
         desc = "c3: 128x128 cloth, wind per frame, 200 iterations; MLP trained on 2000 plain frames (seeds 0-1999)"
     else:
         insts, prm = configs.c4()
-        trajectories, frames, eval_traj, eval_frames, skip = 2, 10, 1, 30, 10
+        trajectories, frames, eval_traj, eval_frames, skip = 2, 30, 1, 30, 10
         desc = ("c4: 64 batched cloths, side U{64..512}, wind per instance, 50 iterations; shared MLP trained on "
-                "20 plain frames of the batch")
+                "60 plain frames of the batch")
     iters = prm["iterations"]
     cloth = ats.Cloth(insts, **prm)
     cloth.autotune(iterations=3)
@@ -348,14 +348,16 @@ def run_learned(args):
     learned.record(cloth, insts, ds, trajectories, frames, iters, seed0=0)
     torch.cuda.synchronize()
     t_record = time.perf_counter() - t
-    model, loss, t_train = learned.train(ds, steps=4000)
+    model, loss, t_train = learned.train(ds)
     ds.close()
-    check_every = 5 if args.workload == "c3" else 10
+    # probes: c3 from each frame's previous count minus 3, then every 5; c4 every 10
+    check_every, schedule = (5, True) if args.workload == "c3" else (10, False)
     res = learned.evaluate(cloth, insts, model, iters, seed0=10000, trajectories=eval_traj, frames=eval_frames,
-                           skip=skip, check_every=check_every)
+                           skip=skip, check_every=check_every, schedule=schedule, lead=3)
     per_instance = learned.plain_per_instance_ms(insts, prm) if args.workload == "c4" else None
     sm = learned.summary(res, iters, per_instance)
     sm["check_every"] = check_every
+    sm["probe_schedule"] = "previous frame's count - 3, then every 5" if schedule else "every 10"
     # fixed budget: the 95th percentile of the iterations the to-residual frames needed,
     # measured on fresh frames (seed0 20000) as a CUDA graph
     budget = int(min(iters, 5 * np.ceil(np.percentile(res["learned_iters"], 95) / 5.0)))

@@ -42,12 +42,15 @@ def record(cloth, insts, dataset, trajectories, frames, iters, seed0):
             cloth.update_velocity()
 
 
-def train(dataset, steps=3000, batch=8192, seed=0):
+def train(dataset, steps=150000, batch=32768, lr=2e-3, seed=0):
+    """Normalisation from the data, then Adam: half the steps at lr, a quarter at lr/3,
+    a quarter at lr/10. Returns (model, mean loss of the last steps, seconds)."""
     m = MLP(seed=seed)
     m.fit_normalization(dataset)
     t = time.perf_counter()
-    loss = m.train(dataset, steps=int(steps * 0.75), batch=batch, lr=1e-3, seed=seed)
-    loss = m.train(dataset, steps=steps - int(steps * 0.75), batch=batch, lr=3e-4, seed=seed + 1)
+    m.train(dataset, steps=steps // 2, batch=batch, lr=lr, seed=seed)
+    m.train(dataset, steps=steps // 4, batch=batch, lr=lr / 3, seed=seed + 1)
+    loss = m.train(dataset, steps=steps - steps // 2 - steps // 4, batch=batch, lr=lr / 10, seed=seed + 2)
     return m, loss, time.perf_counter() - t
 
 
