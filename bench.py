@@ -350,14 +350,16 @@ def run_learned(args):
     t_record = time.perf_counter() - t
     model, loss, t_train = learned.train(ds)
     ds.close()
-    # probes: c3 from each frame's previous count minus 3, then every 5; c4 every 10
-    check_every, schedule = (5, True) if args.workload == "c3" else (10, False)
+    # probes every 5 iterations, the first one at the previous frame's count minus 3
+    # (c3) or at the 75th percentile of the previous frame's counts (c4)
+    check_every, schedule = (5, "prev") if args.workload == "c3" else (5, 75)
     res = learned.evaluate(cloth, insts, model, iters, seed0=10000, trajectories=eval_traj, frames=eval_frames,
                            skip=skip, check_every=check_every, schedule=schedule, lead=3)
     per_instance = learned.plain_per_instance_ms(insts, prm) if args.workload == "c4" else None
     sm = learned.summary(res, iters, per_instance)
     sm["check_every"] = check_every
-    sm["probe_schedule"] = "previous frame's count - 3, then every 5" if schedule else "every 10"
+    sm["probe_schedule"] = ("first at the previous frame's count - 3, then every 5" if schedule == "prev" else
+                            "first at the 75th percentile of the previous frame's counts, then every 5")
     # fixed budget: the 95th percentile of the iterations the to-residual frames needed,
     # measured on fresh frames (seed0 20000) as a CUDA graph
     budget = int(min(iters, 5 * np.ceil(np.percentile(res["learned_iters"], 95) / 5.0)))
@@ -367,7 +369,12 @@ def run_learned(args):
     if per_instance is not None:
         fx["speedup_vs_unbatched"] = fx["learned_fixed_fps"] * per_instance / 1e3
     sm["fixed_budget"] = fx
-    best = max(sm["learned_fps"], sm["fixed_budget"]["learned_fixed_fps"])
+    # the fixed-budget graph counts only when every instance of every evaluated frame
+    # reached the plain residual; the residual-driven frames always do
+    best = sm["learned_fps"]
+    if fx["reached_plain_residual_fraction"] >= 1.0:
+        best = max(best, fx["learned_fixed_fps"])
+    sm["headline_arm"] = "fixed_budget" if best != sm["learned_fps"] else "to_residual"
     out = {"metric": METRIC, "value": best, "unit": UNIT, "n_gpus": 1, "steps": sm["frames"],
            "warmup": skip, "ms_per_step": 1e3 / best, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32 (MLP bf16 / fp32 accumulate)", "data": "synthetic",

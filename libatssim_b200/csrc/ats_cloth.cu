@@ -897,7 +897,7 @@ int frame_to_residual_impl(ats_cloth* c, double tol, const double* tols, const i
         constexpr int kProbesPerSync = 4;
         int done = 0;
         for (size_t p = 0; p < points.size(); ++p) {
-            if (p % kProbesPerSync == 0) {
+            if (p > 0 && p % kProbesPerSync == 0) {  // nothing has been probed before the first point
                 ATS_CUDA(cudaMemcpyAsync(c->host_flag, c->n_active.p, sizeof(int), cudaMemcpyDeviceToHost, st));
                 ATS_CUDA(cudaStreamSynchronize(st));
                 if (*c->host_flag == 0) break;

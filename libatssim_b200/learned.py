@@ -12,9 +12,10 @@ Everything runs through the C ABI; this module only sequences the calls.
                     (the same sweeps replayed untimed) is the target;
            learned  predict, learned guess (potential fallback per instance), then
                     iterations until each instance reaches its r_plain, at most `iters`;
-                    converged instances are skipped. An instance is first probed at
-                    its previous frame's iteration count minus `lead` (with `schedule`),
-                    then every `check_every`.
+                    converged instances are skipped. Probes every `check_every`, the
+                    first one (schedule) at the instance's previous-frame count minus
+                    `lead` ("prev") or at a percentile of all previous-frame counts
+                    (a number), or at check_every (None).
            Frame times are CUDA-event times of each whole frame (host checks included).
 """
 import time
@@ -54,7 +55,7 @@ def train(dataset, steps=150000, batch=32768, lr=2e-3, seed=0):
     return m, loss, time.perf_counter() - t
 
 
-def evaluate(cloth, insts, model, iters, seed0, trajectories=2, frames=40, skip=15, check_every=5, schedule=False,
+def evaluate(cloth, insts, model, iters, seed0, trajectories=2, frames=40, skip=15, check_every=5, schedule=None,
              lead=2, stream=None):
     """Per evaluated frame: plain and learned frame times, iterations, residuals,
     and the FP64 incremental potential reached by both."""
@@ -87,7 +88,11 @@ def evaluate(cloth, insts, model, iters, seed0, trajectories=2, frames=40, skip=
                 # learned: guess, then iterations until every instance reaches r_plain
                 torch.cuda.synchronize()
                 e0.record(st)
-                first = None if (prev is None or not schedule) else np.maximum(1, prev - lead)
+                first = None
+                if prev is not None and schedule == "prev":
+                    first = np.maximum(1, prev - lead)
+                elif prev is not None and schedule is not None:
+                    first = np.full(len(prev), max(1, int(np.percentile(prev, schedule))), dtype=np.int32)
                 torch.cuda.nvtx.range_push("learned_frame")  # lets a profiler select these kernels
                 its, r_l, used = cloth.frame_warm_to_residual(model, r_plain, check_every=check_every,
                                                               max_iterations=iters, first_check=first, stream=st)
