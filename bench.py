@@ -161,16 +161,21 @@ def run_reference(args):
     print(json.dumps(out), flush=True)
 
 
-def profile_traffic():
-    """dram bytes per sweep launch from the committed ncu summary, if any."""
+def profile_traffic(alg_bytes):
+    """DRAM bytes per sweep launch from the committed ncu summary of the c1 sweep
+    (cold and warm-in-frame), scaled to a launch of `alg_bytes` algorithmic bytes
+    when the workload is another one (traffic grows with the vertices swept)."""
     p = os.path.join(ROOT, "profiles", "vbd_sweep_c1_ncu.json")
-    if os.path.exists(p):
-        try:
-            d = json.load(open(p))
-            return d.get("dram_bytes_per_launch"), d.get("dram_bytes_per_launch_warm")
-        except Exception:
-            return None, None
-    return None, None
+    if not os.path.exists(p):
+        return None, None, None
+    try:
+        d = json.load(open(p))
+        scale = alg_bytes / d["alg_bytes_per_launch"]
+        src = "ncu capture of this launch" if abs(scale - 1.0) < 1e-9 else \
+            "ncu capture of the c1 sweep (512^2), scaled by algorithmic bytes"
+        return d["dram_bytes_per_launch"] * scale, d["dram_bytes_per_launch_warm"] * scale, src
+    except Exception:
+        return None, None, None
 
 
 def run_ours(args):
@@ -279,7 +284,7 @@ def run_ours(args):
     e2e_s = float(sharding.allreduce_stats([e2e_s], op="max")[0])
     state_bytes = 2 * 3 * 4 * info.num_verts
 
-    traffic = profile_traffic()
+    traffic = profile_traffic(bytes_launch)
     out = None
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -299,6 +304,7 @@ def run_ours(args):
                        "d2h_bytes_per_step": state_bytes},
                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                             "frac": achieved / peak, "traffic": traffic[0], "traffic_warm_in_frame": traffic[1],
+                            "traffic_source": traffic[2],
                             "kernel": f"vbd_sweep_kernel<{info.threads_per_vertex}>", "mean_launch_us": mean_sweep_ms * 1e3,
                             "alg_bytes_per_launch": bytes_launch, "peak_source": peak_src},
                "gpu_launches": args.steps * (2 + ITERS * info.num_vertex_colors),
@@ -353,10 +359,13 @@ def run_learned(args):
     # probes every 5 iterations, the first one at the previous frame's count minus 3
     # (c3) or at the 75th percentile of the previous frame's counts (c4)
     check_every, schedule = (5, "prev") if args.workload == "c3" else (5, 75)
+    clocks = ClockSampler(local)
+    clocks.start()
     res = learned.evaluate(cloth, insts, model, iters, seed0=10000, trajectories=eval_traj, frames=eval_frames,
                            skip=skip, check_every=check_every, schedule=schedule, lead=3)
     per_instance = learned.plain_per_instance_ms(insts, prm) if args.workload == "c4" else None
     sm = learned.summary(res, iters, per_instance)
+    clk = clocks.stop()
     sm["check_every"] = check_every
     sm["probe_schedule"] = ("first at the previous frame's count - 3, then every 5" if schedule == "prev" else
                             "first at the 75th percentile of the previous frame's counts, then every 5")
@@ -380,6 +389,7 @@ def run_learned(args):
            "vs_baseline": None, "dtype": "f32 (MLP bf16 / fp32 accumulate)", "data": "synthetic",
            "config": {"workload": desc, "instances": cloth.info.num_instances, "vertices": nv,
                       "iterations": iters, "threads_per_vertex": cloth.info.threads_per_vertex},
+           "clocks": clk,
            "target": "each instance's relative residual after the plain solver's iteration budget "
                      "(a 1e-4 residual is not reached by plain VBD on these cloths within thousands of iterations)",
            "learned_vs_plain": sm, "train": {"samples": trajectories * frames * nv, "record_s": t_record,

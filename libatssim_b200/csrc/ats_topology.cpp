@@ -621,10 +621,13 @@ int ats_obj_read(const char* path, int* num_verts, float* positions, int* num_fa
                 int idx = std::atoi(tok.c_str());
                 ids.push_back(idx > 0 ? idx - 1 : (int)(p.size() / 3) + idx);
             }
-            if (ids.size() >= 3 && ids[0] != ids[1] && ids[0] != ids[2] && ids[1] != ids[2]) {
-                f.push_back(ids[0]);
-                f.push_back(ids[1]);
-                f.push_back(ids[2]);
+            // polygons become a fan from their first vertex; degenerate triangles are dropped
+            for (size_t k = 2; k < ids.size(); ++k) {
+                const int a = ids[0], b = ids[k - 1], c = ids[k];
+                if (a == b || a == c || b == c) continue;
+                f.push_back(a);
+                f.push_back(b);
+                f.push_back(c);
             }
         }
     }

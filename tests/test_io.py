@@ -33,3 +33,15 @@ def test_state_roundtrip_and_checks(ats, tmp_path):
     open(p, "wb").write(b"NOPE" + bytes(20))
     with pytest.raises(ats.AtsError, match="not a cloth state"):
         ats.state_read(p)
+
+
+def test_obj_polygons_become_triangle_fans(ats, tmp_path):
+    # a quad, a pentagon with texture/normal indices, a negative (relative) index face
+    # and a degenerate triangle that is dropped
+    p = tmp_path / "poly.obj"
+    p.write_text("v 0 0 0\nv 1 0 0\nv 1 0 1\nv 0 0 1\nv 2 0 0\nv 2 0 1\n"
+                 "f 1 2 3 4\nf 2/1/1 5/2/1 6/3/1 3/4/1 1/5/1\nf -1 -2 -3\nf 1 1 2\n")
+    pos, faces = ats.obj_read(str(p))
+    assert pos.shape == (6, 3)
+    expect = [[0, 1, 2], [0, 2, 3], [1, 4, 5], [1, 5, 2], [1, 2, 0], [5, 4, 3]]
+    assert faces.tolist() == expect
