@@ -362,6 +362,14 @@ class Cloth:
         _check(lib().ats_get_state(self.h, _p(x, ctypes.c_float), _p(v, ctypes.c_float), _stream(stream)))
         return x, v
 
+    def state_into(self, x, v, stream=None):
+        """ats_get_state into caller arrays (C-contiguous float32 (V, 3), e.g. views of
+        pinned host memory, which the copies then reach at full bus speed)."""
+        for a in (x, v):
+            if a.dtype != np.float32 or not a.flags.c_contiguous or a.shape != (self.nv, 3):
+                raise ValueError("state_into needs C-contiguous float32 arrays of shape (num_verts, 3)")
+        _check(lib().ats_get_state(self.h, _p(x, ctypes.c_float), _p(v, ctypes.c_float), _stream(stream)))
+
     def positions(self, stream=None):
         x = np.zeros((self.nv, 3), dtype=np.float32)
         _check(lib().ats_get_positions(self.h, _p(x, ctypes.c_float), _stream(stream)))
