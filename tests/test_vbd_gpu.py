@@ -361,3 +361,55 @@ def test_frame_probe_residual_matches_fp64_residual(ats):
     cloth.vbd_iterations(6)
     r64 = cloth.residual() / n_y
     assert np.allclose(r_frame, r64, rtol=2e-4, atol=0), (r_frame, r64)
+
+
+def _fan_instance(ats, k=40):
+    """A fan of k triangles around one vertex: the centre has k edge neighbours, far
+    more stencil rows than the sweep loads up front."""
+    t = np.linspace(0.0, 2 * np.pi, k, endpoint=False)
+    pos = np.concatenate([[[0.0, 0.0, 0.0]], np.stack([0.3 * np.cos(t), 0.02 * np.sin(3 * t), 0.3 * np.sin(t)], 1)])
+    pos = pos.astype(np.float32)
+    faces = np.array([[0, 1 + i, 1 + (i + 1) % k] for i in range(k)], dtype=np.int32)
+    fixed = np.zeros(k + 1, dtype=np.uint8)
+    fixed[[1, 1 + k // 2]] = 1
+    mass = ats.mass_area_weighted(pos, faces, 0.05)
+    return ats.Instance(pos, faces, mass, fixed, 500.0, 5e-3)
+
+
+def _ragged_instance(ats):
+    """An 8 x 8 grid with a third face on one interior edge (non-manifold), an
+    isolated vertex and a detached triangle."""
+    pos, faces = ats.grid_mesh(8)
+    nv = pos.shape[0]
+    a, b = 3 * 8 + 3, 3 * 8 + 4  # an interior edge of the grid
+    flap = (pos[a] + pos[b]) / 2 + np.array([0.0, 0.08, 0.0], dtype=np.float32)
+    extra = np.array([flap, [0.5, 0.3, 0.5], [1.3, 0.0, 0.0], [1.4, 0.0, 0.0], [1.3, 0.0, 0.1]], dtype=np.float32)
+    pos = np.concatenate([pos, extra]).astype(np.float32)
+    faces = np.concatenate([faces, [[a, b, nv], [nv + 2, nv + 3, nv + 4]]]).astype(np.int32)
+    fixed = np.zeros(pos.shape[0], dtype=np.uint8)
+    fixed[[0, 7]] = 1
+    mass = ats.mass_area_weighted(pos, faces, 0.1)
+    return ats.Instance(pos, faces, mass, fixed, 1e3, 1e-2)
+
+
+@pytest.mark.parametrize("mesh", ["fan", "ragged"])
+def test_irregular_meshes_match_oracle(ats, oracle, mesh):
+    inst = _fan_instance(ats) if mesh == "fan" else _ragged_instance(ats)
+    prm = dict(implicit_dt=1.0 / 60.0, num_substep=1, iterations=30, damping=2.0)
+    s = oracle_scene(oracle, inst, prm)
+    s.run(10)
+    xo, _ = s.state()
+    for tpv in (1, 8):
+        cloth = ats.Cloth([inst], threads_per_vertex=tpv, **prm)
+        for _ in range(10):
+            cloth.frame()
+        xg, _ = cloth.state()
+        assert np.isfinite(xg).all()
+        assert rel_l2(xg, xo) < 1e-4, (mesh, tpv, rel_l2(xg, xo))
+    # XPBD rounds every term as the oracle does
+    sx = oracle_scene(oracle, inst, prm)
+    sx.run(10, solver="xpbd")
+    cx = ats.Cloth([inst], **prm)
+    for _ in range(10):
+        cx.frame(ats.SOLVER_XPBD)
+    assert rel_l2(cx.state()[0], sx.state()[0]) < 1e-6
