@@ -51,38 +51,109 @@ __device__ __forceinline__ void allow_dependent_launch() { asm volatile("griddep
 // term -w d to the force f and the symmetric Hessian h:
 // f += k C d / l, He = k/l^2 d d^T + k max(1 - L/l, 0) (I - d d^T / l^2),
 // with l = max(|d|, FLT_EPSILON) as VBD::compute_stretch_mass_spring.
+// Every operation is an explicitly rounded intrinsic (fmaf / __fmul_rn / __fadd_rn),
+// which the compiler never fuses or reorders: the sweep kernels, whatever their
+// launch shape, compute bit-identical results.
 __device__ __forceinline__ void vbd_edge(float4 xv, float4 xu, float L, float w, float ks, float& fx, float& fy,
                                          float& fz, float& h00, float& h01, float& h02, float& h11, float& h12,
                                          float& h22) {
-    const float dx = xu.x - xv.x, dy = xu.y - xv.y, dz = xu.z - xv.z;
-    fx -= w * dx;
-    fy -= w * dy;
-    fz -= w * dz;
+    const float dx = __fsub_rn(xu.x, xv.x), dy = __fsub_rn(xu.y, xv.y), dz = __fsub_rn(xu.z, xv.z);
+    fx = fmaf(-w, dx, fx);
+    fy = fmaf(-w, dy, fy);
+    fz = fmaf(-w, dz, fz);
     if (L >= 0.f) {
-        const float l2 = dx * dx + dy * dy + dz * dz;
+        const float l2 = fmaf(dx, dx, fmaf(dy, dy, __fmul_rn(dz, dz)));
         const float inv = rsqrtf(fmaxf(l2, kEps * kEps));
-        const float l = fmaxf(l2 * inv, kEps);
-        const float kc = ks * (l - L) * inv;
-        fx += kc * dx;
-        fy += kc * dy;
-        fz += kc * dz;
-        const float xsq = inv * inv;
-        const float b = ks * fmaxf(1.f - L * inv, 0.f);
-        const float c = (ks - b) * xsq;
-        h00 += c * dx * dx + b;
-        h01 += c * dx * dy;
-        h02 += c * dx * dz;
-        h11 += c * dy * dy + b;
-        h12 += c * dy * dz;
-        h22 += c * dz * dz + b;
+        const float l = fmaxf(__fmul_rn(l2, inv), kEps);
+        const float kc = __fmul_rn(__fmul_rn(ks, __fsub_rn(l, L)), inv);
+        fx = fmaf(kc, dx, fx);
+        fy = fmaf(kc, dy, fy);
+        fz = fmaf(kc, dz, fz);
+        const float xsq = __fmul_rn(inv, inv);
+        const float b = __fmul_rn(ks, fmaxf(fmaf(-L, inv, 1.f), 0.f));
+        const float c = __fmul_rn(__fsub_rn(ks, b), xsq);
+        const float cx = __fmul_rn(c, dx), cy = __fmul_rn(c, dy);
+        h00 = __fadd_rn(h00, fmaf(cx, dx, b));
+        h01 = fmaf(cx, dy, h01);
+        h02 = fmaf(cx, dz, h02);
+        h11 = __fadd_rn(h11, fmaf(cy, dy, b));
+        h12 = fmaf(cy, dz, h12);
+        h22 = __fadd_rn(h22, fmaf(__fmul_rn(c, dz), dz, b));
     }
 }
 
 // Bending-only neighbour: quadratic bending in relative coordinates, -w (x_u - x_v).
 __device__ __forceinline__ void vbd_bend(float4 xv, float4 xu, float w, float& fx, float& fy, float& fz) {
-    fx -= w * (xu.x - xv.x);
-    fy -= w * (xu.y - xv.y);
-    fz -= w * (xu.z - xv.z);
+    fx = fmaf(-w, __fsub_rn(xu.x, xv.x), fx);
+    fy = fmaf(-w, __fsub_rn(xu.y, xv.y), fy);
+    fz = fmaf(-w, __fsub_rn(xu.z, xv.z), fz);
+}
+
+// The per-vertex part of a sweep, shared by both sweep kernels: the RE + RB gathered
+// neighbours (rows beyond them go through loops), the lane reduction, inertia and the
+// guarded 3x3 solve; the leader lane of a vertex writes x.
+template <int TPV, int RE, int RB>
+__device__ __forceinline__ void sweep_vertex(const SweepArgs& a, int v, bool leader, int base, int bbase, int erows,
+                                             int brows, float4 xv, const float4 (&xe)[RE], const float (&le)[RE],
+                                             const float (&we)[RE], const float4 (&xb)[RB], const float (&wb)[RB],
+                                             float ks, float4 ip, float4 mv, float4 p0, float4 vv) {
+    float fx = 0.f, fy = 0.f, fz = 0.f;
+    float h00 = 0.f, h01 = 0.f, h02 = 0.f, h11 = 0.f, h12 = 0.f, h22 = 0.f;
+#pragma unroll
+    for (int r = 0; r < RE; ++r) vbd_edge(xv, xe[r], le[r], we[r], ks, fx, fy, fz, h00, h01, h02, h11, h12, h22);
+    for (int r = RE; r < erows; ++r) {
+        const int2 iw = __ldg(&a.st_iw[base + r * 32]);
+        vbd_edge(xv, a.x[iw.x], __ldg(&a.st_rest[base + r * 32]), __int_as_float(iw.y), ks, fx, fy, fz, h00, h01, h02,
+                 h11, h12, h22);
+    }
+#pragma unroll
+    for (int r = 0; r < RB; ++r) vbd_bend(xv, xb[r], wb[r], fx, fy, fz);
+    for (int r = RB; r < brows; ++r) {
+        const int2 iw = __ldg(&a.st_iw[bbase + r * 32]);
+        vbd_bend(xv, a.x[iw.x], __int_as_float(iw.y), fx, fy, fz);
+    }
+    // reduce the TPV lanes of a vertex
+#pragma unroll
+    for (int o = TPV / 2; o > 0; o >>= 1) {
+        fx = __fadd_rn(fx, __shfl_xor_sync(0xffffffffu, fx, o));
+        fy = __fadd_rn(fy, __shfl_xor_sync(0xffffffffu, fy, o));
+        fz = __fadd_rn(fz, __shfl_xor_sync(0xffffffffu, fz, o));
+        h00 = __fadd_rn(h00, __shfl_xor_sync(0xffffffffu, h00, o));
+        h01 = __fadd_rn(h01, __shfl_xor_sync(0xffffffffu, h01, o));
+        h02 = __fadd_rn(h02, __shfl_xor_sync(0xffffffffu, h02, o));
+        h11 = __fadd_rn(h11, __shfl_xor_sync(0xffffffffu, h11, o));
+        h12 = __fadd_rn(h12, __shfl_xor_sync(0xffffffffu, h12, o));
+        h22 = __fadd_rn(h22, __shfl_xor_sync(0xffffffffu, h22, o));
+    }
+    if (!leader) return;
+
+    // inertia: H += m/h^2 I (+1e9 I pinned), f += -m/h^2 ((x - x0) - v h) + m a
+    const float m = p0.w;
+    const float mh = __fmul_rn(m, a.h2inv);
+    fx = __fadd_rn(fx, fmaf(-mh, fmaf(-vv.x, a.h, __fsub_rn(xv.x, p0.x)), __fmul_rn(m, ip.x)));
+    fy = __fadd_rn(fy, fmaf(-mh, fmaf(-vv.y, a.h, __fsub_rn(xv.y, p0.y)), __fmul_rn(m, ip.y)));
+    fz = __fadd_rn(fz, fmaf(-mh, fmaf(-vv.z, a.h, __fsub_rn(xv.z, p0.z)), __fmul_rn(m, ip.z)));
+    const float dg = __fadd_rn(__fadd_rn(mh, mv.y), mv.x);
+    h00 = __fadd_rn(h00, dg);
+    h11 = __fadd_rn(h11, dg);
+    h22 = __fadd_rn(h22, dg);
+
+    // symmetric 3x3 solve by adjugate / determinant, guarded by |det| > FLT_EPSILON
+    const float c00 = fmaf(h11, h22, -__fmul_rn(h12, h12));
+    const float c01 = fmaf(h02, h12, -__fmul_rn(h01, h22));
+    const float c02 = fmaf(h01, h12, -__fmul_rn(h02, h11));
+    const float det = fmaf(h00, c00, fmaf(h01, c01, __fmul_rn(h02, c02)));
+    if (fabsf(det) > kEps) {
+        const float c11 = fmaf(h00, h22, -__fmul_rn(h02, h02));
+        const float c12 = fmaf(h01, h02, -__fmul_rn(h00, h12));
+        const float c22 = fmaf(h00, h11, -__fmul_rn(h01, h01));
+        const float id = __fdiv_rn(1.f, det);
+        float4 xn = xv;
+        xn.x = fmaf(fmaf(c00, fx, fmaf(c01, fy, __fmul_rn(c02, fz))), id, xv.x);
+        xn.y = fmaf(fmaf(c01, fx, fmaf(c11, fy, __fmul_rn(c12, fz))), id, xv.y);
+        xn.z = fmaf(fmaf(c02, fx, fmaf(c12, fy, __fmul_rn(c22, fz))), id, xv.z);
+        a.x[v] = xn;
+    }
 }
 
 // One VBD colour sweep: for every vertex of the colour, inertia + mass-spring
@@ -170,63 +241,7 @@ __global__ void __launch_bounds__(256) vbd_sweep_kernel(SweepArgs a) {
         vv = a.vel[v];
     }
 
-    float fx = 0.f, fy = 0.f, fz = 0.f;
-    float h00 = 0.f, h01 = 0.f, h02 = 0.f, h11 = 0.f, h12 = 0.f, h22 = 0.f;
-#pragma unroll
-    for (int r = 0; r < RE; ++r) vbd_edge(xv, xe[r], le[r], we[r], ks, fx, fy, fz, h00, h01, h02, h11, h12, h22);
-    for (int r = RE; r < erows; ++r) {
-        const int2 iw = __ldg(&a.st_iw[base + r * 32]);
-        vbd_edge(xv, a.x[iw.x], __ldg(&a.st_rest[base + r * 32]), __int_as_float(iw.y), ks, fx, fy, fz, h00, h01, h02,
-                 h11, h12, h22);
-    }
-#pragma unroll
-    for (int r = 0; r < RB; ++r) vbd_bend(xv, xb[r], wb[r], fx, fy, fz);
-    for (int r = RB; r < brows; ++r) {
-        const int2 iw = __ldg(&a.st_iw[bbase + r * 32]);
-        vbd_bend(xv, a.x[iw.x], __int_as_float(iw.y), fx, fy, fz);
-    }
-    // reduce the TPV lanes of a vertex
-#pragma unroll
-    for (int o = TPV / 2; o > 0; o >>= 1) {
-        fx += __shfl_xor_sync(0xffffffffu, fx, o);
-        fy += __shfl_xor_sync(0xffffffffu, fy, o);
-        fz += __shfl_xor_sync(0xffffffffu, fz, o);
-        h00 += __shfl_xor_sync(0xffffffffu, h00, o);
-        h01 += __shfl_xor_sync(0xffffffffu, h01, o);
-        h02 += __shfl_xor_sync(0xffffffffu, h02, o);
-        h11 += __shfl_xor_sync(0xffffffffu, h11, o);
-        h12 += __shfl_xor_sync(0xffffffffu, h12, o);
-        h22 += __shfl_xor_sync(0xffffffffu, h22, o);
-    }
-    if (!leader) return;
-
-    // inertia: H += m/h^2 I (+1e9 I pinned), f += -m/h^2 ((x - x0) - v h) + m a
-    const float m = p0.w;
-    const float mh = m * a.h2inv;
-    fx += -mh * ((xv.x - p0.x) - vv.x * a.h) + m * ip.x;
-    fy += -mh * ((xv.y - p0.y) - vv.y * a.h) + m * ip.y;
-    fz += -mh * ((xv.z - p0.z) - vv.z * a.h) + m * ip.z;
-    const float dg = mh + mv.y + mv.x;
-    h00 += dg;
-    h11 += dg;
-    h22 += dg;
-
-    // symmetric 3x3 solve by adjugate / determinant, guarded by |det| > FLT_EPSILON
-    const float c00 = h11 * h22 - h12 * h12;
-    const float c01 = h02 * h12 - h01 * h22;
-    const float c02 = h01 * h12 - h02 * h11;
-    const float det = h00 * c00 + h01 * c01 + h02 * c02;
-    if (fabsf(det) > kEps) {
-        const float c11 = h00 * h22 - h02 * h02;
-        const float c12 = h01 * h02 - h00 * h12;
-        const float c22 = h00 * h11 - h01 * h01;
-        const float id = 1.f / det;
-        float4 xn = xv;
-        xn.x += (c00 * fx + c01 * fy + c02 * fz) * id;
-        xn.y += (c01 * fx + c11 * fy + c12 * fz) * id;
-        xn.z += (c02 * fx + c12 * fy + c22 * fz) * id;
-        a.x[v] = xn;
-    }
+    sweep_vertex<TPV, RE, RB>(a, v, leader, base, bbase, erows, brows, xv, xe, le, we, xb, wb, ks, ip, mv, p0, vv);
 }
 
 }  // namespace ats
