@@ -271,6 +271,30 @@ def run_ours(args):
     else:
         peak, peak_src = 6650.0, "fallback"
 
+    # --- XPBD at the same scale (the reference's other solver): CUDA-graph frames of
+    # predict, lambda reset, ITERS x (stretch colours + bending colours) projections and
+    # update, L2 flushed between frames; algorithmic bytes 28 V + 20 E + 64 B per iteration
+    x_keep, v_keep = cloth.state()
+    for _ in range(2):
+        cloth.frame(ats.SOLVER_XPBD, stream=stream, graph=True)
+    xpbd_ms = []
+    for i in range(max(3, min(args.steps, 10))):
+        flush.fill_(i & 0xFF)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        cloth.frame(ats.SOLVER_XPBD, stream=stream, graph=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        xpbd_ms.append(e0.elapsed_time(e1))
+    xpbd_frame_ms = float(sharding.allreduce_stats([float(np.median(xpbd_ms))], op="max")[0])
+    xpbd_bytes = (28 * info.num_verts + 20 * info.num_edges + 64 * info.num_bending_edges) * ITERS
+    cloth.set_state(x_keep, v_keep, stream=stream)
+    xpbd = {"frames_per_s": (1 if sharded else world) * 1e3 / xpbd_frame_ms, "ms_per_frame": xpbd_frame_ms,
+            "launches_per_frame": 3 + ITERS * (info.num_stretch_colors + info.num_bending_colors),
+            "achieved_gbs": xpbd_bytes / (xpbd_frame_ms * 1e-3) / 1e9,
+            "note": "whole-frame algorithmic bytes (28V+20E+64B per iteration) over the device-timed frame"}
+
     # --- end to end through the public API with host arrays: every frame uploads the
     # state (x, v) from pinned host memory, runs the frame and reads (x, v) back into it
     x_h = torch.empty((info.num_verts, 3), dtype=torch.float32, pin_memory=True).numpy()
@@ -316,7 +340,8 @@ def run_ours(args):
                             "kernel": f"vbd_sweep_kernel<{info.threads_per_vertex}>", "mean_launch_us": mean_sweep_ms * 1e3,
                             "alg_bytes_per_launch": bytes_launch, "peak_source": peak_src},
                "gpu_launches": args.steps * (2 + ITERS * info.num_vertex_colors),
-               "clocks": clk}
+               "clocks": clk,
+               "xpbd": dict(xpbd, frac_of_peak=xpbd["achieved_gbs"] / peak)}
     if rank == 0 and not args.no_cpu_baseline and args.workload == "c1":
         threads = os.cpu_count() or 1
         s = cpu_port_sample(threads, REF_SAMPLE_ITERS)

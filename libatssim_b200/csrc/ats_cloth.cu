@@ -65,16 +65,27 @@ __global__ void update_kernel(const float4* __restrict__ x, float4* __restrict__
 }
 
 // solve_stretch_mass_spring_template (xpbd_constraints.h:984-1059) for one colour.
+// Programmatic dependent launch: the constraint's ids, rest length, stiffness and the
+// endpoints' inverse masses (constant for the handle) are loaded before the wait on the
+// previous colour; positions and lambda after it.
 __global__ void xpbd_stretch_kernel(float4* __restrict__ x, const float4* __restrict__ vm, const int2* __restrict__ edge,
                                     const float* __restrict__ rest, const float* __restrict__ kst,
                                     float* __restrict__ lambda, int b, int e, float h) {
-    int i = b + blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = b + blockIdx.x * blockDim.x + threadIdx.x;
+    int2 ed = make_int2(0, 0);
+    float L = 0.f, k = 0.f, w0 = 0.f, w1 = 0.f;
+    if (i < e) {
+        ed = __ldg(&edge[i]);
+        L = __ldg(&rest[i]);
+        k = __ldg(&kst[i]);
+        w0 = __ldg(&vm[ed.x]).z;
+        w1 = __ldg(&vm[ed.y]).z;
+    }
+    grid_dependency_wait();
+    allow_dependent_launch();
     if (i >= e) return;
-    int2 ed = edge[i];
     float4 p0 = x[ed.x], p1 = x[ed.y];
-    float w0 = vm[ed.x].z, w1 = vm[ed.y].z;
     float lam = lambda[i];
-    float L = rest[i], k = kst[i];
     float3 d = make_float3(fs(p1.x, p0.x), fs(p1.y, p0.y), fs(p1.z, p0.z));
     float lsq = fdot(d, d);
     if ((double)lsq < 1e-8) return;
@@ -97,10 +108,24 @@ __global__ void xpbd_stretch_kernel(float4* __restrict__ x, const float4* __rest
 // symmetric Q, then k_b.
 __global__ void xpbd_bending_kernel(float4* __restrict__ x, const float4* __restrict__ vm, const int4* __restrict__ idx,
                                     const float4* __restrict__ q, float* __restrict__ lambda, int b, int e, float h) {
-    int i = b + blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = b + blockIdx.x * blockDim.x + threadIdx.x;
+    // constant data before the wait on the previous colour (as xpbd_stretch_kernel)
+    int4 id = make_int4(0, 0, 0, 0);
+    float4 qa = make_float4(0.f, 0.f, 0.f, 0.f), qb = qa, qc = qa;
+    float w[4] = {0.f, 0.f, 0.f, 0.f};
+    if (i < e) {
+        id = __ldg(&idx[i]);
+        qa = __ldg(&q[3 * i]);
+        qb = __ldg(&q[3 * i + 1]);
+        qc = __ldg(&q[3 * i + 2]);
+        w[0] = __ldg(&vm[id.x]).z;
+        w[1] = __ldg(&vm[id.y]).z;
+        w[2] = __ldg(&vm[id.z]).z;
+        w[3] = __ldg(&vm[id.w]).z;
+    }
+    grid_dependency_wait();
+    allow_dependent_launch();
     if (i >= e) return;
-    int4 id = idx[i];
-    float4 qa = q[3 * i], qb = q[3 * i + 1], qc = q[3 * i + 2];
     float Q[4][4];
     Q[0][0] = qa.x; Q[0][1] = Q[1][0] = qa.y; Q[0][2] = Q[2][0] = qa.z; Q[0][3] = Q[3][0] = qa.w;
     Q[1][1] = qb.x; Q[1][2] = Q[2][1] = qb.y; Q[1][3] = Q[3][1] = qb.z; Q[2][2] = qb.w;
@@ -108,12 +133,10 @@ __global__ void xpbd_bending_kernel(float4* __restrict__ x, const float4* __rest
     const float kb = qc.z;
     const int vid[4] = {id.x, id.y, id.z, id.w};
     float3 p[4];
-    float w[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
         float4 t = x[vid[j]];
         p[j] = make_float3(t.x, t.y, t.z);
-        w[j] = vm[vid[j]].z;
     }
     // C = 1/2 sum_ij Q_ij <x_i, x_j>
     float sum = 0.f;
@@ -644,21 +667,37 @@ int launch_reset(ats_cloth* c, cudaStream_t st) {
     return ATS_OK;
 }
 
+// a launch that may begin while the previous kernel of the stream drains
+// (programmatic dependent launch; the kernel waits with griddepcontrol.wait)
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kernel)(KArgs...), int blocks, int threads, cudaStream_t st, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(blocks);
+    cfg.blockDim = dim3(threads);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 int launch_xpbd_stretch(ats_cloth* c, int color, cudaStream_t st) {
     const int b = c->L.xs_color[color], e = c->L.xs_color[color + 1];
     if (e <= b) return ATS_OK;
-    xpbd_stretch_kernel<<<(e - b + 127) / 128, 128, 0, st>>>(c->x.p, c->vm.p, c->xs_edge.p, c->xs_rest.p, c->xs_k.p,
-                                                               c->xs_lambda.p, b, e, c->h);
-    ATS_CUDA(cudaGetLastError());
+    ATS_CUDA(launch_pdl(xpbd_stretch_kernel, (e - b + 127) / 128, 128, st, c->x.p, (const float4*)c->vm.p,
+                        (const int2*)c->xs_edge.p, (const float*)c->xs_rest.p, (const float*)c->xs_k.p,
+                        c->xs_lambda.p, b, e, c->h));
     return ATS_OK;
 }
 
 int launch_xpbd_bending(ats_cloth* c, int color, cudaStream_t st) {
     const int b = c->L.xb_color[color], e = c->L.xb_color[color + 1];
     if (e <= b) return ATS_OK;
-    xpbd_bending_kernel<<<(e - b + 127) / 128, 128, 0, st>>>(c->x.p, c->vm.p, c->xb_idx.p, c->xb_q.p, c->xb_lambda.p,
-                                                               b, e, c->h);
-    ATS_CUDA(cudaGetLastError());
+    ATS_CUDA(launch_pdl(xpbd_bending_kernel, (e - b + 127) / 128, 128, st, c->x.p, (const float4*)c->vm.p,
+                        (const int4*)c->xb_idx.p, (const float4*)c->xb_q.p, c->xb_lambda.p, b, e, c->h));
     return ATS_OK;
 }
 
