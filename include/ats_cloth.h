@@ -212,8 +212,9 @@ int ats_frame_to_residual(ats_cloth* cloth, double tol, int check_every, int max
 int ats_frame_to_residuals(ats_cloth* cloth, const double* tols, const int* first_check, int check_every,
                            int max_iterations, int* iterations, double* residual, ats_stream stream);
 
-/* Times `iterations` VBD iterations for every lanes-per-vertex (1, 2, 4, 8) and
- * block size (64, 128, 256) on this handle's own mesh, keeps the fastest and
+/* Times `iterations` VBD iterations (three times, taking the fastest) for every
+ * lanes-per-vertex (1, 2, 4, 8) and block size (64, 128, 256) on this handle's own
+ * mesh, keeps the fastest and
  * reports it. The iterate x is restored afterwards; captured frame graphs are
  * dropped (they are re-captured on next use). Synchronises `stream`. */
 int ats_autotune(ats_cloth* cloth, int iterations, ats_stream stream, int* tpv, int* block_size);

@@ -523,17 +523,23 @@ __global__ void __launch_bounds__(kSegChunks) segment_final_kernel(const double*
 // predict stores ||grad G(y)|| per instance; later calls deactivate an instance once
 // ||grad G(x)|| <= tol ||grad G(y)|| or its iteration cap is reached; n_active
 // receives the number of instances still iterating.
-// Bookkeeping of the residual-driven frame (one block). init: norm0 = ||grad G(y)||,
-// every instance with a nonzero gradient active. Otherwise, after `done` iterations:
-// every active instance has iters = done; an instance probed now (due) stops when
-// ||grad G|| <= tol ||grad G(y)|| or done >= max_iters. Then due is set for the next
-// probe point `next`: active instances with next == max_iters, or next >= first_i and
-// (next - first_i) a multiple of step (first_i = first[i], or step when first is null).
+// Bookkeeping of the residual-driven frame (one block). The probe schedule lives on the
+// device, so that the same captured chunk graph serves every probe point: pts[0..n-1]
+// are the iteration counts at which probes run and pts[n] = max_iters; *pidx is the
+// index of the probe point just reached (advanced here, once per call).
+// init: norm0 = ||grad G(y)||, every instance with a nonzero gradient active, *pidx = 0.
+// Otherwise, after done = pts[*pidx] iterations: every active instance has iters = done;
+// an instance probed now (due) stops when ||grad G|| <= tols[i] ||grad G(y)|| or
+// done >= max_iters. Then due is set for the next point `next`: active instances with
+// next == max_iters, or next >= first[i] and (next - first[i]) a multiple of step.
 __global__ void __launch_bounds__(256) residual_check_kernel(const double* norm, double* norm0, int* active, int* iters,
-                                                            int* n_active, int* due, int ninst, int init, int done,
-                                                            int next, int step, const int* first, int max_iters,
-                                                            double tol, const double* tols) {
+                                                            int* n_active, int* due, int ninst, int init,
+                                                            const int* pts, int* pidx, int step, const int* first,
+                                                            int max_iters, const double* tols) {
     __shared__ int count[256];
+    const int p = init ? 0 : *pidx;
+    const int done = init ? 0 : pts[p];
+    const int next = init ? pts[0] : pts[p + 1];
     int c = 0;
     for (int i = threadIdx.x; i < ninst; i += blockDim.x) {
         if (init) {
@@ -542,10 +548,9 @@ __global__ void __launch_bounds__(256) residual_check_kernel(const double* norm,
             iters[i] = 0;
         } else if (active[i]) {
             iters[i] = done;
-            const double ti = tols ? tols[i] : tol;
-            if (due[i] && (norm[i] <= ti * norm0[i] || done >= max_iters)) active[i] = 0;
+            if (due[i] && (norm[i] <= tols[i] * norm0[i] || done >= max_iters)) active[i] = 0;
         }
-        const int f = first ? first[i] : step;
+        const int f = first[i];
         due[i] = active[i] && (next >= max_iters || (next >= f && (next - f) % step == 0)) ? 1 : 0;
         c += active[i];
     }
@@ -555,7 +560,10 @@ __global__ void __launch_bounds__(256) residual_check_kernel(const double* norm,
         if (threadIdx.x < s) count[threadIdx.x] += count[threadIdx.x + s];
         __syncthreads();
     }
-    if (threadIdx.x == 0) *n_active = count[0];
+    if (threadIdx.x == 0) {
+        *n_active = count[0];
+        *pidx = init ? 0 : p + 1;
+    }
 }
 
 }  // namespace
@@ -885,6 +893,68 @@ int enqueue_potential(ats_cloth* c, double* g, cudaStream_t st) {
     return segment_sum(c, c->pot_vx.p, g, 0, st);
 }
 
+// Pieces of a residual-driven frame as CUDA graphs, cached on the handle:
+//   (k, 0, 0)       k = 2^j VBD iterations over the active instances;
+//   (0, step, cap)  the probe of the due instances and the bookkeeping.
+// A chunk of any length is the binary decomposition of its iterations, then the probe.
+// Every pointer and argument baked into them is fixed for the handle (the schedule,
+// tolerances and first probes are read from device memory), so a dozen graphs serve
+// every frame; they are dropped with the frame graphs (ats_autotune).
+int piece_graph(ats_cloth* c, int k, int step, int max_iterations, cudaGraphExec_t* out) {
+    const auto key = std::make_tuple(k, step, max_iterations);
+    auto it = c->chunk_graphs.find(key);
+    if (it != c->chunk_graphs.end()) {
+        *out = it->second;
+        return ATS_OK;
+    }
+    cudaStream_t cs = c->capture_stream;
+    cudaGraph_t g = nullptr;
+    ATS_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    int r = ATS_OK;
+    if (k > 0) {
+        r = enqueue_iterations(c, ATS_SOLVER_VBD, k, cs, c->active.p);
+    } else {
+        r = enqueue_residual_norms(c, cs, c->due.p, true);
+        if (!r) {
+            residual_check_kernel<<<1, 256, 0, cs>>>(c->red_out.p, c->norm0.p, c->active.p, c->iters.p,
+                                                      c->n_active.p, c->due.p, c->L.ninst, 0, c->probe_points.p,
+                                                      c->probe_idx.p, step, c->first_check.p, max_iterations,
+                                                      c->tols.p);
+            if (cudaGetLastError() != cudaSuccess) r = ATS_ERR_CUDA;
+        }
+    }
+    cudaError_t e = cudaStreamEndCapture(cs, &g);
+    if (r || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        if (!r) set_error(std::string("residual frame capture failed: ") + cudaGetErrorString(e));
+        return r ? r : ATS_ERR_CUDA;
+    }
+    cudaGraphExec_t exec = nullptr;
+    e = cudaGraphInstantiate(&exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        set_error(std::string("residual frame instantiate failed: ") + cudaGetErrorString(e));
+        return ATS_ERR_CUDA;
+    }
+    c->chunk_graphs[key] = exec;
+    *out = exec;
+    return ATS_OK;
+}
+
+// k iterations (binary pieces), then the probe and the bookkeeping
+int launch_chunk(ats_cloth* c, int k, int step, int max_iterations, cudaStream_t st) {
+    int r;
+    cudaGraphExec_t exec = nullptr;
+    for (int bit = 1 << 20; bit > 0; bit >>= 1)
+        if (k & bit) {
+            if ((r = piece_graph(c, bit, 0, 0, &exec))) return r;
+            ATS_CUDA(cudaGraphLaunch(exec, st));
+        }
+    if ((r = piece_graph(c, 0, step, max_iterations, &exec))) return r;
+    ATS_CUDA(cudaGraphLaunch(exec, st));
+    return ATS_OK;
+}
+
 int frame_to_residual_impl(ats_cloth* c, double tol, const double* tols, const int* first_check, int check_every,
                            int max_iterations, int* iterations, double* residual, cudaStream_t st,
                            const std::function<int(cudaStream_t)>& after_predict) {
@@ -893,64 +963,64 @@ int frame_to_residual_impl(ats_cloth* c, double tol, const double* tols, const i
         return ATS_ERR_INVALID;
     }
     const int ni = c->L.ninst;
-    int r;
-    const double* dtols = nullptr;
-    if (tols) {
-        if (!c->tols.p) ATS_CUDA(c->tols.alloc(ni));
-        ATS_CUDA(cudaMemcpyAsync(c->tols.p, tols, ni * sizeof(double), cudaMemcpyHostToDevice, st));
-        dtols = c->tols.p;
-    }
+    // per-instance tolerances and first probes, on the device (the chunk graphs read them)
+    if (!c->tols.p) ATS_CUDA(c->tols.alloc(ni));
     if (!c->due.p) ATS_CUDA(c->due.alloc(ni));
-    // probe points: every iteration count at which some instance is due (the device
-    // skips instances that are not), and the cap
-    std::vector<char> point(max_iterations + 1, 0);
-    const int* dfirst = nullptr;
-    if (first_check) {
-        if (!c->first_check.p) ATS_CUDA(c->first_check.alloc(ni));
-        std::vector<int> f(ni);
-        for (int i = 0; i < ni; ++i) {
-            f[i] = std::max(1, first_check[i]);
-            for (int k = f[i]; k <= max_iterations; k += check_every) point[k] = 1;
-        }
-        ATS_CUDA(cudaMemcpyAsync(c->first_check.p, f.data(), ni * sizeof(int), cudaMemcpyHostToDevice, st));
-        ATS_CUDA(cudaStreamSynchronize(st));  // f leaves scope
-        dfirst = c->first_check.p;
-    } else {
-        for (int k = check_every; k <= max_iterations; k += check_every) point[k] = 1;
+    if (!c->first_check.p) ATS_CUDA(c->first_check.alloc(ni));
+    if (!c->probe_idx.p) ATS_CUDA(c->probe_idx.alloc(1));
+    std::vector<double> tv(ni);
+    std::vector<int> fv(ni);
+    for (int i = 0; i < ni; ++i) {
+        tv[i] = tols ? tols[i] : tol;
+        fv[i] = first_check ? std::max(1, first_check[i]) : check_every;
     }
+    // probe points: every iteration count at which some instance is due (the device
+    // skips instances that are not), and the cap; then the cap as a sentinel
+    std::vector<char> point(max_iterations + 1, 0);
+    for (int i = 0; i < ni; ++i)
+        for (int k = fv[i]; k <= max_iterations; k += check_every) point[k] = 1;
     if (max_iterations > 0) point[max_iterations] = 1;
-    std::vector<int> points;
+    std::vector<int> pts;
     for (int k = 1; k <= max_iterations; ++k)
-        if (point[k]) points.push_back(k);
-    const int first_point = points.empty() ? 0 : points[0];
+        if (point[k]) pts.push_back(k);
+    const int npoints = (int)pts.size();
+    pts.push_back(max_iterations);
+    if (c->probe_points.n < pts.size()) {
+        // the chunk graphs hold the old address
+        for (auto& kv : c->chunk_graphs) cudaGraphExecDestroy(kv.second);
+        c->chunk_graphs.clear();
+        if (c->probe_points.p) {
+            cudaFree(c->probe_points.p);
+            c->probe_points.p = nullptr;
+            c->probe_points.n = 0;
+        }
+        ATS_CUDA(c->probe_points.alloc(std::max<size_t>(pts.size(), 1024)));
+    }
+    ATS_CUDA(cudaMemcpyAsync(c->tols.p, tv.data(), ni * sizeof(double), cudaMemcpyHostToDevice, st));
+    ATS_CUDA(cudaMemcpyAsync(c->first_check.p, fv.data(), ni * sizeof(int), cudaMemcpyHostToDevice, st));
+    ATS_CUDA(cudaMemcpyAsync(c->probe_points.p, pts.data(), pts.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+    ATS_CUDA(cudaStreamSynchronize(st));  // the host vectors leave scope
+    int r;
     for (int sub = 0; sub < c->prm.num_substep; ++sub) {
         if ((r = launch_predict(c, st))) return r;
         if ((r = enqueue_residual_norms(c, st, nullptr, true))) return r;
         if (after_predict && (r = after_predict(st))) return r;
         residual_check_kernel<<<1, 256, 0, st>>>(c->red_out.p, c->norm0.p, c->active.p, c->iters.p, c->n_active.p,
-                                                  c->due.p, ni, 1, 0, first_point, check_every, dfirst, max_iterations,
-                                                  tol, dtols);
+                                                  c->due.p, ni, 1, c->probe_points.p, c->probe_idx.p, check_every,
+                                                  c->first_check.p, max_iterations, c->tols.p);
         ATS_CUDA(cudaGetLastError());
-        // probes run on the device; the host looks at the number of active instances
-        // only every kProbesPerSync probe points, so it rarely waits on the device
+        // one chunk (graphs) per probe point; the host looks at the number of active
+        // instances only every kProbesPerSync points, so it rarely waits on the device
         constexpr int kProbesPerSync = 4;
         int done = 0;
-        for (size_t p = 0; p < points.size(); ++p) {
+        for (int p = 0; p < npoints; ++p) {
             if (p > 0 && p % kProbesPerSync == 0) {  // nothing has been probed before the first point
                 ATS_CUDA(cudaMemcpyAsync(c->host_flag, c->n_active.p, sizeof(int), cudaMemcpyDeviceToHost, st));
                 ATS_CUDA(cudaStreamSynchronize(st));
                 if (*c->host_flag == 0) break;
             }
-            const int k = points[p];
-            if ((r = enqueue_iterations(c, ATS_SOLVER_VBD, k - done, st, c->active.p)) ||
-                (r = enqueue_residual_norms(c, st, c->due.p, true)))
-                return r;
-            done = k;
-            const int next = p + 1 < points.size() ? points[p + 1] : max_iterations;
-            residual_check_kernel<<<1, 256, 0, st>>>(c->red_out.p, c->norm0.p, c->active.p, c->iters.p,
-                                                      c->n_active.p, c->due.p, ni, 0, done, next, check_every, dfirst,
-                                                      max_iterations, tol, dtols);
-            ATS_CUDA(cudaGetLastError());
+            if ((r = launch_chunk(c, pts[p] - done, check_every, max_iterations, st))) return r;
+            done = pts[p];
         }
         if (sub + 1 == c->prm.num_substep && (iterations || residual)) {
             // report against the last substep: residual relative to ||grad G(y)|| (the
@@ -1306,17 +1376,23 @@ int ats_autotune(ats_cloth* c, int iterations, ats_stream stream, int* out_tpv, 
         for (int b : blocks) {
             c->block = b;
             if ((r = enqueue_iterations(c, ATS_SOLVER_VBD, 1, st))) break;  // warm-up
-            cudaEventRecord(e0, st);
-            if ((r = enqueue_iterations(c, ATS_SOLVER_VBD, iterations, st))) break;
-            cudaEventRecord(e1, st);
-            cudaError_t ce = cudaEventSynchronize(e1);
-            if (ce != cudaSuccess) {
-                set_error(std::string("ats_autotune: ") + cudaGetErrorString(ce));
-                r = ATS_ERR_CUDA;
-                break;
+            // the fastest of three timings (short runs are noisy)
+            float ms = 1e30f;
+            for (int rep = 0; rep < 3 && !r; ++rep) {
+                cudaEventRecord(e0, st);
+                if ((r = enqueue_iterations(c, ATS_SOLVER_VBD, iterations, st))) break;
+                cudaEventRecord(e1, st);
+                cudaError_t ce = cudaEventSynchronize(e1);
+                if (ce != cudaSuccess) {
+                    set_error(std::string("ats_autotune: ") + cudaGetErrorString(ce));
+                    r = ATS_ERR_CUDA;
+                    break;
+                }
+                float t = 0.f;
+                cudaEventElapsedTime(&t, e0, e1);
+                ms = std::min(ms, t);
             }
-            float ms = 0.f;
-            cudaEventElapsedTime(&ms, e0, e1);
+            if (r) break;
             if (ms < best) {
                 best = ms;
                 best_tpv = tpv;

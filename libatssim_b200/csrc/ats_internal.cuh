@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 
 #include <functional>
+#include <map>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -71,6 +73,8 @@ struct ats_cloth {
     // scratch of the FP64 reductions
     DevBuf<double> partial, seg_partial, red_out, g2, norm0, tols;
     DevBuf<int> active, iters, n_active, due, first_check;  // ats_frame_to_residual bookkeeping
+    DevBuf<int> probe_points, probe_idx;                     // its probe schedule, on the device
+    std::map<std::tuple<int, int, int>, cudaGraphExec_t> chunk_graphs;  // residual-frame pieces
     int* host_flag = nullptr;             // pinned copy of n_active
     // learned warm start (uploaded at create; the rest allocated on first use)
     DevBuf<int> feat_nb, inst_eseg, inst_bseg, free_list;
@@ -94,6 +98,8 @@ struct ats_cloth {
             cudaGraphExecDestroy(warm_graph);
             warm_graph = nullptr;
         }
+        for (auto& kv : chunk_graphs) cudaGraphExecDestroy(kv.second);
+        chunk_graphs.clear();
     }
     ~ats_cloth() {
         drop_graphs();

@@ -162,7 +162,7 @@ def plain_per_instance_ms(insts, prm, frames=10, warmup=3, seed0=10000, stream=N
     st = stream if stream is not None else torch.cuda.current_stream()
     handles = [Cloth([i], **prm) for i in insts]
     for h in handles:
-        h.autotune(iterations=2)
+        h.autotune(iterations=10)
     rng_masses = [float(i.mass.sum()) for i in insts]
     for f in range(warmup):
         for h in handles:
