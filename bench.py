@@ -17,13 +17,25 @@ plain Vertex Block Descent with 50 iterations x 4 colours per frame, FP32.
   cpu_baseline  the CPU oracle (a C++ restatement of the reference's CPU VBD,
          the reference itself does not build here) on a bounded sample of the
          same workload, rank 0 only.
+  xpbd   the same cloth solved by XPBD instead (CUDA-graph frames of 50 x
+         (stretch + bending colours) projections): frames/s and bandwidth.
 
 --impl reference times that CPU implementation alone on this workload with all
 host threads (each step = 10 of the frame's 50 iterations, scaled to frames/s).
 
+Other workloads (--workload):
+  c2  256 batched cloths of side U{16..256} with random materials and pins, plain
+      VBD, one launch per colour over all instances; the same keys as c1.
+  c3  a 128 x 128 cloth with a random wind per frame, 200 iterations; c4 64 batched
+      cloths of side U{64..512} with wind, 50 iterations. Both record plain frames,
+      train the warm-start network on the GPU and compare, on held-out frames,
+      plain VBD with learned-guess frames that stop at each instance's plain
+      residual (libatssim_b200/learned.py describes the protocol).
+
 Multi-GPU: the single cloth does not partition (a graph split would need a halo
-exchange per colour), so N > 1 runs N independent replicas ("weak" scaling); the
-timing is the max over ranks.
+exchange per colour), so N > 1 runs N independent replicas ("weak" scaling); c2
+shards its instances over the ranks ("strong" scaling). Timing is the max over
+ranks.
 """
 import argparse
 import json

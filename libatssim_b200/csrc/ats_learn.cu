@@ -368,35 +368,6 @@ __global__ void features_kernel(FeatArgs a, float* __restrict__ out) {
     for (int k = 0; k < kIn; ++k) out[(size_t)v * kIn + k] = f[k];
 }
 
-// guess = y + s * MLP(features) for free vertices; y is the current iterate x.
-__global__ void __launch_bounds__(kThreads) infer_kernel(FeatArgs a, const __nv_bfloat16* wpack, const float* master,
-                                                         const float* nrm, float4* __restrict__ x, float s) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    Tile& S = *reinterpret_cast<Tile*>(smem);
-    load_weights(S, wpack, master, nrm);
-    __syncthreads();
-    const int base = blockIdx.x * kTile;
-    for (int i = threadIdx.x; i < kTile; i += kThreads) {
-        const int v = base + i;
-        float f[kIn];
-        if (v < a.nv) vertex_features(a, v, f);
-        for (int k = 0; k < kInP; ++k)
-            S.x[i][k] = __float2bfloat16_rn(
-                v < a.nv && k < kIn ? (f[k] - S.nrm[kNormInMean + k]) * S.nrm[kNormInScale + k] : 0.f);
-    }
-    __syncthreads();
-    forward(S);
-    for (int i = threadIdx.x; i < kTile; i += kThreads) {
-        const int v = base + i;
-        if (v >= a.nv || a.vm[v].y != 0.f) continue;
-        float4 p = x[v];
-        p.x += s * (S.nrm[kNormOutMean + 0] + S.nrm[kNormOutStd + 0] * S.y[i][0]);
-        p.y += s * (S.nrm[kNormOutMean + 1] + S.nrm[kNormOutStd + 1] * S.y[i][1]);
-        p.z += s * (S.nrm[kNormOutMean + 2] + S.nrm[kNormOutStd + 2] * S.y[i][2]);
-        x[v] = p;
-    }
-}
-
 // Network outputs of n feature rows (the forward pass of ats_mlp_infer).
 __global__ void __launch_bounds__(kThreads) infer_samples_kernel(const float* __restrict__ feat, int n,
                                                                  const __nv_bfloat16* wpack, const float* master,
@@ -673,7 +644,6 @@ int set_smem_limits() {
         g_infer_ctas = std::max(1, sms) * std::max(1, resident);
     }
     ATS_CUDA(cudaFuncSetAttribute(train_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmem));
-    ATS_CUDA(cudaFuncSetAttribute(infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmem));
     ATS_CUDA(cudaFuncSetAttribute(infer_samples_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmem));
     done = true;
     return ATS_OK;
