@@ -354,7 +354,7 @@ def run_ours(args):
                "gpu_launches": args.steps * (2 + ITERS * info.num_vertex_colors),
                "clocks": clk,
                "xpbd": dict(xpbd, frac_of_peak=xpbd["achieved_gbs"] / peak)}
-    if rank == 0 and not args.no_cpu_baseline and args.workload == "c1":
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "c1":
         threads = os.cpu_count() or 1
         s = cpu_port_sample(threads, REF_SAMPLE_ITERS)
         s.frame()
