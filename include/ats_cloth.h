@@ -219,6 +219,20 @@ int ats_frame_to_residuals(ats_cloth* cloth, const double* tols, const int* firs
  * dropped (they are re-captured on next use). Synchronises `stream`. */
 int ats_autotune(ats_cloth* cloth, int iterations, ats_stream stream, int* tpv, int* block_size);
 
+/* Two-device asynchronous iteration, as example2_async_iter.cpp:1160-1200 and
+ * example3 run it: both devices iterate on their own copy of the positions from a
+ * common fork point, then the copies are merged.
+ * ats_async_fork: the current iterate becomes the fork point (id_xpbd_copy_to_cpu_gpu,
+ * example2_async_iter.cpp:1269-1273).
+ * ats_async_merge: merges the other device's iterate (host, caller order, 3 floats per
+ * vertex) into this handle's, as Core::read_and_solve_conflict
+ * (xpbd_constraints.h:815-869) with this handle as "self": with weight > FLT_EPSILON,
+ * fork + weight (dx_self + dx_other) where both moved, the one that moved otherwise;
+ * else the average. The result is the new iterate and the new fork point.
+ * Synchronises `stream`. */
+int ats_async_fork(ats_cloth* cloth, ats_stream stream);
+int ats_async_merge(ats_cloth* cloth, const float* other_positions, float weight, ats_stream stream);
+
 /* FP64 incremental-potential energy of the current iterate against the current
  * frame start (Energy::compute_energy_* of xpbd_constraints.h:2079-2214):
  * out[0] = inertia, out[1] = stretch, out[2] = bending. Synchronises `stream`. */

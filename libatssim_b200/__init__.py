@@ -114,6 +114,8 @@ _SIGNATURES = {
     "ats_frame_to_residual": [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, _ip, _dp, _vp],
     "ats_residual": [_vp, _dp, _vp],
     "ats_potential": [_vp, _dp, _vp],
+    "ats_async_fork": [_vp, _vp],
+    "ats_async_merge": [_vp, _fp, ctypes.c_float, _vp],
     "ats_mlp_create": [ctypes.c_ulonglong, ctypes.POINTER(_vp)],
     "ats_mlp_destroy": [_vp],
     "ats_mlp_get_params": [_vp, _fp],
@@ -361,6 +363,16 @@ class Cloth:
         v = np.zeros((self.nv, 3), dtype=np.float32)
         _check(lib().ats_get_state(self.h, _p(x, ctypes.c_float), _p(v, ctypes.c_float), _stream(stream)))
         return x, v
+
+    def async_fork(self, stream=None):
+        """The current iterate becomes the fork point of two-device iteration."""
+        _check(lib().ats_async_fork(self.h, _stream(stream)))
+
+    def async_merge(self, other_positions, weight=0.5, stream=None):
+        """Merges another device's iterate (caller order) into this one
+        (Core::read_and_solve_conflict); the result is also the new fork point."""
+        o = np.ascontiguousarray(other_positions, dtype=np.float32)
+        _check(lib().ats_async_merge(self.h, _p(o, ctypes.c_float), float(weight), _stream(stream)))
 
     def state_into(self, x, v, stream=None):
         """ats_get_state into caller arrays (C-contiguous float32 (V, 3), e.g. views of

@@ -175,6 +175,44 @@ __global__ void xpbd_bending_kernel(float4* __restrict__ x, const float4* __rest
     }
 }
 
+// Core::read_and_solve_conflict (xpbd_constraints.h:815-869), this device's iterate
+// being "self": with the fork point init, self and other moved by dx_s, dx_o,
+//   weight > FLT_EPSILON: both moved -> init + weight (dx_s + dx_o); one moved -> that
+//                         one; none -> init;
+//   otherwise:            (self + other) / 2;
+// the result becomes both the iterate and the new fork point. "Moved" is
+// |dx|^2 != 0 in FP32, summed x, y, z in that order; every operation is rounded
+// explicitly, in the reference's order.
+__global__ void async_merge_kernel(float4* __restrict__ x, float4* __restrict__ begin, const float* __restrict__ other,
+                                   const int* __restrict__ to_caller, int n, float weight) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const size_t o = 3 * (size_t)to_caller[i];
+    const float4 ps = x[i], init = begin[i];
+    const float po[3] = {other[o], other[o + 1], other[o + 2]};
+    const float s3[3] = {ps.x, ps.y, ps.z}, b3[3] = {init.x, init.y, init.z};
+    float r[3];
+    if (weight > kEps) {
+        float ds[3], dq[3];
+        for (int k = 0; k < 3; ++k) {
+            ds[k] = fs(s3[k], b3[k]);
+            dq[k] = fs(po[k], b3[k]);
+        }
+        const bool act_s = fa(fa(fm(ds[0], ds[0]), fm(ds[1], ds[1])), fm(ds[2], ds[2])) != 0.f;
+        const bool act_o = fa(fa(fm(dq[0], dq[0]), fm(dq[1], dq[1])), fm(dq[2], dq[2])) != 0.f;
+        for (int k = 0; k < 3; ++k) {
+            if (act_s && act_o) r[k] = fa(b3[k], fm(weight, fa(ds[k], dq[k])));
+            else if (act_s) r[k] = s3[k];
+            else if (act_o) r[k] = po[k];
+            else r[k] = b3[k];
+        }
+    } else {
+        for (int k = 0; k < 3; ++k) r[k] = fm(0.5f, fa(s3[k], po[k]));
+    }
+    x[i] = make_float4(r[0], r[1], r[2], ps.w);
+    begin[i] = make_float4(r[0], r[1], r[2], 0.f);
+}
+
 // State I/O between the caller's vertex order (3 floats per vertex) and the layout.
 __global__ void scatter_state_kernel(const float* __restrict__ xc, const float* __restrict__ vc,
                                      const int* __restrict__ to_caller, float4* __restrict__ x, float4* __restrict__ x0,
@@ -1221,6 +1259,34 @@ static int read_back(ats_cloth* c, const float4* src, float* dst, float* staging
     gather_state_kernel<<<(n + 255) / 256, 256, 0, st>>>(src, c->to_caller.p, staging, n);
     ATS_CUDA(cudaGetLastError());
     ATS_CUDA(cudaMemcpyAsync(dst, staging, 12 * (size_t)n, cudaMemcpyDeviceToHost, st));
+    return ATS_OK;
+}
+
+int ats_async_fork(ats_cloth* c, ats_stream stream) {
+    if (!c) {
+        set_error("ats_async_fork: null handle");
+        return ATS_ERR_INVALID;
+    }
+    if (!c->async_begin.p) ATS_CUDA(c->async_begin.alloc(c->L.nv));
+    ATS_CUDA(cudaMemcpyAsync(c->async_begin.p, c->x.p, c->x.bytes(), cudaMemcpyDeviceToDevice, S(stream)));
+    return ATS_OK;
+}
+
+int ats_async_merge(ats_cloth* c, const float* other, float weight, ats_stream stream) {
+    if (!c || !other) {
+        set_error("ats_async_merge: null argument");
+        return ATS_ERR_INVALID;
+    }
+    if (!c->async_begin.p) {
+        set_error("ats_async_merge: no fork point (call ats_async_fork first)");
+        return ATS_ERR_INVALID;
+    }
+    const int n = c->L.nv;
+    cudaStream_t st = S(stream);
+    ATS_CUDA(cudaMemcpyAsync(c->io_x.p, other, 12 * (size_t)n, cudaMemcpyHostToDevice, st));
+    async_merge_kernel<<<(n + 255) / 256, 256, 0, st>>>(c->x.p, c->async_begin.p, c->io_x.p, c->to_caller.p, n, weight);
+    ATS_CUDA(cudaGetLastError());
+    ATS_CUDA(cudaStreamSynchronize(st));
     return ATS_OK;
 }
 

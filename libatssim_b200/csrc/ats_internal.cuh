@@ -70,6 +70,7 @@ struct ats_cloth {
     DevBuf<int> inst_seg;
     DevBuf<int> to_caller;
     DevBuf<float> io_x, io_v;  // caller-order staging of the state
+    DevBuf<float4> async_begin;  // fork point of two-device asynchronous iteration
     // scratch of the FP64 reductions
     DevBuf<double> partial, seg_partial, red_out, g2, norm0, tols;
     DevBuf<int> active, iters, n_active, due, first_check;  // ats_frame_to_residual bookkeeping
@@ -111,7 +112,7 @@ struct ats_cloth {
                slices.bytes() + slice_inst.bytes() + xs_edge.bytes() + xs_rest.bytes() + xs_k.bytes() + xs_lambda.bytes() +
                xb_idx.bytes() + xb_q.bytes() + xb_lambda.bytes() + en_edge.bytes() + en_rest.bytes() + en_k.bytes() +
                en_q.bytes() + en_kb.bytes() + en_bend.bytes() + inst_seg.bytes() + to_caller.bytes() + io_x.bytes() +
-               io_v.bytes() + partial.bytes() +
+               io_v.bytes() + async_begin.bytes() + partial.bytes() +
                seg_partial.bytes() + red_out.bytes() + g2.bytes() + norm0.bytes() + active.bytes() + iters.bytes() +
                n_active.bytes();
     }

@@ -190,3 +190,30 @@ class Scene:
     def grad_norm_of(self, x):
         x = np.ascontiguousarray(x, dtype=np.float32)
         return lib().ato_grad_norm_of(self.h, _p(x, ctypes.c_float))
+
+
+def async_merge(begin, mine, other, weight):
+    """Core::read_and_solve_conflict (src/Solver/xpbd_constraints.h:815-869) over all
+    vertices, in FP32 with one rounding per operation in the reference's order:
+    returns the merged positions (the new iterate and fork point of "mine")."""
+    f = np.float32
+    b, s, o = (np.asarray(a, dtype=np.float32).reshape(-1, 3) for a in (begin, mine, other))
+    w = f(weight)
+    if w > f(1.19209290e-7):
+        ds = (s - b).astype(np.float32)
+        do = (o - b).astype(np.float32)
+
+        def moved(d):
+            sq = (d * d).astype(np.float32)
+            return ((sq[:, 0] + sq[:, 1]).astype(np.float32) + sq[:, 2]).astype(np.float32) != 0
+
+        a_s, a_o = moved(ds), moved(do)
+        both = (b + (w * (ds + do).astype(np.float32)).astype(np.float32)).astype(np.float32)
+        out = b.copy()
+        out[a_s & a_o] = both[a_s & a_o]
+        only_s = a_s & ~a_o
+        only_o = a_o & ~a_s
+        out[only_s] = s[only_s]
+        out[only_o] = o[only_o]
+        return out
+    return (f(0.5) * (s + o).astype(np.float32)).astype(np.float32)
