@@ -641,11 +641,73 @@ int upload_stencil(ats_cloth* c) {
     // a slice lies in one instance: the instance id of its first vertex
     std::vector<int> si(L.slices.size() / 4);
     for (size_t k = 0; k < si.size(); ++k) std::memcpy(&si[k], &L.vm[4 * (size_t)L.slices[4 * k] + 3], sizeof(int));
-    return upload(c->slice_inst, si, si.size());
+    if ((r = upload(c->slice_inst, si, si.size())) || (r = upload(c->color_slices, L.color_slices, L.color_slices.size())))
+        return r;
+    // per-colour lists of the slices still iterating (residual-driven frames)
+    std::vector<int> zeros(std::max<size_t>(si.size(), 1), 0);
+    if ((r = upload(c->act_list, zeros, si.size())) ||
+        (r = upload(c->act_count, zeros, std::max(1, L.n_vcolors))))
+        return r;
+    return ATS_OK;
+}
+
+// The slices of instances still active, listed per colour at the colour's slice
+// offset (a warp appends its run of one colour with one atomic). counts must be zero.
+__global__ void compact_slices_kernel(const int* __restrict__ slice_inst, const int* __restrict__ active,
+                                      const int* __restrict__ color_begin, int ncolors, int nslices,
+                                      int* __restrict__ list, int* __restrict__ counts) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    int col = -1;
+    bool act = false;
+    if (s < nslices) {
+        act = active[slice_inst[s]] != 0;
+        col = 0;
+        while (col + 1 < ncolors && s >= color_begin[col + 1]) ++col;
+    }
+    const unsigned actm = __ballot_sync(0xffffffffu, act);
+    const unsigned peers = __match_any_sync(0xffffffffu, col) & actm;
+    const int leader = peers ? __ffs(peers) - 1 : lane;
+    int base = 0;
+    if (act && lane == leader) base = atomicAdd(&counts[col], __popc(peers));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (act) list[color_begin[col] + base + __popc(peers & ((1u << lane) - 1u))] = s;
+}
+
+int enqueue_compaction(ats_cloth* c, cudaStream_t st) {
+    const int n = (int)c->slices.n, nc = c->L.n_vcolors;
+    if (n == 0 || nc == 0) return ATS_OK;
+    ATS_CUDA(cudaMemsetAsync(c->act_count.p, 0, nc * sizeof(int), st));
+    compact_slices_kernel<<<(n + 255) / 256, 256, 0, st>>>(c->slice_inst.p, c->active.p, c->color_slices.p, nc, n,
+                                                           c->act_list.p, c->act_count.p);
+    ATS_CUDA(cudaGetLastError());
+    return ATS_OK;
+}
+
+// Resident CTAs of vbd_sweep_list_kernel, all SMs together, per (lanes per vertex,
+// block size); queried on first use, which is outside stream capture (the eager
+// iterations of ats_frame_to_residual's first frame come first).
+int list_sweep_ctas(int tpv, int block) {
+    static int cache[4][3] = {};
+    const int ti = tpv == 1 ? 0 : tpv == 2 ? 1 : tpv == 4 ? 2 : 3, bi = block == 64 ? 0 : block == 128 ? 1 : 2;
+    if (!cache[ti][bi]) {
+        int dev = 0, sms = 148, res = 1;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaError_t e;
+        switch (tpv) {
+            case 1: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&res, vbd_sweep_list_kernel<1, 6, 6>, block, 0); break;
+            case 2: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&res, vbd_sweep_list_kernel<2, 3, 3>, block, 0); break;
+            case 4: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&res, vbd_sweep_list_kernel<4, 2, 2>, block, 0); break;
+            default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&res, vbd_sweep_list_kernel<8, 1, 1>, block, 0); break;
+        }
+        cache[ti][bi] = std::max(1, sms) * (e == cudaSuccess && res > 0 ? res : 1);
+    }
+    return cache[ti][bi];
 }
 
 template <int TPV, int RE, int RB>
-cudaError_t sweep_launch(dim3 grid, dim3 block, cudaStream_t st, const SweepArgs& a) {
+cudaError_t sweep_launch(dim3 grid, dim3 block, cudaStream_t st, const SweepArgs& a, bool listed) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = grid;
     cfg.blockDim = block;
@@ -656,6 +718,7 @@ cudaError_t sweep_launch(dim3 grid, dim3 block, cudaStream_t st, const SweepArgs
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
+    if (listed) return cudaLaunchKernelEx(&cfg, vbd_sweep_list_kernel<TPV, RE, RB>, a);
     return cudaLaunchKernelEx(&cfg, vbd_sweep_kernel<TPV, RE, RB>, a);
 }
 
@@ -672,19 +735,26 @@ int launch_sweep(ats_cloth* c, int color, cudaStream_t st, const int* active) {
     a.slices = c->slices.p;
     a.slice_inst = c->slice_inst.p;
     a.inst = c->inst.p;
-    a.active = active;
+    // with an activity mask: only the slices the last compaction listed (the mask
+    // itself is what the compaction read)
+    const bool listed = active != nullptr;
+    a.active = nullptr;  // masked sweeps go through the lists
+    a.list = listed ? c->act_list.p + sb : nullptr;
+    a.list_count = listed ? c->act_count.p + color : nullptr;
     a.slice_begin = sb;
     a.slice_end = se;
     a.h = c->h;
     a.h2inv = c->h2inv;
     const int warps_per_block = c->block / 32;
-    const dim3 grid((se - sb + warps_per_block - 1) / warps_per_block), block(c->block);
+    int blocks = (se - sb + warps_per_block - 1) / warps_per_block;
+    if (listed) blocks = std::min(blocks, list_sweep_ctas(c->L.tpv, c->block));
+    const dim3 grid(blocks), block(c->block);
     cudaError_t e;
     switch (c->L.tpv) {
-        case 1: e = sweep_launch<1, 6, 6>(grid, block, st, a); break;
-        case 2: e = sweep_launch<2, 3, 3>(grid, block, st, a); break;
-        case 4: e = sweep_launch<4, 2, 2>(grid, block, st, a); break;
-        default: e = sweep_launch<8, 1, 1>(grid, block, st, a); break;
+        case 1: e = sweep_launch<1, 6, 6>(grid, block, st, a, listed); break;
+        case 2: e = sweep_launch<2, 3, 3>(grid, block, st, a, listed); break;
+        case 4: e = sweep_launch<4, 2, 2>(grid, block, st, a, listed); break;
+        default: e = sweep_launch<8, 1, 1>(grid, block, st, a, listed); break;
     }
     if (e != cudaSuccess) {
         set_error(std::string("vbd sweep launch: ") + cudaGetErrorString(e));
@@ -959,6 +1029,7 @@ int piece_graph(ats_cloth* c, int k, int step, int max_iterations, cudaGraphExec
                                                       c->probe_idx.p, step, c->first_check.p, max_iterations,
                                                       c->tols.p);
             if (cudaGetLastError() != cudaSuccess) r = ATS_ERR_CUDA;
+            if (!r) r = enqueue_compaction(c, cs);
         }
     }
     cudaError_t e = cudaStreamEndCapture(cs, &g);
@@ -1047,6 +1118,8 @@ int frame_to_residual_impl(ats_cloth* c, double tol, const double* tols, const i
                                                   c->due.p, ni, 1, c->probe_points.p, c->probe_idx.p, check_every,
                                                   c->first_check.p, max_iterations, c->tols.p);
         ATS_CUDA(cudaGetLastError());
+        if ((r = enqueue_compaction(c, st))) return r;
+        list_sweep_ctas(c->L.tpv, c->block);  // occupancy query before any capture
         // one chunk (graphs) per probe point; the host looks at the number of active
         // instances only every kProbesPerSync points, so it rarely waits on the device
         constexpr int kProbesPerSync = 4;

@@ -35,7 +35,9 @@ struct SweepArgs {
     const int4* __restrict__ slices;
     const int* __restrict__ slice_inst;  // instance of each slice
     const float4* __restrict__ inst;
-    const int* __restrict__ active;  // per instance, null = all active
+    const int* __restrict__ active;      // vbd_sweep_kernel: per instance, null = all active
+    const int* __restrict__ list;        // vbd_sweep_list_kernel: this colour's active slices
+    const int* __restrict__ list_count;  // and their number (device)
     int slice_begin, slice_end;
     float h, h2inv;
 };
@@ -242,6 +244,68 @@ __global__ void __launch_bounds__(256) vbd_sweep_kernel(SweepArgs a) {
     }
 
     sweep_vertex<TPV, RE, RB>(a, v, leader, base, bbase, erows, brows, xv, xe, le, we, xb, wb, ks, ip, mv, p0, vv);
+}
+
+// The sweep of a residual-driven frame: only the slices of instances still iterating,
+// listed per colour by the compaction after each probe (order within a colour does not
+// matter: its vertices are independent). A grid of resident size strides over the
+// list, so a converged instance costs nothing, not even a CTA launch.
+template <int TPV, int RE, int RB>
+__global__ void __launch_bounds__(256) vbd_sweep_list_kernel(SweepArgs a) {
+    grid_dependency_wait();  // the list and the positions come from the kernels before
+    allow_dependent_launch();
+    const int lane = threadIdx.x & 31;
+    const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
+    const int count = *a.list_count;
+    for (int idx = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); idx < count; idx += nwarps) {
+        const int slice = a.list[idx];
+        const int4 sd = __ldg(&a.slices[slice]);
+        const int rows = sd.w & 0xffff, erows = sd.w >> 16, brows = rows - erows;
+        const int k = lane / TPV;
+        const bool leader = k < sd.y && (lane % TPV) == 0;
+        const int v = sd.x + min(k, sd.y - 1);
+        const int base = sd.z + lane;
+        const int bbase = base + erows * 32;
+        int ue[RE], ub[RB];
+        float we[RE], le[RE], wb[RB];
+#pragma unroll
+        for (int r = 0; r < RE; ++r) {
+            ue[r] = v;
+            we[r] = 0.f;
+            le[r] = -1.f;
+            if (r < erows) {
+                const int2 iw = __ldg(&a.st_iw[base + r * 32]);
+                ue[r] = iw.x;
+                we[r] = __int_as_float(iw.y);
+                le[r] = __ldg(&a.st_rest[base + r * 32]);
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < RB; ++r) {
+            ub[r] = v;
+            wb[r] = 0.f;
+            if (r < brows) {
+                const int2 iw = __ldg(&a.st_iw[bbase + r * 32]);
+                ub[r] = iw.x;
+                wb[r] = __int_as_float(iw.y);
+            }
+        }
+        const float4 mv = __ldg(&a.vm[v]);
+        const float4 ip = __ldg(&a.inst[__float_as_int(mv.w)]);
+        const float4 xv = a.x[v];
+        float4 xe[RE], xb[RB];
+#pragma unroll
+        for (int r = 0; r < RE; ++r) xe[r] = a.x[ue[r]];
+#pragma unroll
+        for (int r = 0; r < RB; ++r) xb[r] = a.x[ub[r]];
+        float4 p0 = make_float4(0.f, 0.f, 0.f, 0.f), vv = p0;
+        if (leader) {
+            p0 = a.x0[v];
+            vv = a.vel[v];
+        }
+        sweep_vertex<TPV, RE, RB>(a, v, leader, base, bbase, erows, brows, xv, xe, le, we, xb, wb, ip.w, ip, mv, p0,
+                                  vv);
+    }
 }
 
 }  // namespace ats
