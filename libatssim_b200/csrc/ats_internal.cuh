@@ -126,6 +126,8 @@ namespace ats {
 // Kernel launches of one handle (ats_cloth.cu); each returns an ATS_* status.
 int launch_predict(ats_cloth* c, cudaStream_t st);
 int launch_update(ats_cloth* c, cudaStream_t st);
+// With `active` (the residual-driven frames' flags), a sweep runs over the per-colour
+// lists of active slices that enqueue_compaction built from those flags.
 int launch_sweep(ats_cloth* c, int color, cudaStream_t st, const int* active = nullptr);
 int enqueue_iterations(ats_cloth* c, int solver, int iterations, cudaStream_t st, const int* active = nullptr);
 // ||grad G|| per instance into c->red_out.p (FP64 throughout, or FP32 per-vertex terms
