@@ -74,7 +74,7 @@ def build(verbose=False, ptxas_info=False):
     return LIB
 
 
-TEST_SOURCES = ["heft_case.cpp", "vbd_dag.cpp"]
+TEST_SOURCES = ["heft_case.cpp", "vbd_dag.cpp", "launch_modes.cpp"]
 
 
 def build_tests():

@@ -66,3 +66,37 @@ def test_vbd_task_graph_through_scheduler(programs, mode):
     # predict + 8 x 4 colours + last node + update + root + terminal, all on the B200
     assert out["tasks"] == 1 + 8 * 4 + 2 + 2
     assert out["tasks_on_gpu"] >= 8 * 4
+
+
+def test_launch_modes_on_host_devices(programs):
+    # the HEFT 2002 DAG on two host-only "devices" (the first two cost columns); every
+    # mode runs each task it owns once, after its predecessors, on the mode's device
+    d = json.load(open(os.path.join(GOLD, "heft2002.json")))
+    text = "\n".join([f"2 {len(d['computation'])} {len(d['edges'])}"] +
+                     [" ".join(str(c) for c in row[:2]) for row in d["computation"]] +
+                     [f"{a} {b} {w}" for a, b, w in d["edges"]]) + "\n"
+    r = subprocess.run([programs["launch_modes"]], input=text, capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0, r.stderr
+    out = json.loads(r.stdout)
+    proc = {t + 1: p for t, p in enumerate(out["proc"])}
+    assert set(proc.values()) == {0, 1}  # the schedule uses both devices
+    n = len(d["computation"])
+    for mode, m in out["modes"].items():
+        runs = [(t, dev) for t, dev in m["log"] if dev != 2]
+        tasks = [t for t, _ in runs]
+        assert len(tasks) == len(set(tasks)), mode
+        own = {"partial_cpu": {t for t in proc if proc[t] == 0}, "partial_gpu": {t for t in proc if proc[t] == 1}}
+        assert set(tasks) == own.get(mode, set(range(1, n + 1))), mode
+        where = dict(runs)
+        expect_dev = {"cpu": lambda t: 0, "sequence_hetero": lambda t: 0, "gpu": lambda t: 1,
+                      "partial_cpu": lambda t: 0, "partial_gpu": lambda t: 1}.get(mode, lambda t: proc[t])
+        assert all(dev == expect_dev(t) for t, dev in runs), mode
+        pos = {t: i for i, (t, _) in enumerate(m["log"]) if t}
+        for a, b, _ in d["edges"]:
+            if a in pos and b in pos:
+                assert pos[a] < pos[b], (mode, a, b)
+                # a host task waits for a device predecessor: a drain lies between them
+                if mode in ("hetero", "fake_hetero") and where[a] == 1 and where[b] == 0:
+                    assert any(t == 0 and dev == 2 for t, dev in m["log"][pos[a] + 1:pos[b]]), (mode, a, b)
+    # work left on device 1 is drained once at the end of a launch
+    assert out["modes"]["gpu"]["drains"] == 1 and out["modes"]["cpu"]["drains"] == 0
