@@ -174,10 +174,17 @@ def run_reference(args):
     print(json.dumps(out), flush=True)
 
 
-def profile_traffic(alg_bytes):
-    """DRAM bytes per sweep launch from the committed ncu summary of the c1 sweep
-    (cold and warm-in-frame), scaled to a launch of `alg_bytes` algorithmic bytes
-    when the workload is another one (traffic grows with the vertices swept)."""
+def profile_traffic(alg_bytes, workload):
+    """DRAM bytes per sweep launch from the committed ncu summary of this workload's
+    sweep, else the c1 one (cold and warm-in-frame) scaled to a launch of `alg_bytes`
+    algorithmic bytes (traffic grows with the vertices swept)."""
+    own = os.path.join(ROOT, "profiles", f"vbd_sweep_{workload}_ncu.json")
+    if workload != "c1" and os.path.exists(own):
+        try:
+            d = json.load(open(own))
+            return d["dram_bytes_per_launch"], None, "ncu capture of this workload's sweep (cold caches)"
+        except Exception:
+            pass
     p = os.path.join(ROOT, "profiles", "vbd_sweep_c1_ncu.json")
     if not os.path.exists(p):
         return None, None, None
@@ -328,7 +335,7 @@ def run_ours(args):
     e2e_s = float(sharding.allreduce_stats([e2e_s], op="max")[0])
     state_bytes = 2 * 3 * 4 * info.num_verts
 
-    traffic = profile_traffic(bytes_launch)
+    traffic = profile_traffic(bytes_launch, args.workload)
     out = None
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
