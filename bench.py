@@ -1,45 +1,58 @@
 """Benchmark of the CUDA cloth solver (one JSON line on rank 0).
 
-Workload (a step = one simulated frame): a 512 x 512-vertex grid cloth
-(262,144 vertices, 784,385 edges, 782,341 bending edges), k = 1e3 N/m,
-k_b = 1e-2, 0.1 kg area-lumped, two top corners pinned, h = 1/60 s,
-plain Vertex Block Descent with 50 iterations x 4 colours per frame, FP32.
+Headline workload (the default, a step = one simulated frame of the whole batch):
+  c4  64 batched grid cloths of side U{64..512} (6,641,977 vertices), k = 1e3 N/m,
+      k_b = 1e-2, 0.1 kg area-lumped each, two corners pinned, a random wind force
+      per instance per frame, h = 1/60 s. The warm-start network is trained first on
+      60 recorded plain frames of the batch (seeds 0..59; 150k Adam steps).
+      Two forms, each iterated to the SAME fixed relative residual
+      r = ||grad G(x)|| / ||grad G(y)|| <= --tol (1e-4) with an iteration cap
+      (--cap 200), probes every --check-every (10) iterations, converged instances
+      skipped:
+        learned  predict, the network's guess (potential fallback per instance), VBD;
+        plain    predict, VBD (the reference's method, batched).
+      Both run from the same frame-start state each frame (held-out wind seeds
+      10010+); the plain frame's end state starts the next frame.
 
-  value  frames/s with the state resident in HBM, device-timed (CUDA events on
-         the launching stream, one event pair per frame, L2 flushed between frames
-         outside the event pairs), summed over ranks.
-  e2e    frames/s through the public C ABI with host arrays: every frame uploads
-         the state (x, v) from pinned host memory, runs the frame and reads (x, v)
-         back into it (wall clock around the calls, which synchronise).
-  roofline  the colour-sweep kernel: algorithmic bytes per launch
-         (40 V + 12 E + 56 B per iteration, shared by colour) over its mean
-         CUDA-event duration, against the measured HBM copy bandwidth.
-  cpu_baseline  the CPU oracle (a C++ restatement of the reference's CPU VBD,
-         the reference itself does not build here) on a bounded sample of the
-         same workload, rank 0 only.
-  xpbd   the same cloth solved by XPBD instead (CUDA-graph frames of 50 x
-         (stretch + bending colours) projections): frames/s and bandwidth.
+  value  frames/s of the learned form, device-timed (CUDA events around each whole
+         frame, host probes included), with the plain form's frames/s, the speed-up
+         and p50 / p99 beside it; the working set (1.4 GB) is far larger than L2.
+  tolerance  whether 1e-4 is reached under the cap (fraction of instance-frames),
+         and a sweep over tolerances 0.5 .. 1e-4: iterations to each tolerance from
+         FP64 residual traces of both forms, and timed frames to each tolerance.
+  e2e    the learned frame through the public C ABI with host arrays: every frame
+         uploads (x, v) from pinned host memory and reads them back (wall clock).
+  roofline  vbd_sweep_list_kernel, the colour sweep of these frames: algorithmic
+         bytes per launch (40 V + 12 E + 56 B per iteration, shared by colour) over
+         its per-launch time, measured in this run as 50 listed iterations timed with
+         CUDA events (predict, update and two probes included, so a lower bound),
+         against the measured HBM copy bandwidth.
+  cpu_baseline  the CPU oracle (a C++ restatement of the reference's CPU VBD; the
+         reference itself does not build here) iterating the same plain form to the
+         same tolerance and cap on a sample (instance 0, 55,696 of 6,641,977
+         vertices), with all host cores, scaled to the batch by vertex count.
+  gpu_launches  library kernels launched in the timed region (ats_kernel_launches:
+         direct launches plus the kernel nodes of graph replays).
+  extras (N = 1)  c1 (one 512^2 cloth, plain VBD, 50 iterations, L2-resident) frames/s
+         and sweep roofline; the same cloth under XPBD.
 
---impl reference times that CPU implementation alone on this workload with all
-host threads (each step = 10 of the frame's 50 iterations, scaled to frames/s).
+--impl reference: the CPU oracle alone on this workload's plain form (the same tol /
+cap / probes), each step one frame of the sample, scaled to the batch; the median of
+the steps with all host cores, and a 1-core median of 5 frames beside it.
 
-Other workloads (--workload):
-  c2  256 batched cloths of side U{16..256} with random materials and pins, plain
-      VBD, one launch per colour over all instances; the same keys as c1.
-  c3  a 128 x 128 cloth with a random wind per frame, 200 iterations; c4 64 batched
-      cloths of side U{64..512} with wind, 50 iterations. Both record plain frames,
-      train the warm-start network on the GPU and compare, on held-out frames,
-      plain VBD with learned-guess frames that stop at each instance's plain
-      residual (libatssim_b200/learned.py describes the protocol).
+Other workloads (--workload): c1 (512^2 cloth, plain VBD, fixed 50 iterations), c2
+(256 batched cloths, plain VBD, fixed 50 iterations), c3 (one 128^2 cloth with wind,
+the c4 protocol). Each prints its own metric name.
 
-Multi-GPU: the single cloth does not partition (a graph split would need a halo
-exchange per colour), so N > 1 runs N independent replicas ("weak" scaling); c2
-shards its instances over the ranks ("strong" scaling). Timing is the max over
-ranks.
+Multi-GPU: c4's instances are independent, so N ranks split them by balanced
+bin-packing (no collective on the data path, "strong" scaling: the batch is fixed);
+each rank trains its own network on its own instances; frame times are the max over
+ranks. c1 runs N replicas ("weak").
 """
 import argparse
 import json
 import os
+import platform
 import sys
 import threading
 import time
@@ -51,10 +64,18 @@ sys.path.insert(0, ROOT)
 
 METRIC = "frames/s to 1e-4 residual: batched+learned VBD vs plain CUDA VBD, 1 B200"
 UNIT = "frames/s"
-WORKLOAD = "c1: 512x512 grid cloth, plain VBD, 50 iterations x 4 colours per frame"
-WORKLOAD_C2 = "c2: 256 batched grid cloths, side U{16..256}, plain VBD, 50 iterations per frame"
-ITERS = 50
-REF_SAMPLE_ITERS = 10
+WORKLOADS = {
+    "c4": "c4: 64 batched grid cloths, side U{64..512}, wind per instance; batched+learned vs plain batched VBD, "
+          "both iterated to a relative residual of {tol:g} (cap {cap} iterations, probes every {check})",
+    "c3": "c3: 128x128 grid cloth, wind per frame; learned vs plain VBD, both iterated to a relative residual of "
+          "{tol:g} (cap {cap} iterations, probes every {check})",
+    "c1": "c1: 512x512 grid cloth, plain VBD, 50 iterations x 4 colours per frame",
+    "c2": "c2: 256 batched grid cloths, side U{16..256}, plain VBD, 50 iterations per frame",
+}
+METRICS = {"c1": "frames/s, plain VBD, 50 iterations, 512x512 cloth",
+           "c2": "frames/s, plain batched VBD, 50 iterations, 256 cloths",
+           "c3": "frames/s to {tol:g} residual: learned VBD vs plain CUDA VBD, 128x128 cloth"}
+SWEEP_TOLS = [0.5, 0.3, 0.2, 1e-1, 1e-2, 1e-3, 1e-4]
 
 
 def parse():
@@ -63,29 +84,50 @@ def parse():
     p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--workload", default="c4", choices=["c1", "c2", "c3", "c4"])
+    p.add_argument("--tol", type=float, default=1e-4)
+    p.add_argument("--cap", type=int, default=200)
+    p.add_argument("--check-every", type=int, default=10)
+    p.add_argument("--train-steps", type=int, default=150000)
+    p.add_argument("--sweep-cap", type=int, default=400, help="iterations of the residual traces")
+    p.add_argument("--trace-out", default="", help="write the full residual traces (JSON) here")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-extras", action="store_true")
     p.add_argument("--tpv", type=int, default=0)
     p.add_argument("--block", type=int, default=0)
-    p.add_argument("--workload", default="c1", choices=["c1", "c2", "c3", "c4"],
-                   help="c1: 512x512 cloth (the headline); c2: 256 batched instances; c3: learned warm start on a "
-                        "128x128 cloth; c4: 64 batched instances with the learned warm start")
     return p.parse_args()
 
 
 def dist_env():
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return rank, world, local
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
 
 
 def alg_bytes_per_iter(nv, ne, nb):
     return 40 * nv + 12 * ne + 56 * nb
 
 
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return platform.processor() or "unknown"
+
+
+def hbm_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        try:
+            return float(json.load(open(path))["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
 class ClockSampler:
-    """SM clock and throttle reasons polled through NVML during the timed region
-    (nvidia-smi's 200 ms period is longer than the region itself)."""
+    """SM clock and throttle reasons polled through NVML during the timed region."""
 
     REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
                0x80: "hw_power_brake_slowdown"}
@@ -97,6 +139,7 @@ class ClockSampler:
         self.stop_flag = False
         self.handle = None
         self.max_mhz = None
+        self.t = None
 
     def start(self):
         try:
@@ -108,7 +151,7 @@ class ClockSampler:
             self.handle = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
             self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.handle, pynvml.NVML_CLOCK_SM)
             self.nvml = pynvml
-        except Exception as e:  # no NVML: report it
+        except Exception as e:  # no NVML: say so in the line
             self.error = str(e)
             return
         self.t = threading.Thread(target=self._poll, daemon=True)
@@ -125,28 +168,73 @@ class ClockSampler:
                         self.reasons.add(name)
             except Exception:
                 pass
-            time.sleep(0.002)
+            time.sleep(0.005)
 
     def stop(self):
         self.stop_flag = True
         if self.handle is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "note": getattr(self, "error", "no NVML")}
-        self.t.join(timeout=2)
+        if self.t:
+            self.t.join(timeout=2)
         return {"sm_mhz": float(np.median(self.samples)) if self.samples else None, "sm_max_mhz": self.max_mhz,
                 "reasons": sorted(self.reasons), "samples": len(self.samples)}
 
 
-def cpu_port_sample(threads, iters):
-    """Times the CPU oracle on one frame of `iters` iterations of the workload."""
+# ---------------------------------------------------------------- CPU legs (oracle)
+def c4_cpu_sample():
+    """Instance 0 of c4 (236 x 236) and the batch's total vertex count."""
+    from libatssim_b200 import configs
+    insts, prm = configs.c4()
+    return insts[0], prm, sum(i.num_verts for i in insts)
+
+
+def cpu_to_tolerance_frames(threads, frames, tol, cap, check_every, approach=2):
+    """Seconds per frame of the oracle's plain VBD frame iterated to `tol` (cap
+    iterations, probes every check_every) on the c4 sample, after `approach` plain
+    50-iteration frames from rest; winds as instance 0 of the GPU run's frames."""
     from libatssim_b200 import configs
     from oracle import ats_oracle
     ats_oracle.build()
-    insts, prm = configs.c1()
-    inst = insts[0]
-    s = ats_oracle.Scene(inst.positions, inst.faces, inst.mass, inst.fixed, dt=prm["implicit_dt"],
-                         substeps=1, iterations=iters, k_stretch=inst.k_stretch, k_bend=inst.k_bend,
+    inst, prm, _ = c4_cpu_sample()
+    s = ats_oracle.Scene(inst.positions, inst.faces, inst.mass, inst.fixed, dt=prm["implicit_dt"], substeps=1,
+                         iterations=prm["iterations"], k_stretch=inst.k_stretch, k_bend=inst.k_bend,
                          damping=prm["damping"], threads=threads)
-    return s
+    total = float(inst.mass.sum())
+    for f in range(approach):
+        s.set_gravity(configs.wind_accel(np.random.RandomState(10000 + f), total))
+        s.frame()
+    times, iters, res = [], [], []
+    for f in range(frames):
+        s.set_gravity(configs.wind_accel(np.random.RandomState(10010 + f), total))
+        t = time.perf_counter()
+        it, r = s.frame_to_residual(tol, check_every=check_every, max_iterations=cap)
+        times.append(time.perf_counter() - t)
+        iters.append(it)
+        res.append(r)
+    s.close()
+    return np.array(times), np.array(iters), np.array(res)
+
+
+def cpu_plain_fixed_frames(threads, frames, workload):
+    """Seconds per frame of the oracle's plain VBD frame (the handle's full iteration
+    count) on c1's cloth or on a c2 sample instance; returns (times, vertices of the
+    sample, vertices of the workload)."""
+    from libatssim_b200 import configs
+    from oracle import ats_oracle
+    ats_oracle.build()
+    insts, prm = configs.c1() if workload == "c1" else configs.c2()
+    inst = insts[0]
+    s = ats_oracle.Scene(inst.positions, inst.faces, inst.mass, inst.fixed, dt=prm["implicit_dt"], substeps=1,
+                         iterations=prm["iterations"], k_stretch=inst.k_stretch, k_bend=inst.k_bend,
+                         damping=prm["damping"], threads=threads)
+    s.frame()
+    times = []
+    for _ in range(frames):
+        t = time.perf_counter()
+        s.frame()
+        times.append(time.perf_counter() - t)
+    s.close()
+    return np.array(times), inst.num_verts, sum(i.num_verts for i in insts)
 
 
 def run_reference(args):
@@ -154,300 +242,408 @@ def run_reference(args):
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    s = cpu_port_sample(threads, REF_SAMPLE_ITERS)
-    for _ in range(args.warmup):
-        s.frame()
-    t = time.perf_counter()
-    for _ in range(args.steps):
-        s.frame()
-    dt = time.perf_counter() - t
-    per_frame = dt / args.steps * (ITERS / REF_SAMPLE_ITERS)
+    wl = args.workload
+    if wl in ("c4", "c3"):
+        if wl == "c3":
+            print(json.dumps({"impl": "reference", "unavailable": "c3 reference arm not provided; use c4"}))
+            return
+        t_all, it_all, r_all = cpu_to_tolerance_frames(threads, args.warmup + args.steps, args.tol, args.cap,
+                                                       args.check_every)
+        t_all = t_all[args.warmup:]
+        t_one, _, _ = cpu_to_tolerance_frames(1, 5, args.tol, args.cap, args.check_every)
+        inst, _, total_v = c4_cpu_sample()
+        scale = total_v / inst.num_verts
+        per_frame = float(np.median(t_all)) * scale
+        one = float(np.median(t_one)) * scale
+        sample = (f"one frame of c4 instance 0 ({inst.num_verts} of {total_v} vertices) per step, plain VBD to "
+                  f"{args.tol:g} (cap {args.cap}, probes every {args.check_every}), scaled by vertex count; "
+                  f"reached tol in {float(np.mean(r_all <= args.tol)):.2f} of frames, mean iterations "
+                  f"{float(np.mean(it_all)):.0f}")
+        config = {"workload": WORKLOADS["c4"].format(tol=args.tol, cap=args.cap, check=args.check_every),
+                  "vertices": total_v, "tol": args.tol, "cap": args.cap, "check_every": args.check_every}
+        metric = METRIC
+    else:
+        t_all, nv_s, nv_t = cpu_plain_fixed_frames(threads, args.warmup + args.steps, wl)
+        t_all = t_all[args.warmup:]
+        t_one, _, _ = cpu_plain_fixed_frames(1, 5, wl)
+        scale = nv_t / nv_s
+        per_frame = float(np.median(t_all)) * scale
+        one = float(np.median(t_one)) * scale
+        sample = (f"full frames of 50 iterations of {'the cloth' if wl == 'c1' else 'c2 instance 0'}"
+                  + (f", scaled by vertex count ({nv_s} of {nv_t})" if scale != 1 else ""))
+        config = {"workload": WORKLOADS[wl], "vertices": nv_t, "iterations": 50}
+        metric = METRICS[wl]
     fps = 1.0 / per_frame
-    out = {"impl": "reference", "metric": METRIC, "value": fps, "unit": UNIT, "n_gpus": args.gpus,
+    out = {"impl": "reference", "metric": metric, "value": fps, "unit": UNIT, "n_gpus": args.gpus,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_frame * 1e3, "higher_is_better": True,
-           "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-           "config": {"workload": WORKLOAD, "vertices": 262144, "iterations": ITERS, "frames": args.steps},
-           "cpu_baseline": {"value": fps, "unit": UNIT, "cores": threads, "kind": "port",
-                            "sample": f"{REF_SAMPLE_ITERS} of {ITERS} iterations per frame, scaled; "
-                                      "C++ restatement of examples/example2_async_iter.cpp VBD"},
+           "scaling": "strong" if wl == "c4" else "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+           "config": config,
+           "cpu_baseline": {"value": fps, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample,
+                            "statistic": f"median of {args.steps} steps", "cpu_model": cpu_model(),
+                            "nproc": os.cpu_count(),
+                            "one_core": {"value": 1.0 / one, "unit": UNIT, "cores": 1, "statistic": "median of 5"}},
            "e2e": {"value": fps, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
 
 
-def profile_traffic(alg_bytes, workload):
-    """DRAM bytes per sweep launch from the committed ncu summary of this workload's
-    sweep, else the c1 one (cold and warm-in-frame) scaled to a launch of `alg_bytes`
-    algorithmic bytes (traffic grows with the vertices swept)."""
-    own = os.path.join(ROOT, "profiles", f"vbd_sweep_{workload}_ncu.json")
-    if workload != "c1" and os.path.exists(own):
-        try:
-            d = json.load(open(own))
-            return d["dram_bytes_per_launch"], None, "ncu capture of this workload's sweep (cold caches)"
-        except Exception:
-            pass
-    p = os.path.join(ROOT, "profiles", "vbd_sweep_c1_ncu.json")
-    if not os.path.exists(p):
-        return None, None, None
-    try:
-        d = json.load(open(p))
-        scale = alg_bytes / d["alg_bytes_per_launch"]
-        src = "ncu capture of this launch" if abs(scale - 1.0) < 1e-9 else \
-            "ncu capture of the c1 sweep (512^2), scaled by algorithmic bytes"
-        return d["dram_bytes_per_launch"] * scale, d["dram_bytes_per_launch_warm"] * scale, src
-    except Exception:
-        return None, None, None
-
-
-def run_ours(args):
+# ---------------------------------------------------------------- GPU arm
+def init_dist(world, local):
     import torch
-    rank, world, local = dist_env()
     torch.cuda.set_device(local)
     if world > 1:
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    import libatssim_b200 as ats
-    from libatssim_b200 import build, configs
-    build.build()
+
+
+def maxrank(v):
     from libatssim_b200 import sharding
-    insts, prm = configs.c1() if args.workload == "c1" else configs.c2()
-    sharded = args.workload == "c2" and world > 1
-    if sharded:
-        insts, _ = sharding.shard(insts, prm["iterations"])  # this rank's instances, no data-path collective
-    t_create = time.perf_counter()
-    cloth = ats.Cloth(insts, threads_per_vertex=args.tpv, block_size=args.block, **prm)
-    t_create = time.perf_counter() - t_create
-    stream = torch.cuda.current_stream()
-    tuned = None
-    if not args.tpv and not args.block:
-        tuned = cloth.autotune(iterations=20, stream=stream)
+    return float(sharding.allreduce_stats([float(v)], op="max")[0])
+
+
+def sweep_roofline(cloth, stream, reps=3, iters=50):
+    """Per-launch time of vbd_sweep_list_kernel: `iters` listed iterations over every
+    instance (a to-residual frame with tol 0 and one probe at the cap), CUDA-event
+    timed; predict, update and the probes are inside, so this bounds the sweep from
+    above. Returns (ms per launch, frame ms, algorithmic bytes per launch)."""
+    import torch
+    info = cloth.info
+    x0, v0 = cloth.state(stream=stream)
+    ms = []
+    for _ in range(reps):
+        cloth.set_state(x0, v0, stream=stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        cloth.frame_to_residual(0.0, check_every=iters, max_iterations=iters, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    cloth.set_state(x0, v0, stream=stream)
+    frame_ms = float(np.median(ms))
+    per_launch = frame_ms / (iters * info.num_vertex_colors)
+    bytes_launch = alg_bytes_per_iter(info.num_verts, info.num_edges, info.num_bending_edges) / info.num_vertex_colors
+    return per_launch, frame_ms, bytes_launch
+
+
+def plain_extras(stream, peak):
+    """c1 (one 512^2 cloth, L2-resident): plain VBD CUDA-graph frames and XPBD frames,
+    each L2-flushed between frames, device-timed; the sweep per launch from a graph
+    frame of 50 iterations."""
+    import torch
+
+    import libatssim_b200 as ats
+    from libatssim_b200 import configs
+    insts, prm = configs.c1()
+    cloth = ats.Cloth(insts, **prm)
+    cloth.autotune(iterations=20, stream=stream)
     info = cloth.info
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
 
-    def barrier():
+    def timed(solver, frames):
+        for _ in range(3):
+            cloth.frame(solver, stream=stream, graph=True)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(frames)]
+        torch.cuda.synchronize()
+        for i in range(frames):
+            flush.fill_(i & 0xFF)
+            ev[i][0].record(stream)
+            cloth.frame(solver, stream=stream, graph=True)
+            ev[i][1].record(stream)
+        torch.cuda.synchronize()
+        return np.array([a.elapsed_time(b) for a, b in ev])
+
+    vbd_ms = timed(ats.SOLVER_VBD, 200)
+    launches = 50 * info.num_vertex_colors
+    per_launch_upper = float(np.median(vbd_ms)) / launches  # predict and update inside: an upper bound
+    bytes_launch = alg_bytes_per_iter(info.num_verts, info.num_edges, info.num_bending_edges) / info.num_vertex_colors
+    xpbd_ms = timed(ats.SOLVER_XPBD, 50)
+    xpbd_bytes = (28 * info.num_verts + 20 * info.num_edges + 64 * info.num_bending_edges) * 50
+    out = {"workload": WORKLOADS["c1"], "frames_per_s": 1e3 / float(np.mean(vbd_ms)),
+           "ms_per_frame_p50": float(np.median(vbd_ms)), "frames_timed": int(len(vbd_ms)),
+           "sweep": {"kernel": f"vbd_sweep_kernel<{info.threads_per_vertex}>",
+                     "us_per_launch_upper_bound": per_launch_upper * 1e3,
+                     "achieved_gbs_lower_bound": bytes_launch / (per_launch_upper * 1e-3) / 1e9,
+                     "frac_of_measured_hbm": bytes_launch / (per_launch_upper * 1e-3) / 1e9 / peak,
+                     "note": "the 64 MB working set is L2-resident inside a frame: an L2 figure, not HBM"},
+           "xpbd": {"frames_per_s": 1e3 / float(np.mean(xpbd_ms)), "ms_per_frame_p50": float(np.median(xpbd_ms)),
+                    "launches_per_frame": 3 + 50 * (info.num_stretch_colors + info.num_bending_colors),
+                    "achieved_gbs": xpbd_bytes / (float(np.median(xpbd_ms)) * 1e-3) / 1e9,
+                    "frac_of_measured_hbm": xpbd_bytes / (float(np.median(xpbd_ms)) * 1e-3) / 1e9 / peak}}
+    cloth.close()
+    del flush
+    return out
+
+
+def run_learned(args):
+    """c4 (or c3): learned and plain forms to the same fixed tolerance."""
+    import torch
+    rank, world, local = dist_env()
+    init_dist(world, local)
+    import libatssim_b200 as ats
+    from libatssim_b200 import build, configs, learned, sharding
+    build.build()
+    wl = args.workload
+    if wl == "c4":
+        all_insts, prm = configs.c4()
+        traj, frames = 2, 30
+    else:
+        all_insts, prm = configs.c3()
+        traj, frames = 20, 100
+    insts = all_insts
+    if world > 1:
+        insts, _ = sharding.shard(all_insts, args.cap)
+    rec_iters = prm["iterations"]
+    stream = torch.cuda.current_stream()
+    t0 = time.perf_counter()
+    cloth = ats.Cloth(insts, **prm)
+    t_create = time.perf_counter() - t0
+    tuned = cloth.autotune(iterations=20, stream=stream)
+    info = cloth.info
+    nv = info.num_verts
+    # training data: plain frames of this rank's instances
+    ds = ats.Dataset(traj * frames * nv)
+    t0 = time.perf_counter()
+    learned.record(cloth, insts, ds, traj, frames, rec_iters, seed0=0)
+    torch.cuda.synchronize()
+    t_record = time.perf_counter() - t0
+    model, loss, t_train = learned.train(ds, steps=args.train_steps)
+    ds.close()
+
+    # the measured frames: a moving cloth, held-out winds
+    learned.approach(cloth, insts, 10, seed0=10000, stream=stream)
+    clocks = ClockSampler(local)
+    launches = {}
+
+    def on_timed(start):
+        # the timed frames are bracketed by a barrier and a device synchronisation
         if world > 1:
             torch.distributed.barrier()
         torch.cuda.synchronize()
+        if start:
+            clocks.start()
+            launches["a"] = ats.kernel_launches()
+        else:
+            launches["b"] = ats.kernel_launches()
 
-    # warm-up (also captures the frame graph)
-    for _ in range(args.warmup):
-        cloth.frame(stream=stream, graph=True)
-    torch.cuda.synchronize()
-
-    # --- device-timed frames, L2 flushed between frames outside the event pairs
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    clocks = ClockSampler(local)
-    clocks.start()
-    barrier()
-    for i in range(args.steps):
-        flush.fill_(i & 0xFF)
-        starts[i].record(stream)
-        cloth.frame(stream=stream, graph=True)
-        ends[i].record(stream)
-    barrier()
+    res = learned.fixed_tolerance_frames(cloth, insts, model, args.tol, args.cap, args.check_every, args.steps,
+                                         args.warmup, seed0=10010, stream=stream, on_timed=on_timed)
     clk = clocks.stop()
-    ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
-    ms = float(sharding.allreduce_stats([ms], op="max")[0])  # max over ranks
-    ms_per_step = ms / args.steps
-    # replicas: every rank advances a whole cloth per step; sharded c2: all ranks
-    # together advance the 256 instances once per step
-    value = (1 if sharded else world) * 1e3 / ms_per_step
+    lm, pm = res["learned_ms"], res["plain_ms"]
+    learned_ms = maxrank(np.mean(lm))
+    plain_ms = maxrank(np.mean(pm))
+    reached_l = float(np.mean(res["learned_res"] <= args.tol))
+    reached_p = float(np.mean(res["plain_res"] <= args.tol))
+    vw = np.array([i.num_verts for i in insts], dtype=np.float64)
+    its_l = float(np.sum(res["learned_iters"] * vw) / (vw.sum() * len(lm)))
+    its_p = float(np.sum(res["plain_iters"] * vw) / (vw.sum() * len(pm)))
 
-    # --- residual reached after the frame's iterations (reported, not timed)
-    x_end, v_end = cloth.state()
-    cloth.predict(stream=stream)
-    r0 = cloth.residual(stream=stream)[0]
-    for _ in range(ITERS):
-        for c in range(info.num_vertex_colors):
-            cloth.vbd_color_sweep(c, stream=stream)
-    r1 = cloth.residual(stream=stream)[0]
-    cloth.set_state(x_end, v_end, stream=stream)
+    # sweep roofline in this run (listed sweep over all instances)
+    per_launch, rf_frame_ms, bytes_launch = sweep_roofline(cloth, stream)
+    peak, peak_src = hbm_peak()
+    achieved = bytes_launch / (per_launch * 1e-3) / 1e9
+    sweeps_per_learned_frame = float(np.mean(res["learned_iters"].max(axis=1))) * info.num_vertex_colors
 
-    # --- per-launch sweep duration: CUDA events around ITERS back-to-back iterations
-    # (ITERS x colours sweep launches, chained by programmatic dependent launch as in
-    # the frame), L2 flushed before each repetition as between timed frames
-    reps = []
-    for rep in range(3):
-        flush.fill_(rep)
-        cloth.predict(stream=stream)
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        cloth.vbd_iterations(ITERS, stream=stream)
-        e1.record(stream)
-        cloth.update_velocity(stream=stream)
-        reps.append((e0, e1))
-    torch.cuda.synchronize()
-    mean_sweep_ms = float(np.mean([a.elapsed_time(b) for a, b in reps])) / (ITERS * info.num_vertex_colors)
-    bytes_iter = alg_bytes_per_iter(info.num_verts, info.num_edges, info.num_bending_edges)
-    bytes_launch = bytes_iter / info.num_vertex_colors
-    achieved = bytes_launch / (mean_sweep_ms * 1e-3) / 1e9
-    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    if os.path.exists(peaks_path):
-        peak = float(json.load(open(peaks_path))["hbm_gbs"])
-        peak_src = "measured"
-    else:
-        peak, peak_src = 6650.0, "fallback"
-
-    # --- XPBD at the same scale (the reference's other solver): CUDA-graph frames of
-    # predict, lambda reset, ITERS x (stretch colours + bending colours) projections and
-    # update, L2 flushed between frames; algorithmic bytes 28 V + 20 E + 64 B per iteration
-    x_keep, v_keep = cloth.state()
-    for _ in range(2):
-        cloth.frame(ats.SOLVER_XPBD, stream=stream, graph=True)
-    xpbd_ms = []
-    for i in range(max(3, min(args.steps, 10))):
-        flush.fill_(i & 0xFF)
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        cloth.frame(ats.SOLVER_XPBD, stream=stream, graph=True)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        xpbd_ms.append(e0.elapsed_time(e1))
-    xpbd_frame_ms = float(sharding.allreduce_stats([float(np.median(xpbd_ms))], op="max")[0])
-    xpbd_bytes = (28 * info.num_verts + 20 * info.num_edges + 64 * info.num_bending_edges) * ITERS
-    cloth.set_state(x_keep, v_keep, stream=stream)
-    xpbd = {"frames_per_s": (1 if sharded else world) * 1e3 / xpbd_frame_ms, "ms_per_frame": xpbd_frame_ms,
-            "launches_per_frame": 3 + ITERS * (info.num_stretch_colors + info.num_bending_colors),
-            "achieved_gbs": xpbd_bytes / (xpbd_frame_ms * 1e-3) / 1e9,
-            "note": "whole-frame algorithmic bytes (28V+20E+64B per iteration) over the device-timed frame"}
-
-    # --- end to end through the public API with host arrays: every frame uploads the
-    # state (x, v) from pinned host memory, runs the frame and reads (x, v) back into it
-    x_h = torch.empty((info.num_verts, 3), dtype=torch.float32, pin_memory=True).numpy()
-    v_h = torch.empty((info.num_verts, 3), dtype=torch.float32, pin_memory=True).numpy()
+    # end to end through the C ABI with host arrays
+    x_h = torch.empty((nv, 3), dtype=torch.float32, pin_memory=True).numpy()
+    v_h = torch.empty((nv, 3), dtype=torch.float32, pin_memory=True).numpy()
     cloth.state_into(x_h, v_h, stream=stream)
-    e2e_steps = max(3, min(args.steps, 10))
-    for _ in range(2):  # warm-up of the host path
+    masses = [float(i.mass.sum()) for i in insts]
+    e2e_frames = 5
+    for f in range(e2e_frames + 1):
+        if f == 1:
+            if world > 1:
+                torch.distributed.barrier()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+        cloth.set_accel(learned.wind_table(np.random.RandomState(20000 + f), masses), stream=stream)
         cloth.set_state(x_h, v_h, stream=stream)
-        cloth.frame(stream=stream, graph=True)
+        cloth.frame_warm_to_residual(model, args.tol, check_every=args.check_every, max_iterations=args.cap,
+                                     stream=stream)
         cloth.state_into(x_h, v_h, stream=stream)
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        cloth.set_state(x_h, v_h, stream=stream)
-        cloth.frame(stream=stream, graph=True)
-        cloth.state_into(x_h, v_h, stream=stream)
-    barrier()
-    e2e_s = (time.perf_counter() - t0) / e2e_steps
-    e2e_s = float(sharding.allreduce_stats([e2e_s], op="max")[0])
-    state_bytes = 2 * 3 * 4 * info.num_verts
+    torch.cuda.synchronize()
+    e2e_s = maxrank((time.perf_counter() - t0) / e2e_frames)
+    state_bytes = 2 * 3 * 4 * nv
 
-    traffic = profile_traffic(bytes_launch, args.workload)
+    sweep, trace, timed_tols = None, None, None
+    if world == 1:
+        points = sorted(set([0, 1, 2, 3, 5, 7, 10, 15, 20, 30, 40, 50, 70, 100, 150, 200, 300, 400, 600, 800, 1000,
+                             1500, 2000, 3000, 4000, 5000]) | {args.sweep_cap})
+        points = [p for p in points if p <= args.sweep_cap]
+        sweep, trace = learned.tolerance_sweep(cloth, insts, model, SWEEP_TOLS, points, 2, seed0=30000,
+                                               stream=stream)
+        timed_tols = [learned.timed_to_tolerance(cloth, insts, model, t, args.cap, args.check_every, 2,
+                                                 seed0=40000 + 10 * k, stream=stream)
+                      for k, t in enumerate(SWEEP_TOLS[:-1])]
+        if args.trace_out:
+            os.makedirs(os.path.dirname(os.path.abspath(args.trace_out)), exist_ok=True)
+            json.dump({"workload": wl, "sweep": sweep, "trace": trace, "timed": timed_tols},
+                      open(args.trace_out, "w"), indent=1)
+
+    extras = None
+    if world == 1 and not args.no_extras:
+        extras = plain_extras(stream, peak)
+
     out = None
     if rank == 0:
-        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-               "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
-               "scaling": "strong" if sharded else "weak",
-               "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-               "config": {"workload": WORKLOAD if args.workload == "c1" else WORKLOAD_C2,
-                          "instances": info.num_instances, "create_s": t_create, "vertices": info.num_verts, "edges": info.num_edges,
-                          "bending_edges": info.num_bending_edges, "colors": info.num_vertex_colors,
-                          "iterations": ITERS, "threads_per_vertex": info.threads_per_vertex,
-                          "block_size": info.block_size, "autotuned": tuned is not None,
-                          "parallelism": f"instance-shards{world}" if sharded else f"replicas{world}",
-                          "l2": "flushed between frames (256 MiB write, outside the event pairs)"},
-               "residual": {"relative_after_frame": float(r1 / r0), "definition":
-                            "||grad G(x)|| / ||grad G(y)||, FP64, free vertices"},
-               "e2e": {"value": (1 if sharded else world) / e2e_s, "unit": UNIT, "h2d_bytes_per_step": state_bytes,
-                       "d2h_bytes_per_step": state_bytes},
+        value = 1e3 / learned_ms
+        plain_fps = 1e3 / plain_ms
+        tol_s = f"{args.tol:g}"
+        out = {"metric": METRIC if wl == "c4" else METRICS["c3"].format(tol=args.tol), "value": value, "unit": UNIT,
+               "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": learned_ms,
+               "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+               "dtype": "f32 (MLP bf16 / fp32 accumulate; residuals fp64)", "data": "synthetic",
+               "config": {"workload": WORKLOADS[wl].format(tol=args.tol, cap=args.cap, check=args.check_every),
+                          "instances": len(all_insts), "vertices": sum(i.num_verts for i in all_insts),
+                          "tol": args.tol, "cap": args.cap, "check_every": args.check_every,
+                          "parallelism": f"instance-shards{world}", "create_s": t_create,
+                          "threads_per_vertex": info.threads_per_vertex, "block_size": info.block_size,
+                          "autotuned": list(tuned),
+                          "l2": "inputs larger than L2 (1.4 GB working set per frame); no flush"},
+               "headline": {"form": "learned (batched + learned warm start)", "learned_fps": value,
+                            "plain_fps": plain_fps, "speedup_vs_plain": plain_ms / learned_ms,
+                            "target_speedup": 2.0, "pass_2x": bool(plain_ms / learned_ms >= 2.0 and
+                                                                   reached_l >= 1.0),
+                            "learned_ms_p50": float(np.percentile(lm, 50)),
+                            "learned_ms_p99": float(np.percentile(lm, 99)),
+                            "plain_ms_p50": float(np.percentile(pm, 50)),
+                            "plain_ms_p99": float(np.percentile(pm, 99)),
+                            "reached_tol_fraction": {"learned": reached_l, "plain": reached_p},
+                            "iterations_vertex_weighted": {"learned": its_l, "plain": its_p},
+                            "residual_at_stop_median": {"learned": float(np.median(res["learned_res"])),
+                                                        "plain": float(np.median(res["plain_res"]))},
+                            "guess_kept_fraction": float(res["used"].mean()),
+                            "verdict": (f"{tol_s} reached by {reached_l:.0%} (learned) / {reached_p:.0%} (plain) "
+                                        f"of instance-frames within {args.cap} iterations; speed-up "
+                                        f"{plain_ms / learned_ms:.2f}x against the 2x target")},
+               "tolerance_sweep": sweep, "timed_to_tolerance": timed_tols,
+               "e2e": {"value": 1.0 / e2e_s, "unit": UNIT, "h2d_bytes_per_step": state_bytes,
+                       "d2h_bytes_per_step": state_bytes,
+                       "path": "ats_set_state from pinned host, ats_frame_warm_to_residual, ats_get_state to pinned "
+                               "host; wall clock"},
                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                            "frac": achieved / peak, "traffic": traffic[0], "traffic_warm_in_frame": traffic[1],
-                            "traffic_source": traffic[2],
-                            "kernel": f"vbd_sweep_kernel<{info.threads_per_vertex}>", "mean_launch_us": mean_sweep_ms * 1e3,
-                            "alg_bytes_per_launch": bytes_launch, "peak_source": peak_src},
-               "gpu_launches": args.steps * (2 + ITERS * info.num_vertex_colors),
+                            "frac": achieved / peak, "traffic": None,
+                            "traffic_note": "not captured in this run; the committed ncu summaries under profiles/ "
+                                            "hold the DRAM bytes of this kernel",
+                            "kernel": f"vbd_sweep_list_kernel<{info.threads_per_vertex}>",
+                            "us_per_launch_upper_bound": per_launch * 1e3, "alg_bytes_per_launch": bytes_launch,
+                            "timing": "50 listed iterations over all instances, CUDA events, predict/update/2 probes "
+                                      "included", "peak_source": peak_src,
+                            "sweeps_per_learned_frame": sweeps_per_learned_frame,
+                            "sweep_share_of_learned_frame_upper": sweeps_per_learned_frame * per_launch / learned_ms},
+               "gpu_launches": int(launches.get("b", 0) - launches.get("a", 0)),
                "clocks": clk,
-               "xpbd": dict(xpbd, frac_of_peak=xpbd["achieved_gbs"] / peak)}
-    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "c1":
+               "train": {"samples": traj * frames * nv, "record_s": t_record, "train_s": t_train,
+                         "steps": args.train_steps, "final_loss_normalised": loss}}
+        if extras is not None:
+            out["extras"] = extras
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and wl == "c4":
         threads = os.cpu_count() or 1
-        s = cpu_port_sample(threads, REF_SAMPLE_ITERS)
-        s.frame()
-        t = time.perf_counter()
-        n = 2
-        for _ in range(n):
-            s.frame()
-        per_frame = (time.perf_counter() - t) / n * (ITERS / REF_SAMPLE_ITERS)
+        t_cpu, it_cpu, r_cpu = cpu_to_tolerance_frames(threads, 3, args.tol, args.cap, args.check_every)
+        inst0, _, total_v = c4_cpu_sample()
+        per_frame = float(np.median(t_cpu)) * total_v / inst0.num_verts
         out["cpu_baseline"] = {"value": 1.0 / per_frame, "unit": UNIT, "cores": threads, "kind": "port",
-                               "sample": f"{n} frames of {REF_SAMPLE_ITERS}/{ITERS} iterations, scaled"}
+                               "sample": f"c4 instance 0 ({inst0.num_verts} of {total_v} vertices), 3 frames of plain "
+                                         f"VBD to {args.tol:g} (cap {args.cap}; mean iterations "
+                                         f"{float(np.mean(it_cpu)):.0f}), median, scaled by vertex count",
+                               "cpu_model": cpu_model(), "nproc": os.cpu_count()}
     if out is not None:
         print(json.dumps(out), flush=True)
+    model.close()
     cloth.close()
     if world > 1:
         torch.distributed.destroy_process_group()
 
 
-def run_learned(args):
-    """c3 / c4: plain VBD against the learned warm start, frames/s to the plain
-    solver's own residual (libatssim_b200/learned.py describes the protocol)."""
+def run_plain(args):
+    """c1 / c2: plain VBD, fixed 50 iterations, CUDA-graph frames."""
     import torch
     rank, world, local = dist_env()
-    torch.cuda.set_device(local)
+    init_dist(world, local)
     import libatssim_b200 as ats
-    from libatssim_b200 import build, configs, learned
+    from libatssim_b200 import build, configs, sharding
     build.build()
-    if args.workload == "c3":
-        insts, prm = configs.c3()
-        trajectories, frames, eval_traj, eval_frames, skip = 20, 100, 2, 40, 15
-        desc = "c3: 128x128 cloth, wind per frame, 200 iterations; MLP trained on 2000 plain frames (seeds 0-1999)"
-    else:
-        insts, prm = configs.c4()
-        trajectories, frames, eval_traj, eval_frames, skip = 2, 30, 1, 30, 10
-        desc = ("c4: 64 batched cloths, side U{64..512}, wind per instance, 50 iterations; shared MLP trained on "
-                "60 plain frames of the batch")
-    iters = prm["iterations"]
-    cloth = ats.Cloth(insts, **prm)
-    cloth.autotune(iterations=20)
-    nv = cloth.info.num_verts
-    ds = ats.Dataset(trajectories * frames * nv)
-    t = time.perf_counter()
-    learned.record(cloth, insts, ds, trajectories, frames, iters, seed0=0)
-    torch.cuda.synchronize()
-    t_record = time.perf_counter() - t
-    model, loss, t_train = learned.train(ds)
-    ds.close()
-    # probes every 5 iterations, the first one at the previous frame's count minus 3
-    # (c3) or at the 75th percentile of the previous frame's counts (c4)
-    check_every, schedule = (5, "prev") if args.workload == "c3" else (5, 75)
+    insts, prm = configs.c1() if args.workload == "c1" else configs.c2()
+    sharded = args.workload == "c2" and world > 1
+    if sharded:
+        insts, _ = sharding.shard(insts, prm["iterations"])
+    cloth = ats.Cloth(insts, threads_per_vertex=args.tpv, block_size=args.block, **prm)
+    stream = torch.cuda.current_stream()
+    if not args.tpv and not args.block:
+        cloth.autotune(iterations=20, stream=stream)
+    info = cloth.info
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    for _ in range(args.warmup):
+        cloth.frame(stream=stream, graph=True)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     clocks = ClockSampler(local)
     clocks.start()
-    res = learned.evaluate(cloth, insts, model, iters, seed0=10000, trajectories=eval_traj, frames=eval_frames,
-                           skip=skip, check_every=check_every, schedule=schedule, lead=3)
-    per_instance = learned.plain_per_instance_ms(insts, prm) if args.workload == "c4" else None
-    sm = learned.summary(res, iters, per_instance)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    l0 = ats.kernel_launches()
+    for i in range(args.steps):
+        flush.fill_(i & 0xFF)
+        ev[i][0].record(stream)
+        cloth.frame(stream=stream, graph=True)
+        ev[i][1].record(stream)
+    torch.cuda.synchronize()
+    l1 = ats.kernel_launches()
     clk = clocks.stop()
-    sm["check_every"] = check_every
-    sm["probe_schedule"] = ("first at the previous frame's count - 3, then every 5" if schedule == "prev" else
-                            "first at the 75th percentile of the previous frame's counts, then every 5")
-    # fixed budget: the most iterations any to-residual frame needed,
-    # measured on fresh frames (seed0 20000) as a CUDA graph
-    budget = int(min(iters, 5 * np.ceil(np.max(res["learned_iters"]) / 5.0)))
-    fx = learned.evaluate_fixed(cloth, insts, model, budget, iters, seed0=20000, trajectories=eval_traj,
-                                frames=eval_frames, skip=skip)
-    fx["speedup_vs_plain"] = fx["learned_fixed_fps"] / sm["plain_fps"]
-    if per_instance is not None:
-        fx["speedup_vs_unbatched"] = fx["learned_fixed_fps"] * per_instance / 1e3
-    sm["fixed_budget"] = fx
-    # the fixed-budget graph counts only when every instance of every evaluated frame
-    # reached the plain residual; the residual-driven frames always do
-    best = sm["learned_fps"]
-    if fx["reached_plain_residual_fraction"] >= 1.0:
-        best = max(best, fx["learned_fixed_fps"])
-    sm["headline_arm"] = "fixed_budget" if best != sm["learned_fps"] else "to_residual"
-    out = {"metric": METRIC, "value": best, "unit": UNIT, "n_gpus": 1, "steps": sm["frames"],
-           "warmup": skip, "ms_per_step": 1e3 / best, "higher_is_better": True, "scaling": "weak",
-           "vs_baseline": None, "dtype": "f32 (MLP bf16 / fp32 accumulate)", "data": "synthetic",
-           "config": {"workload": desc, "instances": cloth.info.num_instances, "vertices": nv,
-                      "iterations": iters, "threads_per_vertex": cloth.info.threads_per_vertex},
-           "clocks": clk,
-           "target": "each instance's relative residual after the plain solver's iteration budget "
-                     "(a 1e-4 residual is not reached by plain VBD on these cloths within thousands of iterations)",
-           "learned_vs_plain": sm, "train": {"samples": trajectories * frames * nv, "record_s": t_record,
-                                             "train_s": t_train, "final_loss_normalised": loss}}
+    ms = np.array([a.elapsed_time(b) for a, b in ev])
+    ms_step = maxrank(np.mean(ms))
+    value = (1 if sharded else world) * 1e3 / ms_step
+    peak, peak_src = hbm_peak()
+    bytes_launch = alg_bytes_per_iter(info.num_verts, info.num_edges, info.num_bending_edges) / info.num_vertex_colors
+    per_launch = ms_step / (prm["iterations"] * info.num_vertex_colors)
+    achieved = bytes_launch / (per_launch * 1e-3) / 1e9
+    x_h = torch.empty((info.num_verts, 3), dtype=torch.float32, pin_memory=True).numpy()
+    v_h = torch.empty((info.num_verts, 3), dtype=torch.float32, pin_memory=True).numpy()
+    cloth.state_into(x_h, v_h, stream=stream)
+    n_e2e = 20
+    for f in range(n_e2e + 1):
+        if f == 1:
+            if world > 1:
+                torch.distributed.barrier()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+        cloth.set_state(x_h, v_h, stream=stream)
+        cloth.frame(stream=stream, graph=True)
+        cloth.state_into(x_h, v_h, stream=stream)
+    e2e_s = maxrank((time.perf_counter() - t0) / n_e2e)
+    state_bytes = 2 * 3 * 4 * info.num_verts
+    out = None
     if rank == 0:
+        out = {"metric": METRICS[args.workload], "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+               "scaling": "strong" if sharded else "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+               "config": {"workload": WORKLOADS[args.workload], "instances": info.num_instances,
+                          "vertices": info.num_verts, "iterations": prm["iterations"],
+                          "threads_per_vertex": info.threads_per_vertex, "block_size": info.block_size,
+                          "parallelism": f"instance-shards{world}" if sharded else f"replicas{world}",
+                          "l2": "flushed between frames (256 MiB write, outside the event pairs)"},
+               "e2e": {"value": (1 if sharded else world) / e2e_s, "unit": UNIT, "h2d_bytes_per_step": state_bytes,
+                       "d2h_bytes_per_step": state_bytes},
+               "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                            "frac": achieved / peak, "traffic": None,
+                            "kernel": f"vbd_sweep_kernel<{info.threads_per_vertex}>",
+                            "us_per_launch_upper_bound": per_launch * 1e3, "alg_bytes_per_launch": bytes_launch,
+                            "timing": "whole graph frame over its sweep launches (predict and update included)",
+                            "peak_source": peak_src},
+               "gpu_launches": int(l1 - l0), "clocks": clk}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        t_cpu, nv_s, nv_t = cpu_plain_fixed_frames(threads, 3, args.workload)
+        per_frame = float(np.median(t_cpu)) * nv_t / nv_s
+        out["cpu_baseline"] = {"value": 1.0 / per_frame, "unit": UNIT, "cores": threads, "kind": "port",
+                               "sample": "3 full frames (50 iterations), median"
+                                         + (f", instance 0 scaled by vertex count" if nv_t != nv_s else ""),
+                               "cpu_model": cpu_model(), "nproc": os.cpu_count()}
+    if out is not None:
         print(json.dumps(out), flush=True)
+    cloth.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
 
 
 def main():
@@ -457,7 +653,7 @@ def main():
     elif args.workload in ("c3", "c4"):
         run_learned(args)
     else:
-        run_ours(args)
+        run_plain(args)
 
 
 if __name__ == "__main__":

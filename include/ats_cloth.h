@@ -259,8 +259,9 @@ int ats_potential(ats_cloth* cloth, double* out_per_instance, ats_stream stream)
  * (device, 3 doubles) receives inertia, stretch and bending, the terms ats_energy
  * computes. Scratch is a static 96 KiB device array that every GPU which loads the
  * library keeps until exit: at most 8,388,608 vertices, edges and bending edges per
- * call (larger calls fail with ATS_ERR_INVALID). The first call on a device looks
- * up that array's device address; make that first call before any stream capture.
+ * call (larger calls fail with ATS_ERR_INVALID). Every call looks up that array's
+ * device address on the current device (a runtime query, no allocation); the first
+ * call on a device may load the module, so make it before any stream capture.
  * Calls share the array: calls that overlap on the GPU race and may return wrong
  * sums. Enqueues on `stream` and returns without synchronising. */
 int ats_energy_noalloc(const float* x, const float* x_start, const float* v, const float* mass,
@@ -269,8 +270,10 @@ int ats_energy_noalloc(const float* x, const float* x_start, const float* v, con
                        float k_bend, const float* accel, float h, double* out3, ats_stream stream);
 
 /* ---------------------------------------------------------------- learned warm start
- * No counterpart in the reference: a per-vertex MLP (24 -> 64 -> 64 -> 64 -> 3, exact
- * GELU, BF16 weights and activations, FP32 accumulation on the tensor cores) predicts
+ * No counterpart in the reference: a per-vertex MLP (24 -> 64 -> 64 -> 64 -> 3, GELU
+ * by a degree-8 polynomial within 1.2e-4 of z Phi(z) (csrc/ats_gelu.cuh, generated by
+ * csrc/fit_gelu.py), BF16 weights and activations, FP32 accumulation on the tensor
+ * cores) predicts
  * the frame's solved position; the plain VBD iterations always run afterwards.
  * Features of vertex v (h the substep, s = 9.8 h^2, y the inertial prediction):
  * h v / s, (y - x0) / s, and (x0_u - x0_v) / rest length of the edge neighbours in six
@@ -338,6 +341,12 @@ int ats_frame_warm(ats_cloth* cloth, const ats_mlp* mlp, int fallback, int itera
 int ats_frame_warm_to_residual(ats_cloth* cloth, const ats_mlp* mlp, int fallback, double tol, const double* tols,
                                const int* first_check, int check_every, int max_iterations, int* iterations,
                                double* residual, int* used, ats_stream stream);
+
+/* Kernels the library has launched in this process: every direct launch, plus the
+ * kernel nodes of every CUDA-graph replay (a kernel enqueued during stream capture is
+ * counted when its graph is replayed). A diagnostic with no counterpart in the
+ * reference; benchmarks read it before and after a timed region. */
+int ats_kernel_launches(long long* count);
 
 /* Message of the last failed call on this thread ("" if none). */
 const char* ats_last_error(void);

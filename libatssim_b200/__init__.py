@@ -139,6 +139,7 @@ _SIGNATURES = {
     "ats_frame_warm_to_residual": [_vp, _vp, ctypes.c_int, ctypes.c_double, _dp, _ip, ctypes.c_int, ctypes.c_int, _ip,
                                    _dp, _ip, _vp],
     "ats_frame_to_residuals": [_vp, _dp, _ip, ctypes.c_int, ctypes.c_int, _ip, _dp, _vp],
+    "ats_kernel_launches": [ctypes.POINTER(ctypes.c_longlong)],
     "ats_energy_noalloc": [_vp, _vp, _vp, _vp, _vp, ctypes.c_int, _vp, _vp, ctypes.c_int, _vp, _vp, ctypes.c_int,
                            ctypes.c_float, ctypes.c_float, _fp, ctypes.c_float, _vp, _vp],
 }
@@ -190,6 +191,14 @@ def energy_noalloc(x, x_start, v, mass, fixed, num_verts, edges, rest_length, nu
     _check(lib().ats_energy_noalloc(x, x_start, v, mass, fixed, int(num_verts), edges, rest_length, int(num_edges),
                                     bending, q, int(num_bending_edges), float(k_stretch), float(k_bend),
                                     _p(acc, ctypes.c_float), float(h), out3, _stream(stream)))
+
+
+def kernel_launches():
+    """Kernels launched by the library so far in this process (direct launches plus
+    the kernel nodes of CUDA-graph replays)."""
+    n = ctypes.c_longlong(0)
+    _check(lib().ats_kernel_launches(ctypes.byref(n)))
+    return int(n.value)
 
 
 # ---------------------------------------------------------------- mesh helpers

@@ -13,8 +13,10 @@
 #include <cstring>
 #include <atomic>
 #include <memory>
+#include <mutex>
 #include <thread>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "ats_internal.cuh"
@@ -24,6 +26,41 @@ namespace ats {
 
 static thread_local std::string g_last_error;
 void set_error(const std::string& msg) { g_last_error = msg; }
+
+static std::atomic<long long> g_kernel_launches{0};
+static std::mutex g_graph_mu;
+static std::unordered_map<cudaGraphExec_t, int> g_graph_kernels;
+
+void count_launch(cudaStream_t st) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) return;
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+}
+
+void register_graph(cudaGraphExec_t exec, cudaGraph_t g) {
+    size_t n = 0;
+    int kernels = 0;
+    if (cudaGraphGetNodes(g, nullptr, &n) == cudaSuccess && n > 0) {
+        std::vector<cudaGraphNode_t> nodes(n);
+        if (cudaGraphGetNodes(g, nodes.data(), &n) == cudaSuccess)
+            for (size_t i = 0; i < n; ++i) {
+                cudaGraphNodeType t;
+                if (cudaGraphNodeGetType(nodes[i], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++kernels;
+            }
+    }
+    std::lock_guard<std::mutex> lock(g_graph_mu);
+    g_graph_kernels[exec] = kernels;
+}
+
+void count_graph_launch(cudaGraphExec_t exec) {
+    int k = 0;
+    {
+        std::lock_guard<std::mutex> lock(g_graph_mu);
+        auto it = g_graph_kernels.find(exec);
+        if (it != g_graph_kernels.end()) k = it->second;
+    }
+    g_kernel_launches.fetch_add(k, std::memory_order_relaxed);
+}
 
 namespace {
 
@@ -525,10 +562,10 @@ cudaError_t stencil_eval_launch(int tpv, const EvalArgs& a, cudaStream_t st) {
     const int blocks = (a.nslices * 32 + 127) / 128;
     if (blocks == 0) return cudaSuccess;
     switch (tpv) {
-        case 1: stencil_eval_kernel<1, 6, 6, MODE><<<blocks, 128, 0, st>>>(a); break;
-        case 2: stencil_eval_kernel<2, 3, 3, MODE><<<blocks, 128, 0, st>>>(a); break;
-        case 4: stencil_eval_kernel<4, 2, 2, MODE><<<blocks, 128, 0, st>>>(a); break;
-        default: stencil_eval_kernel<8, 1, 1, MODE><<<blocks, 128, 0, st>>>(a); break;
+        case 1: stencil_eval_kernel<1, 6, 6, MODE><<<blocks, 128, 0, st>>>(a); count_launch(st); break;
+        case 2: stencil_eval_kernel<2, 3, 3, MODE><<<blocks, 128, 0, st>>>(a); count_launch(st); break;
+        case 4: stencil_eval_kernel<4, 2, 2, MODE><<<blocks, 128, 0, st>>>(a); count_launch(st); break;
+        default: stencil_eval_kernel<8, 1, 1, MODE><<<blocks, 128, 0, st>>>(a); count_launch(st); break;
     }
     return cudaGetLastError();
 }
@@ -679,7 +716,7 @@ int enqueue_compaction(ats_cloth* c, cudaStream_t st) {
     if (n == 0 || nc == 0) return ATS_OK;
     ATS_CUDA(cudaMemsetAsync(c->act_count.p, 0, nc * sizeof(int), st));
     compact_slices_kernel<<<(n + 255) / 256, 256, 0, st>>>(c->slice_inst.p, c->active.p, c->color_slices.p, nc, n,
-                                                           c->act_list.p, c->act_count.p);
+                                                           c->act_list.p, c->act_count.p); count_launch(st);
     ATS_CUDA(cudaGetLastError());
     return ATS_OK;
 }
@@ -718,8 +755,10 @@ cudaError_t sweep_launch(dim3 grid, dim3 block, cudaStream_t st, const SweepArgs
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (listed) return cudaLaunchKernelEx(&cfg, vbd_sweep_list_kernel<TPV, RE, RB>, a);
-    return cudaLaunchKernelEx(&cfg, vbd_sweep_kernel<TPV, RE, RB>, a);
+    const cudaError_t e = listed ? cudaLaunchKernelEx(&cfg, vbd_sweep_list_kernel<TPV, RE, RB>, a)
+                                 : cudaLaunchKernelEx(&cfg, vbd_sweep_kernel<TPV, RE, RB>, a);
+    if (e == cudaSuccess) count_launch(st);
+    return e;
 }
 
 int launch_sweep(ats_cloth* c, int color, cudaStream_t st, const int* active) {
@@ -765,14 +804,14 @@ int launch_sweep(ats_cloth* c, int color, cudaStream_t st, const int* active) {
 
 int launch_predict(ats_cloth* c, cudaStream_t st) {
     const int n = c->L.nv;
-    predict_kernel<<<(n + 255) / 256, 256, 0, st>>>(c->x.p, c->x0.p, c->vel.p, c->vm.p, c->inst.p, n, c->h);
+    predict_kernel<<<(n + 255) / 256, 256, 0, st>>>(c->x.p, c->x0.p, c->vel.p, c->vm.p, c->inst.p, n, c->h); count_launch(st);
     ATS_CUDA(cudaGetLastError());
     return ATS_OK;
 }
 
 int launch_update(ats_cloth* c, cudaStream_t st) {
     const int n = c->L.nv;
-    update_kernel<<<(n + 255) / 256, 256, 0, st>>>(c->x.p, c->x0.p, c->vel.p, n, c->h, c->damp);
+    update_kernel<<<(n + 255) / 256, 256, 0, st>>>(c->x.p, c->x0.p, c->vel.p, n, c->h, c->damp); count_launch(st);
     ATS_CUDA(cudaGetLastError());
     return ATS_OK;
 }
@@ -797,7 +836,9 @@ cudaError_t launch_pdl(void (*kernel)(KArgs...), int blocks, int threads, cudaSt
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, kernel, args...);
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, kernel, args...);
+    if (e == cudaSuccess) count_launch(st);
+    return e;
 }
 
 int launch_xpbd_stretch(ats_cloth* c, int color, cudaStream_t st) {
@@ -866,9 +907,9 @@ EvalArgs eval_args(ats_cloth* c) {
 int segment_sum(ats_cloth* c, const double* per_vertex, double* out, int take_sqrt, cudaStream_t st,
                 const int* mask = nullptr) {
     segment_partial_kernel<<<dim3(kSegChunks, c->L.ninst), kRedThreads, 0, st>>>(per_vertex, c->inst_seg.p,
-                                                                                   c->seg_partial.p, mask);
+                                                                                   c->seg_partial.p, mask); count_launch(st);
     ATS_CUDA(cudaGetLastError());
-    segment_final_kernel<<<c->L.ninst, kSegChunks, 0, st>>>(c->seg_partial.p, out, take_sqrt, mask);
+    segment_final_kernel<<<c->L.ninst, kSegChunks, 0, st>>>(c->seg_partial.p, out, take_sqrt, mask); count_launch(st);
     ATS_CUDA(cudaGetLastError());
     return ATS_OK;
 }
@@ -966,10 +1007,10 @@ int enqueue_residual_norms(ats_cloth* c, cudaStream_t st, const int* active, boo
         const int blocks = (a.nslices * 32 + 127) / 128;
         if (blocks > 0) {
             switch (c->L.tpv) {
-                case 1: stencil_grad32_kernel<1, 6, 6><<<blocks, 128, 0, st>>>(a, c->h, c->h2inv); break;
-                case 2: stencil_grad32_kernel<2, 3, 3><<<blocks, 128, 0, st>>>(a, c->h, c->h2inv); break;
-                case 4: stencil_grad32_kernel<4, 2, 2><<<blocks, 128, 0, st>>>(a, c->h, c->h2inv); break;
-                default: stencil_grad32_kernel<8, 1, 1><<<blocks, 128, 0, st>>>(a, c->h, c->h2inv); break;
+                case 1: stencil_grad32_kernel<1, 6, 6><<<blocks, 128, 0, st>>>(a, c->h, c->h2inv); count_launch(st); break;
+                case 2: stencil_grad32_kernel<2, 3, 3><<<blocks, 128, 0, st>>>(a, c->h, c->h2inv); count_launch(st); break;
+                case 4: stencil_grad32_kernel<4, 2, 2><<<blocks, 128, 0, st>>>(a, c->h, c->h2inv); count_launch(st); break;
+                default: stencil_grad32_kernel<8, 1, 1><<<blocks, 128, 0, st>>>(a, c->h, c->h2inv); count_launch(st); break;
             }
             ATS_CUDA(cudaGetLastError());
         }
@@ -1027,7 +1068,7 @@ int piece_graph(ats_cloth* c, int k, int step, int max_iterations, cudaGraphExec
             residual_check_kernel<<<1, 256, 0, cs>>>(c->red_out.p, c->norm0.p, c->active.p, c->iters.p,
                                                       c->n_active.p, c->due.p, c->L.ninst, 0, c->probe_points.p,
                                                       c->probe_idx.p, step, c->first_check.p, max_iterations,
-                                                      c->tols.p);
+                                                      c->tols.p); count_launch(cs);
             if (cudaGetLastError() != cudaSuccess) r = ATS_ERR_CUDA;
             if (!r) r = enqueue_compaction(c, cs);
         }
@@ -1040,6 +1081,7 @@ int piece_graph(ats_cloth* c, int k, int step, int max_iterations, cudaGraphExec
     }
     cudaGraphExec_t exec = nullptr;
     e = cudaGraphInstantiate(&exec, g, 0);
+    if (e == cudaSuccess) register_graph(exec, g);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) {
         set_error(std::string("residual frame instantiate failed: ") + cudaGetErrorString(e));
@@ -1058,9 +1100,11 @@ int launch_chunk(ats_cloth* c, int k, int step, int max_iterations, cudaStream_t
         if (k & bit) {
             if ((r = piece_graph(c, bit, 0, 0, &exec))) return r;
             ATS_CUDA(cudaGraphLaunch(exec, st));
+            count_graph_launch(exec);
         }
     if ((r = piece_graph(c, 0, step, max_iterations, &exec))) return r;
     ATS_CUDA(cudaGraphLaunch(exec, st));
+    count_graph_launch(exec);
     return ATS_OK;
 }
 
@@ -1116,7 +1160,7 @@ int frame_to_residual_impl(ats_cloth* c, double tol, const double* tols, const i
         if (after_predict && (r = after_predict(st))) return r;
         residual_check_kernel<<<1, 256, 0, st>>>(c->red_out.p, c->norm0.p, c->active.p, c->iters.p, c->n_active.p,
                                                   c->due.p, ni, 1, c->probe_points.p, c->probe_idx.p, check_every,
-                                                  c->first_check.p, max_iterations, c->tols.p);
+                                                  c->first_check.p, max_iterations, c->tols.p); count_launch(st);
         ATS_CUDA(cudaGetLastError());
         if ((r = enqueue_compaction(c, st))) return r;
         list_sweep_ctas(c->L.tpv, c->block);  // occupancy query before any capture
@@ -1159,6 +1203,15 @@ int frame_to_residual_impl(ats_cloth* c, double tol, const double* tols, const i
 extern "C" {
 
 const char* ats_last_error(void) { return g_last_error.c_str(); }
+
+int ats_kernel_launches(long long* count) {
+    if (!count) {
+        set_error("ats_kernel_launches: null output");
+        return ATS_ERR_INVALID;
+    }
+    *count = g_kernel_launches.load(std::memory_order_relaxed);
+    return ATS_OK;
+}
 
 int ats_cloth_create(const ats_instance_desc* inst, int ninst, const ats_solver_params* prm, ats_cloth** out) {
     if (!inst || ninst <= 0 || !prm || !out) {
@@ -1307,7 +1360,7 @@ int ats_set_state(ats_cloth* c, const float* x, const float* v, ats_stream strea
     ATS_CUDA(cudaMemcpyAsync(c->io_x.p, x, 12 * (size_t)n, cudaMemcpyHostToDevice, st));
     if (v) ATS_CUDA(cudaMemcpyAsync(c->io_v.p, v, 12 * (size_t)n, cudaMemcpyHostToDevice, st));
     scatter_state_kernel<<<(n + 255) / 256, 256, 0, st>>>(c->io_x.p, c->io_v.p, c->to_caller.p, c->x.p, c->x0.p,
-                                                          c->vel.p, n, v ? 1 : 0);
+                                                          c->vel.p, n, v ? 1 : 0); count_launch(st);
     ATS_CUDA(cudaGetLastError());
     ATS_CUDA(cudaStreamSynchronize(st));
     return ATS_OK;
@@ -1321,7 +1374,7 @@ int ats_set_positions(ats_cloth* c, const float* x, ats_stream stream) {
     cudaStream_t st = S(stream);
     const int n = c->L.nv;
     ATS_CUDA(cudaMemcpyAsync(c->io_x.p, x, 12 * (size_t)n, cudaMemcpyHostToDevice, st));
-    scatter_positions_kernel<<<(n + 255) / 256, 256, 0, st>>>(c->io_x.p, c->to_caller.p, c->x.p, n);
+    scatter_positions_kernel<<<(n + 255) / 256, 256, 0, st>>>(c->io_x.p, c->to_caller.p, c->x.p, n); count_launch(st);
     ATS_CUDA(cudaGetLastError());
     ATS_CUDA(cudaStreamSynchronize(st));
     return ATS_OK;
@@ -1329,7 +1382,7 @@ int ats_set_positions(ats_cloth* c, const float* x, ats_stream stream) {
 
 static int read_back(ats_cloth* c, const float4* src, float* dst, float* staging, cudaStream_t st) {
     const int n = c->L.nv;
-    gather_state_kernel<<<(n + 255) / 256, 256, 0, st>>>(src, c->to_caller.p, staging, n);
+    gather_state_kernel<<<(n + 255) / 256, 256, 0, st>>>(src, c->to_caller.p, staging, n); count_launch(st);
     ATS_CUDA(cudaGetLastError());
     ATS_CUDA(cudaMemcpyAsync(dst, staging, 12 * (size_t)n, cudaMemcpyDeviceToHost, st));
     return ATS_OK;
@@ -1357,7 +1410,7 @@ int ats_async_merge(ats_cloth* c, const float* other, float weight, ats_stream s
     const int n = c->L.nv;
     cudaStream_t st = S(stream);
     ATS_CUDA(cudaMemcpyAsync(c->io_x.p, other, 12 * (size_t)n, cudaMemcpyHostToDevice, st));
-    async_merge_kernel<<<(n + 255) / 256, 256, 0, st>>>(c->x.p, c->async_begin.p, c->io_x.p, c->to_caller.p, n, weight);
+    async_merge_kernel<<<(n + 255) / 256, 256, 0, st>>>(c->x.p, c->async_begin.p, c->io_x.p, c->to_caller.p, n, weight); count_launch(st);
     ATS_CUDA(cudaGetLastError());
     ATS_CUDA(cudaStreamSynchronize(st));
     return ATS_OK;
@@ -1475,6 +1528,7 @@ int ats_frame_graph(ats_cloth* c, int solver, ats_stream stream) {
             return ATS_ERR_CUDA;
         }
         e = cudaGraphInstantiate(&c->graph[solver], g, 0);
+        if (e == cudaSuccess) register_graph(c->graph[solver], g);
         cudaGraphDestroy(g);
         if (e != cudaSuccess) {
             set_error(std::string("ats_frame_graph: instantiate failed: ") + cudaGetErrorString(e));
@@ -1482,6 +1536,7 @@ int ats_frame_graph(ats_cloth* c, int solver, ats_stream stream) {
         }
     }
     ATS_CUDA(cudaGraphLaunch(c->graph[solver], S(stream)));
+    count_graph_launch(c->graph[solver]);
     return ATS_OK;
 }
 
@@ -1596,9 +1651,9 @@ int ats_energy(ats_cloth* c, double* out3, ats_stream stream) {
     a.nb = c->L.nb;
     a.h = (double)c->h;
     a.partial = c->partial.p;
-    energy_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(a);
+    energy_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(a); count_launch(st);
     ATS_CUDA(cudaGetLastError());
-    sum_partials3_kernel<<<1, kRedThreads, 0, st>>>(c->partial.p, kRedBlocks, c->red_out.p);
+    sum_partials3_kernel<<<1, kRedThreads, 0, st>>>(c->partial.p, kRedBlocks, c->red_out.p); count_launch(st);
     ATS_CUDA(cudaGetLastError());
     ATS_CUDA(cudaMemcpyAsync(out3, c->red_out.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
     ATS_CUDA(cudaStreamSynchronize(st));

@@ -42,6 +42,14 @@ struct DevBuf {
 
 inline cudaStream_t S(ats_stream s) { return (cudaStream_t)s; }
 
+// Kernel-launch accounting behind ats_kernel_launches: count_launch after every direct
+// launch (skipped while `st` is being captured, since the kernel then becomes a graph
+// node), register_graph when a graph is instantiated (its kernel nodes are counted
+// once), count_graph_launch at every replay.
+void count_launch(cudaStream_t st);
+void register_graph(cudaGraphExec_t exec, cudaGraph_t g);
+void count_graph_launch(cudaGraphExec_t exec);
+
 }  // namespace ats
 
 struct ats_cloth {

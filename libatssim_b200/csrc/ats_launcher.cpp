@@ -451,11 +451,18 @@ void Scheduler::launch(LaunchMode mode, const std::function<LaunchParam(const Ta
         std::fprintf(stderr, "launch: this mode needs scheduler_dag() first\n");
         return;
     }
-    // scheduled modes: tasks in order of scheduled start
+    // scheduled modes: tasks in order of scheduled start; ties (a zero-length task and
+    // its successor start together) go by end time, then by topological position, so a
+    // task never runs before a predecessor that the schedule placed at the same instant
+    std::vector<uint> topo_pos(list_task.size(), 0);
+    for (size_t i = 0; i < order.size(); ++i)
+        if (order[i] < topo_pos.size()) topo_pos[order[i]] = (uint)i;
     std::vector<ScheduleEvent> plan;
     for (const auto& jobs : proc_schedules) plan.insert(plan.end(), jobs.begin(), jobs.end());
-    std::stable_sort(plan.begin(), plan.end(), [](const ScheduleEvent& a, const ScheduleEvent& b) {
-        return a.start != b.start ? a.start < b.start : a.proc < b.proc;
+    std::stable_sort(plan.begin(), plan.end(), [&](const ScheduleEvent& a, const ScheduleEvent& b) {
+        if (a.start != b.start) return a.start < b.start;
+        if (a.end != b.end) return a.end < b.end;
+        return topo_pos[a.task_id] < topo_pos[b.task_id];
     });
     if (mode == LaunchModePartialCPU || mode == LaunchModePartialGPU) {
         const uint want = mode == LaunchModePartialCPU ? 0u : 1u;

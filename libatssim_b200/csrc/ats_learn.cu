@@ -703,20 +703,20 @@ int enqueue_warm_start(ats_cloth* c, const ats_mlp* m, int fallback, cudaStream_
     int r;
     if ((r = set_smem_limits()) || (r = ensure_learn_buffers(c))) return r;
     const int nv = c->L.nv;
-    copy4_kernel<<<(nv + 255) / 256, 256, 0, st>>>(c->x.p, c->y_buf.p, nv);
+    copy4_kernel<<<(nv + 255) / 256, 256, 0, st>>>(c->x.p, c->y_buf.p, nv); count_launch(st);
     ATS_CUDA(cudaGetLastError());
     {
         const int tiles = (nv + kWarpRows - 1) / kWarpRows;
         const int grid = std::max(1, std::min((tiles + 3) / 4, g_infer_ctas));
         infer_warp_kernel<<<grid, kThreads, 0, st>>>(feat_args(c), m->wpack.p, m->master.p, m->nrm.p, c->x.p,
-                                                     9.8f * c->h * c->h);
+                                                     9.8f * c->h * c->h); count_launch(st);
     }
     ATS_CUDA(cudaGetLastError());
     if (fallback) {
         if ((r = enqueue_potential_pair(c, c->y_buf.p, c->pot_guess.p, c->pot_y.p, st))) return r;
         const int n = std::max(nv, c->L.ninst);
         fallback_kernel<<<(n + 255) / 256, 256, 0, st>>>(c->x.p, c->y_buf.p, c->vm.p, c->pot_y.p, c->pot_guess.p,
-                                                          c->guess_used.p, nv, c->L.ninst);
+                                                          c->guess_used.p, nv, c->L.ninst); count_launch(st);
         ATS_CUDA(cudaGetLastError());
     }
     return ATS_OK;
@@ -842,9 +842,9 @@ int ats_mlp_fit_normalization(ats_mlp* m, const ats_dataset* d, ats_stream strea
     ATS_CUDA(pf.alloc((size_t)blocks * 2 * kIn));
     ATS_CUDA(pt.alloc((size_t)blocks * 2 * kOut));
     cudaStream_t st = S(stream);
-    column_moments_kernel<<<blocks, 32, 0, st>>>(d->feat.p, d->size, kIn, pf.p);
+    column_moments_kernel<<<blocks, 32, 0, st>>>(d->feat.p, d->size, kIn, pf.p); count_launch(st);
     ATS_CUDA(cudaGetLastError());
-    column_moments_kernel<<<blocks, 32, 0, st>>>(d->targ.p, d->size, kOut, pt.p);
+    column_moments_kernel<<<blocks, 32, 0, st>>>(d->targ.p, d->size, kOut, pt.p); count_launch(st);
     ATS_CUDA(cudaGetLastError());
     std::vector<double> hf((size_t)blocks * 2 * kIn), ht((size_t)blocks * 2 * kOut);
     ATS_CUDA(cudaMemcpyAsync(hf.data(), pf.p, hf.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -941,9 +941,9 @@ int ats_record_frame_begin(ats_cloth* c, ats_stream stream) {
         if (!fl.empty()) ATS_CUDA(cudaMemcpy(c->free_list.p, fl.data(), fl.size() * sizeof(int), cudaMemcpyHostToDevice));
     }
     cudaStream_t st = S(stream);
-    copy4_kernel<<<(nv + 255) / 256, 256, 0, st>>>(c->x.p, c->y_buf.p, nv);
+    copy4_kernel<<<(nv + 255) / 256, 256, 0, st>>>(c->x.p, c->y_buf.p, nv); count_launch(st);
     ATS_CUDA(cudaGetLastError());
-    features_kernel<<<(nv + 255) / 256, 256, 0, st>>>(feat_args(c), c->feat_stage.p);
+    features_kernel<<<(nv + 255) / 256, 256, 0, st>>>(feat_args(c), c->feat_stage.p); count_launch(st);
     ATS_CUDA(cudaGetLastError());
     return ATS_OK;
 }
@@ -960,7 +960,7 @@ int ats_record_frame_end(ats_cloth* c, ats_dataset* d, ats_stream stream) {
     }
     if (nfree > 0) {
         append_kernel<<<(nfree + 255) / 256, 256, 0, S(stream)>>>(c->feat_stage.p, c->x.p, c->y_buf.p, c->free_list.p, nfree,
-                                                                  1.f / (9.8f * c->h * c->h), d->feat.p, d->targ.p, d->size);
+                                                                  1.f / (9.8f * c->h * c->h), d->feat.p, d->targ.p, d->size); count_launch(S(stream));
         ATS_CUDA(cudaGetLastError());
     }
     d->size += nfree;
@@ -984,14 +984,14 @@ int ats_mlp_train(ats_mlp* m, const ats_dataset* d, int steps, int batch, float 
         train_tile_kernel<<<ctas, kThreads, kTileSmem, st>>>(d->feat.p, d->targ.p, d->size, batch, 1,
                                                               seed * 0x9E3779B97F4A7C15ull + (uint64_t)m->step,
                                                               m->wpack.p, m->master.p, m->nrm.p, m->partial.p,
-                                                              m->loss_partial.p);
+                                                              m->loss_partial.p); count_launch(st);
         ATS_CUDA(cudaGetLastError());
         reduce_adam_kernel<<<(kParams + 255) / 256, 256, 0, st>>>(m->partial.p, ctas, m->master.p, m->m1.p, m->m2.p,
-                                                                  nullptr, m->wpack.p, lr, 0.9f, 0.999f, 1e-8f, m->step, 1);
+                                                                  nullptr, m->wpack.p, lr, 0.9f, 0.999f, 1e-8f, m->step, 1); count_launch(st);
         ATS_CUDA(cudaGetLastError());
         if (mean_loss && s >= steps - std::min(steps, 20)) {
             float l = 0.f;
-            sum_loss_kernel<<<1, 32, 0, st>>>(m->loss_partial.p, ctas, m->loss.p);
+            sum_loss_kernel<<<1, 32, 0, st>>>(m->loss_partial.p, ctas, m->loss.p); count_launch(st);
             ATS_CUDA(cudaMemcpyAsync(&l, m->loss.p, sizeof(float), cudaMemcpyDeviceToHost, st));
             ATS_CUDA(cudaStreamSynchronize(st));
             loss_acc += l / (double)(batch * kOut);
@@ -1016,12 +1016,12 @@ int ats_mlp_batch_gradient(ats_mlp* m, const ats_dataset* d, int batch, unsigned
     train_tile_kernel<<<ctas, kThreads, kTileSmem, st>>>(d->feat.p, d->targ.p, d->size, batch, 1,
                                                           seed * 0x9E3779B97F4A7C15ull + 0x5851F42D4C957F2Dull,
                                                           m->wpack.p, m->master.p, m->nrm.p, m->partial.p,
-                                                          m->loss_partial.p);
+                                                          m->loss_partial.p); count_launch(st);
     ATS_CUDA(cudaGetLastError());
     reduce_adam_kernel<<<(kParams + 255) / 256, 256, 0, st>>>(m->partial.p, ctas, m->master.p, m->m1.p, m->m2.p,
-                                                              m->grad.p, m->wpack.p, 0.f, 0.9f, 0.999f, 1e-8f, 1, 0);
+                                                              m->grad.p, m->wpack.p, 0.f, 0.9f, 0.999f, 1e-8f, 1, 0); count_launch(st);
     ATS_CUDA(cudaGetLastError());
-    sum_loss_kernel<<<1, 32, 0, st>>>(m->loss_partial.p, ctas, m->loss.p);
+    sum_loss_kernel<<<1, 32, 0, st>>>(m->loss_partial.p, ctas, m->loss.p); count_launch(st);
     ATS_CUDA(cudaMemcpyAsync(grad, m->grad.p, kParams * sizeof(float), cudaMemcpyDeviceToHost, st));
     float l = 0.f;
     ATS_CUDA(cudaMemcpyAsync(&l, m->loss.p, sizeof(float), cudaMemcpyDeviceToHost, st));
@@ -1041,7 +1041,7 @@ int ats_mlp_apply_gradient(ats_mlp* m, const float* grad, float lr, ats_stream s
     ATS_CUDA(cudaMemcpyAsync(m->partial.p, grad, kParams * sizeof(float), cudaMemcpyHostToDevice, st));
     ++m->step;
     reduce_adam_kernel<<<(kParams + 255) / 256, 256, 0, st>>>(m->partial.p, 1, m->master.p, m->m1.p, m->m2.p, nullptr,
-                                                              m->wpack.p, lr, 0.9f, 0.999f, 1e-8f, m->step, 1);
+                                                              m->wpack.p, lr, 0.9f, 0.999f, 1e-8f, m->step, 1); count_launch(st);
     ATS_CUDA(cudaGetLastError());
     ATS_CUDA(cudaStreamSynchronize(st));
     return ATS_OK;
@@ -1063,12 +1063,12 @@ int ats_mlp_gradient(ats_mlp* m, const float* features, const float* targets, in
     ATS_CUDA(cudaMemcpyAsync(f.p, features, (size_t)n * kIn * sizeof(float), cudaMemcpyHostToDevice, st));
     ATS_CUDA(cudaMemcpyAsync(t.p, targets, (size_t)n * kOut * sizeof(float), cudaMemcpyHostToDevice, st));
     train_tile_kernel<<<ctas, kThreads, kTileSmem, st>>>(f.p, t.p, n, n, 0, 0, m->wpack.p, m->master.p, m->nrm.p,
-                                                          m->partial.p, m->loss_partial.p);
+                                                          m->partial.p, m->loss_partial.p); count_launch(st);
     ATS_CUDA(cudaGetLastError());
     reduce_adam_kernel<<<(kParams + 255) / 256, 256, 0, st>>>(m->partial.p, ctas, m->master.p, m->m1.p, m->m2.p,
-                                                              m->grad.p, m->wpack.p, 0.f, 0.9f, 0.999f, 1e-8f, 1, 0);
+                                                              m->grad.p, m->wpack.p, 0.f, 0.9f, 0.999f, 1e-8f, 1, 0); count_launch(st);
     ATS_CUDA(cudaGetLastError());
-    sum_loss_kernel<<<1, 32, 0, st>>>(m->loss_partial.p, ctas, m->loss.p);
+    sum_loss_kernel<<<1, 32, 0, st>>>(m->loss_partial.p, ctas, m->loss.p); count_launch(st);
     ATS_CUDA(cudaMemcpyAsync(grad, m->grad.p, kParams * sizeof(float), cudaMemcpyDeviceToHost, st));
     float l = 0.f;
     ATS_CUDA(cudaMemcpyAsync(&l, m->loss.p, sizeof(float), cudaMemcpyDeviceToHost, st));
@@ -1134,6 +1134,7 @@ int ats_frame_warm(ats_cloth* c, const ats_mlp* m, int fallback, int iterations,
             return ATS_ERR_CUDA;
         }
         e = cudaGraphInstantiate(&c->warm_graph, g, 0);
+        if (e == cudaSuccess) register_graph(c->warm_graph, g);
         cudaGraphDestroy(g);
         if (e != cudaSuccess) {
             set_error(std::string("ats_frame_warm: instantiate failed: ") + cudaGetErrorString(e));
@@ -1144,6 +1145,7 @@ int ats_frame_warm(ats_cloth* c, const ats_mlp* m, int fallback, int iterations,
         c->warm_key_fallback = fallback;
     }
     ATS_CUDA(cudaGraphLaunch(c->warm_graph, S(stream)));
+    count_graph_launch(c->warm_graph);
     return ATS_OK;
 }
 
@@ -1182,7 +1184,7 @@ int ats_mlp_infer(const ats_mlp* m, const float* features, int n, float* outputs
     cudaStream_t st = S(stream);
     ATS_CUDA(cudaMemcpyAsync(f.p, features, (size_t)n * kIn * sizeof(float), cudaMemcpyHostToDevice, st));
     infer_samples_kernel<<<(n + kTile - 1) / kTile, kThreads, kTileSmem, st>>>(f.p, n, m->wpack.p, m->master.p,
-                                                                                m->nrm.p, o.p);
+                                                                                m->nrm.p, o.p); count_launch(st);
     ATS_CUDA(cudaGetLastError());
     ATS_CUDA(cudaMemcpyAsync(outputs, o.p, (size_t)n * kOut * sizeof(float), cudaMemcpyDeviceToHost, st));
     ATS_CUDA(cudaStreamSynchronize(st));

@@ -21,7 +21,6 @@
 
 #include <cuda_runtime.h>
 
-#include <mutex>
 #include <string>
 
 #include "../../include/ats_cloth.h"
@@ -36,38 +35,22 @@ constexpr int kNoallocThreads = 256;
 constexpr int kNoallocChunk = 2048;         // elements of one term per block
 constexpr int kNoallocMaxPartials = 4096;   // blocks per term
 constexpr long long kNoallocMaxElements = (long long)kNoallocChunk * kNoallocMaxPartials;  // 8,388,608
-constexpr int kMaxDevices = 64;
 
 // Partial sums: [term][block], term 0 inertia, 1 stretch, 2 bending.
 static __device__ __align__(256) double g_noalloc_partials[3 * kNoallocMaxPartials];
 
-double* g_partials_addr[kMaxDevices] = {};
-std::mutex g_partials_mu;
-
-// Device address of g_noalloc_partials on the current device, looked up once per
-// device (the host-side symbol is only a stand-in, never a device address).
+// Device address of g_noalloc_partials on the current device. The host-side symbol
+// is only a stand-in, never a device address, so every call asks the runtime for the
+// address: once the module is loaded the lookup is cheap, and a cached pointer would
+// go stale after cudaDeviceReset or a rebuilt primary context reloads the module.
 int partials_address(double** out) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) {
-        ats::set_error(std::string("ats_energy_noalloc: cudaGetDevice: ") + cudaGetErrorString(e));
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
+    if (e != cudaSuccess || !p) {
+        ats::set_error(std::string("ats_energy_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
         return ATS_ERR_CUDA;
     }
-    if (dev < 0 || dev >= kMaxDevices) {
-        ats::set_error("ats_energy_noalloc: device ordinal beyond the supported 64");
-        return ATS_ERR_INVALID;
-    }
-    std::lock_guard<std::mutex> lock(g_partials_mu);
-    if (!g_partials_addr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_partials);
-        if (e != cudaSuccess || !p) {
-            ats::set_error(std::string("ats_energy_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-            return ATS_ERR_CUDA;
-        }
-        g_partials_addr[dev] = (double*)p;
-    }
-    *out = g_partials_addr[dev];
+    *out = (double*)p;
     return ATS_OK;
 }
 

@@ -6,17 +6,21 @@ Everything runs through the C ABI; this module only sequences the calls.
            predict -> ats_record_frame_begin -> `iters` VBD iterations ->
            ats_record_frame_end -> update, trajectories restarted from rest.
   train    normalisation from the data, then Adam on batches drawn from it.
-  evaluate on held-out wind seeds, from the same frame-start states:
-           plain    the CUDA-graph frame (predict, `iters` iterations, update) is timed;
-                    its per-instance residual r_plain = ||grad G(x)|| / ||grad G(y)||
-                    (the same sweeps replayed untimed) is the target;
-           learned  predict, learned guess (potential fallback per instance), then
-                    iterations until each instance reaches its r_plain, at most `iters`;
-                    converged instances are skipped. Probes every `check_every`, the
-                    first one (schedule) at the instance's previous-frame count minus
-                    `lead` ("prev") or at a percentile of all previous-frame counts
-                    (a number), or at check_every (None).
-           Frame times are CUDA-event times of each whole frame (host checks included).
+  fixed_tolerance_frames
+           the comparison at one fixed relative residual `tol` with an iteration
+           cap, on held-out wind seeds. Per frame, from the same start state:
+             learned  predict, the network's guess (per-instance potential fallback),
+                      then VBD iterations until each instance's residual
+                      ||grad G(x)|| / ||grad G(y)|| <= tol or `cap` iterations;
+             plain    predict, then VBD iterations to the same tol / cap.
+           Both probe every `check_every` iterations (and at the cap) and skip the
+           instances that have stopped. The plain frame's end state starts the next
+           frame, so the trajectory is the plain form's. Frame times are CUDA events
+           around each whole frame, host checks included.
+  residual_traces / tolerance_sweep
+           the relative residual of every instance at fixed iteration counts for
+           both forms from the same start (untimed, FP64), and from it the iterations
+           each form needs to reach each tolerance.
 """
 import time
 
@@ -53,104 +57,6 @@ def train(dataset, steps=150000, batch=32768, lr=2e-3, seed=0):
     m.train(dataset, steps=steps // 4, batch=batch, lr=lr / 3, seed=seed + 1)
     loss = m.train(dataset, steps=steps - steps // 2 - steps // 4, batch=batch, lr=lr / 10, seed=seed + 2)
     return m, loss, time.perf_counter() - t
-
-
-def evaluate(cloth, insts, model, iters, seed0, trajectories=2, frames=40, skip=15, check_every=5, schedule=None,
-             lead=2, stream=None):
-    """Per evaluated frame: plain and learned frame times, iterations, residuals,
-    and the FP64 incremental potential reached by both."""
-    import torch
-    masses = [float(i.mass.sum()) for i in insts]
-    x_rest = np.concatenate([i.positions for i in insts])
-    st = stream if stream is not None else torch.cuda.current_stream()
-    out = {"plain_ms": [], "learned_ms": [], "learned_iters": [], "used": [], "g_plain": [], "g_learned": [],
-           "r_plain": [], "r_learned": []}
-    prev = None  # iterations of the previous learned frame, per instance
-    for t in range(trajectories):
-        cloth.set_state(x_rest, np.zeros_like(x_rest))
-        for f in range(frames):
-            cloth.set_accel(wind_table(np.random.RandomState(seed0 + t * frames + f), masses))
-            if f >= skip:
-                x0, v0 = cloth.state()
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                # plain: the CUDA-graph frame (predict, iters x colours, update)
-                torch.cuda.synchronize()
-                e0.record(st)
-                cloth.frame(graph=True, stream=st)
-                e1.record(st)
-                torch.cuda.synchronize()
-                out["plain_ms"].append(e0.elapsed_time(e1))
-                # its per-instance residual (the same sweeps, replayed untimed)
-                cloth.set_state(x0, v0)
-                _, r_plain = cloth.frame_to_residual(0.0, check_every=iters, max_iterations=iters, stream=st)
-                out["r_plain"].append(r_plain)
-                out["g_plain"].append(final_potential(cloth, x0, v0))
-                # learned: guess, then iterations until every instance reaches r_plain
-                torch.cuda.synchronize()
-                e0.record(st)
-                first = None
-                if prev is not None and schedule == "prev":
-                    first = np.maximum(1, prev - lead)
-                elif prev is not None and schedule is not None:
-                    first = np.full(len(prev), max(1, int(np.percentile(prev, schedule))), dtype=np.int32)
-                torch.cuda.nvtx.range_push("learned_frame")  # lets a profiler select these kernels
-                its, r_l, used = cloth.frame_warm_to_residual(model, r_plain, check_every=check_every,
-                                                              max_iterations=iters, first_check=first, stream=st)
-                torch.cuda.nvtx.range_pop()
-                prev = its.copy()
-                e1.record(st)
-                torch.cuda.synchronize()
-                out["learned_ms"].append(e0.elapsed_time(e1))
-                out["learned_iters"].append(its)
-                out["used"].append(used)
-                out["r_learned"].append(r_l)
-                out["g_learned"].append(final_potential(cloth, x0, v0))
-            cloth.frame(graph=True)
-    return {k: np.array(v) for k, v in out.items()}
-
-
-def evaluate_fixed(cloth, insts, model, budget, iters, seed0, trajectories=2, frames=40, skip=15, stream=None):
-    """The learned frame with a fixed iteration budget, replayed as a CUDA graph:
-    per evaluated frame its time and, per instance, whether it reached the residual of
-    the plain frame (plain `iters` iterations from the same start)."""
-    import torch
-    masses = [float(i.mass.sum()) for i in insts]
-    x_rest = np.concatenate([i.positions for i in insts])
-    st = stream if stream is not None else torch.cuda.current_stream()
-    ms, reached, ratio = [], [], []
-    # capture the graph before timing (a replay after capture is what a frame costs)
-    cloth.set_state(x_rest, np.zeros_like(x_rest))
-    cloth.frame_warm(model, fallback=True, iterations=budget, graph=True, stream=st)
-    torch.cuda.synchronize()
-    for t in range(trajectories):
-        cloth.set_state(x_rest, np.zeros_like(x_rest))
-        for f in range(frames):
-            cloth.set_accel(wind_table(np.random.RandomState(seed0 + t * frames + f), masses))
-            if f >= skip:
-                x0, v0 = cloth.state()
-                _, r_plain = cloth.frame_to_residual(0.0, check_every=iters, max_iterations=iters, stream=st)
-                cloth.set_state(x0, v0)
-                cloth.predict(stream=st)
-                r0 = cloth.residual(stream=st)
-                cloth.warm_start(model, fallback=True, stream=st)
-                cloth.vbd_iterations(budget, stream=st)
-                r_l = cloth.residual(stream=st) / r0
-                reached.append(r_l <= r_plain * (1 + 1e-9))
-                ratio.append(r_l / r_plain)
-                cloth.set_state(x0, v0)
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                torch.cuda.synchronize()
-                e0.record(st)
-                cloth.frame_warm(model, fallback=True, iterations=budget, graph=True, stream=st)
-                e1.record(st)
-                torch.cuda.synchronize()
-                ms.append(e0.elapsed_time(e1))
-                cloth.set_state(x0, v0)
-            cloth.frame(graph=True)
-    return {"budget": int(budget), "learned_fixed_fps": float(1e3 / np.mean(ms)),
-            "learned_fixed_ms_p50": float(np.percentile(ms, 50)), "learned_fixed_ms_p99": float(np.percentile(ms, 99)),
-            "reached_plain_residual_fraction": float(np.mean(np.concatenate(reached))),
-            "residual_ratio_median": float(np.median(np.concatenate(ratio)))}
 
 
 def plain_per_instance_ms(insts, prm, frames=10, warmup=3, seed0=10000, stream=None):
@@ -194,28 +100,134 @@ def final_potential(cloth, x0, v0):
     return e
 
 
-def summary(res, iters, per_instance_ms=None):
-    plain = res["plain_ms"]
-    learned = res["learned_ms"]
-    it = res["learned_iters"].astype(np.float64)
-    extra = {}
-    if per_instance_ms is not None:
-        extra = {"plain_unbatched_fps": float(1e3 / per_instance_ms),
-                 "speedup_vs_unbatched": float(per_instance_ms / np.mean(learned))}
-    return {**extra,
-        "frames": int(len(plain)),
-        "plain_fps": float(1e3 / np.mean(plain)),
-        "learned_fps": float(1e3 / np.mean(learned)),
-        "speedup": float(np.mean(plain) / np.mean(learned)),
-        "plain_ms_p50": float(np.percentile(plain, 50)),
-        "plain_ms_p99": float(np.percentile(plain, 99)),
-        "learned_ms_p50": float(np.percentile(learned, 50)),
-        "learned_ms_p99": float(np.percentile(learned, 99)),
-        "iterations_plain": int(iters),
-        "iterations_learned_mean": float(it.mean()),
-        "iterations_learned_p50": float(np.median(it)),
-        "guess_kept_fraction": float(res["used"].mean()),
-        "residual_plain_median": float(np.median(res["r_plain"])),
-        "residual_learned_median": float(np.median(res["r_learned"])),
-        "potential_rel_diff_median": float(np.median((res["g_learned"] - res["g_plain"]) / np.abs(res["g_plain"]))),
-    }
+
+def approach(cloth, insts, frames, seed0, stream=None):
+    """From rest, `frames` plain CUDA-graph frames with a seeded wind per frame (the
+    cloth is moving when the measured frames begin)."""
+    masses = [float(i.mass.sum()) for i in insts]
+    x_rest = np.concatenate([i.positions for i in insts])
+    cloth.set_state(x_rest, np.zeros_like(x_rest))
+    for f in range(frames):
+        cloth.set_accel(wind_table(np.random.RandomState(seed0 + f), masses), stream=stream)
+        cloth.frame(graph=True, stream=stream)
+
+
+def fixed_tolerance_frames(cloth, insts, model, tol, cap, check_every, frames, warmup, seed0, stream=None,
+                           on_timed=None):
+    """The learned and the plain frame to the same relative residual `tol` (at most
+    `cap` iterations) from the same start, `warmup` untimed then `frames` timed frames
+    with winds seeded seed0, seed0 + 1, ... Returns per-frame times (ms), and per frame
+    and instance the iterations, relative residuals and whether the guess was kept.
+    on_timed(True/False) brackets the timed frames (e.g. a clock sampler)."""
+    import torch
+    st = stream if stream is not None else torch.cuda.current_stream()
+    masses = [float(i.mass.sum()) for i in insts]
+    out = {k: [] for k in ("learned_ms", "plain_ms", "learned_iters", "plain_iters", "learned_res", "plain_res",
+                           "used")}
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    for f in range(warmup + frames):
+        timed = f >= warmup
+        if timed and f == warmup and on_timed:
+            on_timed(True)
+        cloth.set_accel(wind_table(np.random.RandomState(seed0 + f), masses), stream=st)
+        x0, v0 = cloth.state(stream=st)
+        torch.cuda.synchronize()
+        ev[0].record(st)
+        it_l, r_l, used = cloth.frame_warm_to_residual(model, tol, check_every=check_every, max_iterations=cap,
+                                                       stream=st)
+        ev[1].record(st)
+        cloth.set_state(x0, v0, stream=st)
+        torch.cuda.synchronize()
+        ev[2].record(st)
+        it_p, r_p = cloth.frame_to_residual(tol, check_every=check_every, max_iterations=cap, stream=st)
+        ev[3].record(st)
+        torch.cuda.synchronize()
+        if timed:
+            out["learned_ms"].append(ev[0].elapsed_time(ev[1]))
+            out["plain_ms"].append(ev[2].elapsed_time(ev[3]))
+            out["learned_iters"].append(it_l)
+            out["plain_iters"].append(it_p)
+            out["learned_res"].append(r_l)
+            out["plain_res"].append(r_p)
+            out["used"].append(used)
+    if on_timed:
+        on_timed(False)
+    return {k: np.array(v) for k, v in out.items()}
+
+
+def residual_traces(cloth, model, points, stream=None):
+    """From the current frame-start state: predict, then (plain) VBD iterations with
+    the FP64 relative residual of every instance after each count in `points`, and the
+    same from the learned guess. Returns (plain, learned), arrays (len(points), ninst);
+    the frame-start state is restored."""
+    x0, v0 = cloth.state(stream=stream)
+    traces = []
+    for warm in (False, True):
+        cloth.set_state(x0, v0, stream=stream)
+        cloth.predict(stream=stream)
+        r0 = cloth.residual(stream=stream)
+        if warm:
+            cloth.warm_start(model, fallback=True, stream=stream)
+        done = 0
+        rows = []
+        for k in points:
+            if k > done:
+                cloth.vbd_iterations(k - done, stream=stream)
+                done = k
+            rows.append(np.where(r0 > 0, cloth.residual(stream=stream) / np.where(r0 > 0, r0, 1.0), 0.0))
+        traces.append(np.array(rows))
+    cloth.set_state(x0, v0, stream=stream)
+    return traces[0], traces[1]
+
+
+def iterations_to(trace, points, tol):
+    """Per instance the first count in `points` at which the trace is <= tol (-1: never)."""
+    hit = trace <= tol
+    first = np.argmax(hit, axis=0)
+    return np.where(hit.any(axis=0), np.asarray(points)[first], -1)
+
+
+def tolerance_sweep(cloth, insts, model, tols, points, frames, seed0, stream=None):
+    """Residual traces of both forms over `frames` held-out frames (the trajectory
+    advanced by plain CUDA-graph frames between them), and per tolerance the
+    iterations each form needs (vertex-weighted over instance-frames that reached it
+    within max(points), and the fraction that did)."""
+    masses = [float(i.mass.sum()) for i in insts]
+    nv = np.array([i.num_verts for i in insts], dtype=np.float64)
+    plain, learned = [], []
+    for f in range(frames):
+        cloth.set_accel(wind_table(np.random.RandomState(seed0 + f), masses), stream=stream)
+        p, l = residual_traces(cloth, model, points, stream=stream)
+        plain.append(p)
+        learned.append(l)
+        cloth.frame(graph=True, stream=stream)
+    plain = np.concatenate(plain, axis=1)  # (points, frames * ninst)
+    learned = np.concatenate(learned, axis=1)
+    w = np.tile(nv, frames)
+    rows = []
+    for tol in tols:
+        row = {"tol": tol}
+        for name, tr in (("plain", plain), ("learned", learned)):
+            it = iterations_to(tr, points, tol)
+            ok = it >= 0
+            row[name + "_reached_fraction"] = float(ok.mean())
+            row[name + "_iterations_vertex_weighted"] = (float(np.sum(it[ok] * w[ok]) / np.sum(w[ok]))
+                                                         if ok.any() else None)
+            row[name + "_iterations_p50"] = float(np.median(it[ok])) if ok.any() else None
+        rows.append(row)
+    trace = {"points": list(map(int, points)),
+             "plain_median": np.median(plain, axis=1).tolist(), "learned_median": np.median(learned, axis=1).tolist(),
+             "plain_max": np.max(plain, axis=1).tolist(), "learned_max": np.max(learned, axis=1).tolist(),
+             "plain_min": np.min(plain, axis=1).tolist(), "learned_min": np.min(learned, axis=1).tolist()}
+    return rows, trace
+
+
+def timed_to_tolerance(cloth, insts, model, tol, cap, check_every, frames, seed0, stream=None):
+    """Mean frame time (ms) of both forms to `tol` (cap iterations) over `frames`
+    held-out frames from the same starts, and the fraction of instance-frames that
+    reached tol; the trajectory is advanced by the plain frame."""
+    res = fixed_tolerance_frames(cloth, insts, model, tol, cap, check_every, frames, 0, seed0, stream=stream)
+    return {"tol": tol, "plain_ms": float(np.mean(res["plain_ms"])), "learned_ms": float(np.mean(res["learned_ms"])),
+            "speedup": float(np.mean(res["plain_ms"]) / np.mean(res["learned_ms"])),
+            "plain_reached_fraction": float(np.mean(res["plain_res"] <= tol)),
+            "learned_reached_fraction": float(np.mean(res["learned_res"] <= tol))}

@@ -647,6 +647,55 @@ static double grad_norm(const Scene& s, const std::vector<V3>& x) {
     return std::sqrt(n2);
 }
 
+// The same norm gathered per vertex on the thread pool (each vertex sums its own
+// inertia, spring and bending terms over its adjacency lists, then the squares are
+// summed in vertex order): the probe of the CPU to-residual frame. It differs from
+// grad_norm only in FP64 summation order.
+static double grad_norm_pool(const Scene& s, const std::vector<V3>& x) {
+    const double h = (double)s.sub_dt();
+    std::vector<double> g2(s.nv, 0.0);
+    s.pool->parallel_for(s.nv, 256, [&](uint vid) {
+        if (s.fixed[vid]) return;
+        double gr[3];
+        const double m = s.mass[vid];
+        for (int k = 0; k < 3; ++k) {
+            const double a = (double)s.p.gravity[k];
+            const double y = (double)comp(s.x_start[vid], k) + h * (double)comp(s.v[vid], k) + h * h * a;
+            gr[k] = m / (h * h) * ((double)comp(x[vid], k) - y);
+        }
+        for (uint e : s.adj_edges[vid]) {
+            const auto& ed = s.edges[e];
+            double d[3], l2 = 0;
+            for (int k = 0; k < 3; ++k) {
+                d[k] = (double)comp(x[ed[1]], k) - (double)comp(x[ed[0]], k);
+                l2 += d[k] * d[k];
+            }
+            const double l = std::sqrt(l2);
+            if (l < 1e-30) continue;
+            const double C = l - (double)s.rest_len[e];
+            const double sign = (uint)ed[1] == vid ? 1.0 : -1.0;
+            for (int k = 0; k < 3; ++k) gr[k] += sign * (double)s.p.k_stretch * C * d[k] / l;
+        }
+        for (uint e : s.adj_bending[vid]) {
+            const auto& be = s.bending[e];
+            const M4& Q = s.Q[e];
+            for (int i = 0; i < 4; ++i) {
+                if ((uint)be[i] != vid) continue;
+                for (int k = 0; k < 3; ++k) {
+                    double acc = 0;
+                    for (int j = 0; j < 4; ++j)
+                        if (j != i) acc += (double)Q.c[i][j] * ((double)comp(x[be[j]], k) - (double)comp(x[be[i]], k));
+                    gr[k] += (double)s.p.k_bend * acc;
+                }
+            }
+        }
+        g2[vid] = gr[0] * gr[0] + gr[1] * gr[1] + gr[2] * gr[2];
+    });
+    double n2 = 0;
+    for (uint vid = 0; vid < s.nv; ++vid) n2 += g2[vid];
+    return std::sqrt(n2);
+}
+
 }  // namespace ato
 
 // ---------------------------------------------------------------- C API (ctypes)
@@ -832,6 +881,48 @@ void ato_frame(void* h, int solver, double* energy_log, int with_bending, double
     s->v_frame_end = s->v;
 }
 
+// One VBD frame iterated to a relative residual, the CPU counterpart of the GPU's
+// residual-driven frame (the reference defines no residual; it is the norm of the
+// incremental-potential gradient over free vertices, relative to its value at the
+// inertial prediction y). Per substep: predict; r0 = ||grad G(y)||; VBD iterations
+// (example2:1481-1509), probed after every check_every iterations and at
+// max_iterations; the substep stops once ||grad G(x)|| <= tol * r0 (or at once when
+// r0 == 0); then the velocity update. Returns the iterations of the last substep;
+// *rel_out (nullable) receives its last probed relative residual.
+int ato_frame_to_residual(void* h, double tol, int check_every, int max_iterations, double* rel_out) {
+    Scene* s = (Scene*)h;
+    s->x_frame_start = s->x_frame_end;
+    s->v_frame_start = s->v_frame_end;
+    s->x_start = s->x_frame_start;
+    s->v_start = s->v_frame_start;
+    s->x = s->x_frame_start;
+    s->v = s->v_frame_start;
+    if (check_every < 1) check_every = 1;
+    int used = 0;
+    double rel = 0.0;
+    for (int sub = 0; sub < s->p.num_substep; ++sub) {
+        predict_position(*s);
+        const double r0 = grad_norm_pool(*s, s->x);
+        used = 0;
+        rel = r0 > 0.0 ? 1.0 : 0.0;
+        if (r0 > 0.0) {
+            while (used < max_iterations) {
+                const int chunk = std::min(check_every, max_iterations - used);
+                for (int it = 0; it < chunk; ++it)
+                    for (uint c = 0; c < s->vert_colors.size(); ++c) vbd_color(*s, c);
+                used += chunk;
+                rel = grad_norm_pool(*s, s->x) / r0;
+                if (rel <= tol) break;
+            }
+        }
+        update_velocity(*s);
+    }
+    s->x_frame_end = s->x;
+    s->v_frame_end = s->v;
+    if (rel_out) *rel_out = rel;
+    return used;
+}
+
 // Runs `frames` frames back to back (no logging), for the CPU baseline timing.
 void ato_run_frames(void* h, int solver, int frames) {
     for (int f = 0; f < frames; ++f) ato_frame(h, solver, nullptr, 0, nullptr);
@@ -850,6 +941,12 @@ double ato_grad_norm_of(void* h, const float* xin) {
     std::vector<V3> x(s->nv);
     for (uint i = 0; i < s->nv; ++i) x[i] = v3(xin[3 * i], xin[3 * i + 1], xin[3 * i + 2]);
     return grad_norm(*s, x);
+}
+double ato_grad_norm_pool_of(void* h, const float* xin) {
+    Scene* s = (Scene*)h;
+    std::vector<V3> x(s->nv);
+    for (uint i = 0; i < s->nv; ++i) x[i] = v3(xin[3 * i], xin[3 * i + 1], xin[3 * i + 2]);
+    return grad_norm_pool(*s, x);
 }
 // Prepare a frame for energy_of / grad_norm_of: x_start = frame end state, v = frame end v.
 void ato_begin_frame(void* h) {

@@ -62,10 +62,14 @@ def lib():
         L.ato_set_gravity.argtypes = [P, ctypes.c_float, ctypes.c_float, ctypes.c_float]
         L.ato_frame.argtypes = [P, ctypes.c_int, dp, ctypes.c_int, dp]
         L.ato_run_frames.argtypes = [P, ctypes.c_int, ctypes.c_int]
+        L.ato_frame_to_residual.argtypes = [P, ctypes.c_double, ctypes.c_int, ctypes.c_int, dp]
+        L.ato_frame_to_residual.restype = ctypes.c_int
         L.ato_energy_of.argtypes = [P, fp, ctypes.c_int]
         L.ato_energy_of.restype = ctypes.c_double
         L.ato_grad_norm_of.argtypes = [P, fp]
         L.ato_grad_norm_of.restype = ctypes.c_double
+        L.ato_grad_norm_pool_of.argtypes = [P, fp]
+        L.ato_grad_norm_pool_of.restype = ctypes.c_double
         L.ato_begin_frame.argtypes = [P]
         L.ato_reference_pins.argtypes = [fp, ctypes.c_int, u8p]
         _lib = L
@@ -177,6 +181,13 @@ class Scene:
                         _p(r, ctypes.c_double) if r is not None else None)
         return e, r
 
+    def frame_to_residual(self, tol, check_every=10, max_iterations=1000):
+        """One VBD frame iterated until ||grad G(x)|| <= tol ||grad G(y)||, probed every
+        check_every iterations and at max_iterations -> (iterations, relative residual)."""
+        r = ctypes.c_double(0.0)
+        it = lib().ato_frame_to_residual(self.h, float(tol), int(check_every), int(max_iterations), ctypes.byref(r))
+        return int(it), float(r.value)
+
     def run(self, frames, solver="vbd"):
         lib().ato_run_frames(self.h, 0 if solver == "vbd" else 1, frames)
 
@@ -186,6 +197,11 @@ class Scene:
     def energy_of(self, x, with_bending=True):
         x = np.ascontiguousarray(x, dtype=np.float32)
         return lib().ato_energy_of(self.h, _p(x, ctypes.c_float), int(with_bending))
+
+    def grad_norm_pool_of(self, x):
+        """grad_norm_of gathered per vertex on the thread pool (the to-residual probe)."""
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        return lib().ato_grad_norm_pool_of(self.h, _p(x, ctypes.c_float))
 
     def grad_norm_of(self, x):
         x = np.ascontiguousarray(x, dtype=np.float32)

@@ -1,7 +1,7 @@
 """Generates the golden fixtures under tests/golden/ from the reference tree.
 
-Run in a container that has the reference checkout (read-only) at
-REFERENCE_ROOT (default /root/reference); the GPU box never runs this script.
+Run where a reference checkout exists, with REFERENCE_ROOT set to its root
+(required; the script exits otherwise); the GPU box never runs this script.
 
 Outputs:
   square8k_mesh.npz          positions (float32, V x 3) and 0-based faces (int32, F x 3)
@@ -25,7 +25,7 @@ import sys
 
 import numpy as np
 
-REF = os.environ.get("REFERENCE_ROOT", "/root/reference")
+REF = os.environ.get("REFERENCE_ROOT")
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
@@ -72,6 +72,8 @@ def heft_case():
 
 
 def main():
+    if not REF or not os.path.isdir(REF):
+        sys.exit("set REFERENCE_ROOT to the root of a libAtsSim checkout")
     pos, faces = read_obj(os.path.join(REF, "resources/models/square8K.obj"))
     np.savez_compressed(os.path.join(HERE, "square8k_mesh.npz"), positions=pos, faces=faces)
     json.dump(energy_lists(), open(os.path.join(HERE, "example2_energy_frame30.json"), "w"), indent=1)
