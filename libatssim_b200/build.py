@@ -74,7 +74,7 @@ def build(verbose=False, ptxas_info=False):
     return LIB
 
 
-TEST_SOURCES = ["heft_case.cpp", "vbd_dag.cpp", "launch_modes.cpp"]
+TEST_SOURCES = ["heft_case.cpp", "vbd_dag.cpp", "launch_modes.cpp", "example2_sequence.cpp"]
 
 
 def build_tests():
@@ -89,7 +89,7 @@ def build_tests():
         exe = os.path.join(out_dir, src[:-4])
         deps = [path, lib, os.path.join(root, "include", "ats_launcher.hpp"), os.path.join(root, "include", "ats_cloth.h")]
         if _stale(exe, deps):
-            _run([CXX, "-O2", "-std=c++17", "-I" + os.path.join(root, "include"), "-o", exe, path,
+            _run([CXX, "-O2", "-std=c++20", "-I" + os.path.join(root, "include"), "-o", exe, path,
                   "-L" + LIBDIR, "-lats_b200", "-Wl,-rpath," + LIBDIR, "-lpthread"])
         outs[src[:-4]] = exe
     return outs

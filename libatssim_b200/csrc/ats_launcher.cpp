@@ -18,33 +18,23 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
+#include <cmath>
 #include <chrono>
+#include <condition_variable>
 #include <cstdio>
 #include <functional>
+#include <mutex>
+#include <set>
 #include <stack>
+#include <thread>
 
 namespace Launcher {
 
-const std::map<FunctionID, std::string> taskNames = {
-    {id_xpbd_non, "id_xpbd_non"},
-    {id_additional_root, "id_additional_root"},
-    {id_additional_terminal, "id_additional_terminal"},
-    {id_task_heft_2002, "id_task_heft_2002"},
-    {id_xpbd_constraint_stretch_mass_spring, "id_xpbd_constraint_stretch_mass_spring"},
-    {id_xpbd_constraint_bending, "id_xpbd_constraint_bending"},
-    {id_xpbd_constraint_last_node, "id_xpbd_constraint_last_node"},
-    {id_xpbd_constraint_self_collision_vv_half_cloth, "id_xpbd_constraint_self_collision_vv_half_cloth"},
-    {id_vbd_evaluate_inertia, "id_vbd_evaluate_inertia"},
-    {id_vbd_evaluate_stretch_mass_spring, "id_vbd_evaluate_stretch_mass_spring"},
-    {id_vbd_evaluate_bending, "id_vbd_evaluate_bending"},
-    {id_vbd_step, "id_vbd_step"},
-    {id_vbd_all_in_one, "id_vbd_all_in_one"},
-    {id_xpbd_predict_position, "id_xpbd_predict_position"},
-    {id_xpbd_reset_constrains, "id_xpbd_reset_constrains"},
-    {id_xpbd_reset_collision_constrains, "id_xpbd_reset_collision_constrains"},
-    {id_xpbd_update_velocity, "id_xpbd_update_velocity"},
-    {id_xpbd_copy_to_cpu_gpu, "id_xpbd_copy_to_cpu_gpu"},
-    {id_xpbd_read_and_solve_conflict, "id_xpbd_read_and_solve_conflict"},
+const std::unordered_map<FunctionID, std::string> taskNames = {
+#define ATS_LAUNCHER_NAME_ENTRY(name) {name, #name},
+    ATS_LAUNCHER_FUNCTION_IDS(ATS_LAUNCHER_NAME_ENTRY)
+#undef ATS_LAUNCHER_NAME_ENTRY
 };
 
 static const char* name_of(FunctionID f) {
@@ -67,6 +57,13 @@ const Implementation& Task::get_implementation(const DeviceType& t, bool& find) 
         }
     find = false;
     return list_implementation.empty() ? none : list_implementation[0];
+}
+
+void Task::print_with_cluster(const uint tid) const {
+    if (iter_idx != -1u)
+        std::printf("    Task %u in iteration %2u's cluster %u => %s\n", tid, iter_idx, cluster_idx, name_of(func_id));
+    else
+        std::printf("    Task %u with cluster %u => %s\n", tid, cluster_idx, name_of(func_id));
 }
 
 uint Scheduler::add_task(const Task& task) {
@@ -179,11 +176,13 @@ void Scheduler::profile_costs(const std::function<LaunchParam(const Task&)>& tas
                               std::vector<std::pair<FunctionID, uint>>& keys, std::vector<std::vector<double>>& costs) {
     keys.clear();
     costs.clear();
+    repeats = std::max(1, repeats);
     std::map<std::pair<uint, uint>, uint> seen;  // (func, cluster) -> representative task
     for (uint t = 0; t < list_task.size(); ++t) {
         const auto key = std::make_pair((uint)list_task[t].func_id, list_task[t].cluster_idx);
         if (!seen.count(key)) seen[key] = t;
     }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
     for (const auto& kv : seen) {
         const Task& task = list_task[kv.second];
         std::vector<double> row(nprocs, (double)inf);
@@ -194,15 +193,36 @@ void Scheduler::profile_costs(const std::function<LaunchParam(const Task&)>& tas
             drain(p);
             imp.launch_task(task_to_param(task));  // warm-up
             drain(p);
-            const auto t0 = std::chrono::steady_clock::now();
-            for (int r = 0; r < repeats; ++r) imp.launch_task(task_to_param(task));
-            drain(p);
-            const auto t1 = std::chrono::steady_clock::now();
-            row[p] = std::chrono::duration<double, std::milli>(t1 - t0).count() / std::max(1, repeats);
+            auto sit = device_stream.find(p);
+            if (p != DeviceTypeCpu && sit != device_stream.end()) {
+                // device time between two events on the device's stream
+                cudaStream_t st = (cudaStream_t)sit->second;
+                if (!e0 && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)) {
+                    std::fprintf(stderr, "profile_costs: cudaEventCreate failed\n");
+                    return;
+                }
+                cudaEventRecord(e0, st);
+                for (int r = 0; r < repeats; ++r) imp.launch_task(task_to_param(task));
+                cudaEventRecord(e1, st);
+                float ms = 0.f;
+                if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+                    std::fprintf(stderr, "profile_costs: event timing failed\n");
+                    continue;
+                }
+                row[p] = (double)ms / repeats;
+            } else {
+                const auto t0 = std::chrono::steady_clock::now();
+                for (int r = 0; r < repeats; ++r) imp.launch_task(task_to_param(task));
+                drain(p);
+                const auto t1 = std::chrono::steady_clock::now();
+                row[p] = std::chrono::duration<double, std::milli>(t1 - t0).count() / repeats;
+            }
         }
         keys.push_back({task.func_id, task.cluster_idx});
         costs.push_back(row);
     }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
 }
 
 void Scheduler::standardizing_dag(const std::vector<std::function<void(const LaunchParam&)>>& empty_fns) {
@@ -214,6 +234,8 @@ void Scheduler::standardizing_dag(const std::vector<std::function<void(const Lau
     for (uint t = 0; t < list_task.size(); ++t)
         if (list_task[t].predecessors.empty()) sources.push_back(t);
     root_node = add_task(Task(id_additional_root, 0, false, true, empty));
+    list_task[root_node].is_computation_time_constant = true;
+    list_task[root_node].is_empty_node = true;
     computation_matrix.push_back(std::vector<float>(nprocs, 0.f));
     list_order.insert(list_order.begin(), root_node);
     for (uint t : sources) set_connect(root_node, t, 0.f);
@@ -221,6 +243,8 @@ void Scheduler::standardizing_dag(const std::vector<std::function<void(const Lau
     for (uint t = 0; t < list_task.size(); ++t)
         if (list_task[t].successors.empty()) sinks.push_back(t);
     terminal_node = add_task(Task(id_additional_terminal, 0, false, true, empty));
+    list_task[terminal_node].is_computation_time_constant = true;
+    list_task[terminal_node].is_empty_node = true;
     computation_matrix.push_back(std::vector<float>(nprocs, 0.f));
     list_order.push_back(terminal_node);
     for (uint t : sinks) set_connect(t, terminal_node, 0.f);
@@ -358,11 +382,47 @@ void Scheduler::scheduler_dag() {
 
 void Scheduler::make_wait_events() {
     wait_events.clear();
+    launch_events.clear();
     if (proc_schedules.empty()) return;
-    for (uint t = 0; t < list_task.size(); ++t)
+    const uint n = (uint)list_task.size();
+    for (uint t = 0; t < n; ++t)
         for (uint pred : list_task[t].predecessors)
             if (task_schedules[pred].proc != task_schedules[t].proc)
                 wait_events.push_back(WaitEvent{t, task_schedules[t].proc, pred});
+    // launch events: split every processor's job list before a task that waits for
+    // another processor and after a task that another processor waits for
+    launch_events.assign(proc_schedules.size(), {});
+    for (uint p = 0; p < proc_schedules.size(); ++p) {
+        const auto& jobs = proc_schedules[p];
+        LaunchEvent cur;
+        bool open = false;
+        for (uint i = 0; i < jobs.size(); ++i) {
+            const Task& t = list_task[jobs[i].task_id];
+            std::vector<uint> waits;
+            for (uint pred : t.predecessors)
+                if (task_schedules[pred].proc != p) waits.push_back(pred);
+            bool signal = false;
+            for (uint succ : t.successors) signal |= task_schedules[succ].proc != p;
+            if (open && !waits.empty()) {
+                launch_events[p].push_back(cur);
+                open = false;
+            }
+            if (!open) {
+                cur = LaunchEvent();
+                cur.proc = p;
+                cur.start_idx = i;
+                open = true;
+            }
+            cur.end_idx = i;
+            cur.waits.insert(cur.waits.end(), waits.begin(), waits.end());
+            if (signal) {
+                cur.signal = true;
+                launch_events[p].push_back(cur);
+                open = false;
+            }
+        }
+        if (open) launch_events[p].push_back(cur);
+    }
 }
 
 float Scheduler::get_scheduled_end_time() const {
@@ -403,20 +463,277 @@ void Scheduler::print_sort_by_typology() const {
                     name_of(list_task[t].func_id));
 }
 
+void Scheduler::print_schedule_to_graph_xpbd() const {
+    if (proc_schedules.empty()) {
+        std::fprintf(stderr, "print_schedule_to_graph_xpbd: no schedule; call scheduler_dag first\n");
+        return;
+    }
+    // colour key: the rank of the task's function id among the scheduled ones, plus
+    // its cluster (so the colours of one function sit next to each other)
+    std::set<uint> funcs;
+    for (const auto& jobs : proc_schedules)
+        for (const auto& e : jobs) funcs.insert((uint)list_task[e.task_id].func_id);
+    std::map<uint, uint> base;
+    uint next = 0;
+    for (uint f : funcs) {
+        base[f] = next;
+        uint maxc = 0;
+        for (const auto& t : list_task)
+            if ((uint)t.func_id == f) maxc = std::max(maxc, t.cluster_idx);
+        next += maxc + 1;
+    }
+    std::printf("\n Task of each processor\n");
+    for (size_t p = 0; p < proc_schedules.size(); ++p) {
+        const auto& jobs = proc_schedules[p];
+        std::printf("    [");
+        for (size_t i = 0; i < jobs.size(); ++i) {
+            const ScheduleEvent& e = jobs[i];
+            const Task& t = list_task[e.task_id];
+            std::printf("(%u, %u, %d, %4.3f, %4.3f)%s", base[(uint)t.func_id] + t.cluster_idx, e.task_id,
+                        (int)t.buffer_idx, (double)e.start, (double)e.end, i + 1 < jobs.size() ? ", " : "");
+        }
+        std::printf("],\n");
+        for (size_t i = 0; i < jobs.size(); ++i) {
+            const ScheduleEvent& e = jobs[i];
+            if (e.task_id < computation_matrix.size() && p < computation_matrix[e.task_id].size() &&
+                std::fabs((e.end - e.start) - computation_matrix[e.task_id][p]) > 0.001f)
+                std::fprintf(stderr, "   task %u: scheduled length %g does not match its cost %g\n", e.task_id,
+                             (double)(e.end - e.start), (double)computation_matrix[e.task_id][p]);
+        }
+    }
+    std::printf("    [");
+    for (const WaitEvent& w : wait_events) {
+        const ScheduleEvent& in = task_schedules[w.wait_task];
+        const ScheduleEvent& cur = task_schedules[w.task_id];
+        std::printf("(%u, %u, %u, %u, %4.3f, %4.3f), ", in.proc, w.wait_task, cur.proc, w.task_id, (double)in.end,
+                    (double)cur.start);
+    }
+    std::printf("],\n");
+}
+
 void Scheduler::set_device_sync(DeviceType d, std::function<void()> fn) { device_sync[d] = std::move(fn); }
+
+void Scheduler::set_device_stream(DeviceType d, void* cuda_stream) { device_stream[d] = cuda_stream; }
 
 void Scheduler::drain(DeviceType d) const {
     auto it = device_sync.find(d);
     if (it != device_sync.end()) {
         it->second();
-    } else if (d != DeviceTypeCpu) {
-        cudaError_t e = cudaDeviceSynchronize();
-        if (e != cudaSuccess) std::fprintf(stderr, "launch: device sync failed: %s\n", cudaGetErrorString(e));
+        return;
     }
+    if (d == DeviceTypeCpu) return;
+    auto st = device_stream.find(d);
+    const cudaError_t e = st != device_stream.end() ? cudaStreamSynchronize((cudaStream_t)st->second)
+                                                    : cudaDeviceSynchronize();
+    if (e != cudaSuccess) std::fprintf(stderr, "launch: device drain failed: %s\n", cudaGetErrorString(e));
+}
+
+void Scheduler::refit_runtime_cost(const std::vector<float>& runtime_cost_cpu, const std::vector<float>& runtime_cost_gpu) {
+    if (launch_events.size() < 2 || proc_schedules.size() < 2) return;
+    const std::vector<float>* measured[2] = {&runtime_cost_cpu, &runtime_cost_gpu};
+    for (uint p = 0; p < 2; ++p) {
+        const auto& events = launch_events[p];
+        const auto& jobs = proc_schedules[p];
+        const float inner = fn_get_inner_communication_cost(p);
+        for (size_t k = 0; k < events.size() && k < measured[p]->size(); ++k) {
+            const LaunchEvent& ev = events[k];
+            float planned = 0.f;
+            uint free_tasks = 0;
+            for (uint i = ev.start_idx; i <= ev.end_idx; ++i) {
+                const uint tid = jobs[i].task_id;
+                planned += computation_matrix[tid][p];
+                if (i != ev.end_idx) planned += inner;
+                if (!list_task[tid].is_computation_time_constant) ++free_tasks;
+            }
+            if (free_tasks == 0) continue;
+            const float share = ((*measured[p])[k] - planned) / (float)free_tasks;
+            for (uint i = ev.start_idx; i <= ev.end_idx; ++i) {
+                const uint tid = jobs[i].task_id;
+                if (!list_task[tid].is_computation_time_constant)
+                    computation_matrix[tid][p] = std::max(computation_matrix[tid][p] + 0.5f * share, 0.f);
+            }
+        }
+    }
+}
+
+// LaunchModeHetero: the GPU launch events are issued by a second host thread, the CPU
+// ones run on the calling thread, both in schedule order. A GPU event that depends on
+// CPU tasks is issued once the CPU thread has finished them (host counter). A CPU
+// event that depends on GPU tasks waits until the GPU event holding them is issued,
+// then for its completion: the CUDA event recorded after it on the device stream
+// (set_device_stream), polled; without a stream, the device drain (the sync hook, or a
+// device synchronisation). Every wait is bounded by wait_timeout_ms.
+void Scheduler::launch_hetero(const std::function<LaunchParam(const Task&)>& task_to_param, bool fully_not_wait) {
+    last_status = LaunchOk;
+    if (launch_events.size() < 2 || proc_schedules.size() < 2) {
+        std::fprintf(stderr, "launch: Hetero needs scheduler_dag() and make_wait_events() with two processors\n");
+        last_status = LaunchMissingImplementation;
+        return;
+    }
+    const auto& cpu_ev = launch_events[0];
+    const auto& gpu_ev = launch_events[1];
+    const auto& cpu_jobs = proc_schedules[0];
+    const auto& gpu_jobs = proc_schedules[1];
+    const uint n = (uint)list_task.size();
+    std::vector<int> cpu_pos(n, -1), gpu_event_of(n, -1);
+    for (uint i = 0; i < cpu_jobs.size(); ++i) cpu_pos[cpu_jobs[i].task_id] = (int)i;
+    for (uint g = 0; g < gpu_ev.size(); ++g)
+        for (uint i = gpu_ev[g].start_idx; i <= gpu_ev[g].end_idx; ++i) gpu_event_of[gpu_jobs[i].task_id] = (int)g;
+    auto sit = device_stream.find(DeviceTypeGpu);
+    const bool use_events = sit != device_stream.end();
+    cudaStream_t st = use_events ? (cudaStream_t)sit->second : nullptr;
+    int device = 0;
+    if (use_events) cudaGetDevice(&device);
+    const size_t G = gpu_ev.size();
+    std::vector<cudaEvent_t> ev_begin(use_events ? G : 0, nullptr), ev_end(use_events ? G : 0, nullptr);
+    auto destroy_events = [&] {
+        for (auto e : ev_begin)
+            if (e) cudaEventDestroy(e);
+        for (auto e : ev_end)
+            if (e) cudaEventDestroy(e);
+    };
+    for (size_t g = 0; g < ev_begin.size(); ++g)
+        if (cudaEventCreate(&ev_begin[g]) != cudaSuccess || cudaEventCreate(&ev_end[g]) != cudaSuccess) {
+            std::fprintf(stderr, "launch: cudaEventCreate failed\n");
+            destroy_events();
+            last_status = LaunchCudaError;
+            return;
+        }
+    std::mutex mu;
+    std::condition_variable cv;
+    int cpu_done = 0;       // CPU jobs finished (a prefix of cpu_jobs)
+    size_t gpu_issued = 0;  // GPU launch events issued (and their end events recorded)
+    std::atomic<int> status{LaunchOk};
+    const auto limit = std::chrono::duration<double, std::milli>(wait_timeout_ms);
+    std::vector<float> cpu_cost(cpu_ev.size(), 0.f), gpu_cost(G, 0.f);
+    auto fail = [&](LaunchStatus s) {
+        int ok = LaunchOk;
+        status.compare_exchange_strong(ok, (int)s);
+        cv.notify_all();
+    };
+    auto run_task = [&](uint tid, DeviceType d) -> bool {
+        const Task& t = list_task[tid];
+        bool found = false;
+        const Implementation& imp = t.get_implementation(d, found);
+        if (!found) {
+            std::fprintf(stderr, "launch: task %u (%s) has no implementation for device %u\n", tid, name_of(t.func_id), d);
+            fail(LaunchMissingImplementation);
+            return false;
+        }
+        try {
+            imp.launch_task(task_to_param(t));
+        } catch (...) {
+            std::fprintf(stderr, "launch: task %u (%s) threw\n", tid, name_of(t.func_id));
+            fail(LaunchTaskFailed);
+            return false;
+        }
+        return true;
+    };
+    std::thread gpu_thread([&] {
+        if (use_events) cudaSetDevice(device);
+        for (size_t g = 0; g < G && status.load() == LaunchOk; ++g) {
+            const LaunchEvent& e = gpu_ev[g];
+            int need = 0;
+            for (uint w : e.waits)
+                if (cpu_pos[w] >= 0) need = std::max(need, cpu_pos[w] + 1);
+            if (!fully_not_wait && need > 0) {
+                std::unique_lock<std::mutex> lk(mu);
+                if (!cv.wait_for(lk, limit, [&] { return cpu_done >= need || status.load() != LaunchOk; })) {
+                    lk.unlock();
+                    std::fprintf(stderr, "launch: GPU event %zu waited too long for CPU task %d\n", g, need - 1);
+                    fail(LaunchWaitTimeout);
+                    break;
+                }
+                if (status.load() != LaunchOk) break;
+            }
+            const auto t0 = std::chrono::steady_clock::now();
+            if (use_events) cudaEventRecord(ev_begin[g], st);
+            bool ok = true;
+            for (uint i = e.start_idx; i <= e.end_idx && ok; ++i) ok = run_task(gpu_jobs[i].task_id, DeviceTypeGpu);
+            if (use_events) cudaEventRecord(ev_end[g], st);
+            else gpu_cost[g] = (float)std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                gpu_issued = g + 1;
+            }
+            cv.notify_all();
+            if (!ok) break;
+        }
+    });
+    // waits until GPU launch event g is issued, then until it has completed
+    auto wait_gpu_event = [&](size_t g) -> bool {
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            if (!cv.wait_for(lk, limit, [&] { return gpu_issued > g || status.load() != LaunchOk; })) {
+                lk.unlock();
+                std::fprintf(stderr, "launch: GPU event %zu was not issued in time\n", g);
+                fail(LaunchWaitTimeout);
+                return false;
+            }
+            if (gpu_issued <= g) return false;
+        }
+        if (!use_events) {
+            drain(DeviceTypeGpu);
+            return true;
+        }
+        const auto t0 = std::chrono::steady_clock::now();
+        for (;;) {
+            const cudaError_t q = cudaEventQuery(ev_end[g]);
+            if (q == cudaSuccess) return true;
+            if (q != cudaErrorNotReady) {
+                std::fprintf(stderr, "launch: GPU event %zu: %s\n", g, cudaGetErrorString(q));
+                fail(LaunchCudaError);
+                return false;
+            }
+            if (std::chrono::steady_clock::now() - t0 > limit) {
+                std::fprintf(stderr, "launch: GPU event %zu did not complete in time\n", g);
+                fail(LaunchWaitTimeout);
+                return false;
+            }
+            std::this_thread::sleep_for(std::chrono::microseconds(20));
+        }
+    };
+    for (size_t c = 0; c < cpu_ev.size() && status.load() == LaunchOk; ++c) {
+        const LaunchEvent& e = cpu_ev[c];
+        bool ok = true;
+        if (!fully_not_wait) {
+            int last = -1;
+            for (uint w : e.waits) last = std::max(last, gpu_event_of[w]);
+            if (last >= 0) ok = wait_gpu_event((size_t)last);  // one stream: earlier events complete first
+        }
+        if (!ok) break;
+        const auto t0 = std::chrono::steady_clock::now();
+        for (uint i = e.start_idx; i <= e.end_idx && ok; ++i) ok = run_task(cpu_jobs[i].task_id, DeviceTypeCpu);
+        cpu_cost[c] = (float)std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            cpu_done = (int)e.end_idx + 1;
+        }
+        cv.notify_all();
+        if (!ok) break;
+    }
+    gpu_thread.join();
+    if (status.load() == LaunchOk && G > 0 && !fully_not_wait) {
+        if (use_events) wait_gpu_event(G - 1);
+        else drain(DeviceTypeGpu);
+    }
+    if (status.load() == LaunchOk) {
+        for (size_t g = 0; g < ev_begin.size(); ++g) {
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, ev_begin[g], ev_end[g]) == cudaSuccess) gpu_cost[g] = ms;
+        }
+        last_runtime_costs = {cpu_cost, gpu_cost};
+        if (runtime_refit && !fully_not_wait) refit_runtime_cost(cpu_cost, gpu_cost);
+    } else if (use_events) {
+        cudaStreamSynchronize(st);  // nothing of this launch stays in flight
+    }
+    destroy_events();
+    last_status = (LaunchStatus)status.load();
 }
 
 void Scheduler::launch(LaunchMode mode, const std::function<LaunchParam(const Task&)>& task_to_param, bool fully_not_wait,
                        const std::vector<std::function<void()>>& /*assemble_impl*/) {
+    last_status = LaunchOk;
     const std::vector<uint>& order = !sorted_nodes.empty() ? sorted_nodes : list_order;
     if (order.empty()) {
         std::fprintf(stderr, "launch: neither a topological nor a ranked order; call topological_sort first\n");
@@ -481,9 +798,12 @@ void Scheduler::launch(LaunchMode mode, const std::function<LaunchParam(const Ta
         }
         return;
     }
-    // Hetero / ProgressiveHetero / FakeHetero: each task on its scheduled device. A
-    // host task that depends on device work not yet drained waits for it first;
-    // device work that depends on host tasks is enqueued after them (start order).
+    if (mode == LaunchModeHetero || mode == LaunchModeProgressiveHetero) {
+        launch_hetero(task_to_param, fully_not_wait);
+        return;
+    }
+    // FakeHetero: each task on its scheduled device, one at a time in order of
+    // scheduled start, the GPU drained after every task.
     const bool synchronous = mode == LaunchModeFakeHetero;
     std::vector<uint8_t> pending(list_task.size(), 0);  // device task enqueued, not yet drained
     for (const auto& e : plan) {

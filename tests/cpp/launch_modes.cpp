@@ -3,8 +3,10 @@
 // with HEFT, then runs it in every launch mode. Both implementations of a task only
 // record (task number, device) in execution order; the device-1 sync hook records a
 // drain as (0, 2). Prints, per mode, the execution log, and the schedule's processor
-// per task.
+// per task. The Hetero mode runs device-1 tasks from a second host thread, so the log
+// is guarded by a mutex and its order is the order of execution.
 #include <cstdio>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -14,9 +16,11 @@ int main() {
     unsigned nprocs = 0, ntasks = 0, nedges = 0;
     if (std::scanf("%u %u %u", &nprocs, &ntasks, &nedges) != 3 || nprocs != 2) return 2;
     std::vector<std::pair<unsigned, unsigned>> log;
+    std::mutex log_mu;
     unsigned drains = 0;
     auto impl = [&](unsigned dev) {
-        return Launcher::Implementation(dev, [&log, dev](const Launcher::LaunchParam& p) {
+        return Launcher::Implementation(dev, [&log, &log_mu, dev](const Launcher::LaunchParam& p) {
+            std::lock_guard<std::mutex> lock(log_mu);
             if (p.iter_idx >= 1) log.push_back({p.iter_idx, dev});
         });
     };
@@ -44,6 +48,7 @@ int main() {
     s.scheduler_dag();
     s.make_wait_events();
     s.set_device_sync(1, [&] {
+        std::lock_guard<std::mutex> lock(log_mu);
         ++drains;
         log.push_back({0u, 2u});  // a drain of device 1, in execution order
     });
@@ -72,7 +77,8 @@ int main() {
         log.clear();
         drains = 0;
         s.launch(m.second, to_param, false);
-        std::printf("%s\"%s\": {\"drains\": %u, \"log\": [", first ? "" : ", ", m.first, drains);
+        std::printf("%s\"%s\": {\"status\": %d, \"drains\": %u, \"log\": [", first ? "" : ", ", m.first,
+                    (int)s.get_last_launch_status(), drains);
         for (size_t i = 0; i < log.size(); ++i) std::printf("%s[%u, %u]", i ? ", " : "", log[i].first, log[i].second);
         std::printf("]}");
         first = false;

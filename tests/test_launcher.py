@@ -82,6 +82,7 @@ def test_launch_modes_on_host_devices(programs):
     assert set(proc.values()) == {0, 1}  # the schedule uses both devices
     n = len(d["computation"])
     for mode, m in out["modes"].items():
+        assert m["status"] == 0, mode
         runs = [(t, dev) for t, dev in m["log"] if dev != 2]
         tasks = [t for t, _ in runs]
         assert len(tasks) == len(set(tasks)), mode
@@ -100,3 +101,32 @@ def test_launch_modes_on_host_devices(programs):
                     assert any(t == 0 and dev == 2 for t, dev in m["log"][pos[a] + 1:pos[b]]), (mode, a, b)
     # work left on device 1 is drained once at the end of a launch
     assert out["modes"]["gpu"]["drains"] == 1 and out["modes"]["cpu"]["drains"] == 0
+
+
+@pytest.mark.parametrize("mode", ["sequence", "fake", "hetero"])
+def test_example2_scheduler_sequence(programs, mode):
+    """examples/example2_async_iter.cpp:1305-1460 written against ats_launcher.hpp: the
+    reference's ids (id_additional_root = 0, predict 62, vbd_all_in_one 54, last node
+    45, update 66 in launcher.h:14-221), every task run once, each cluster's iterations
+    in order, predict first and the velocity update last."""
+    iters, clusters = 3, 4
+    r = subprocess.run([programs["example2_sequence"], str(iters), str(clusters), mode], capture_output=True,
+                       text=True, timeout=60)
+    assert r.returncode == 0, r.stderr
+    lines = r.stdout.strip().splitlines()
+    assert "Task of each processor" in r.stdout  # print_schedule_to_graph_xpbd
+    out = json.loads(lines[-1])
+    assert out["status"] == 0
+    assert out["ids"] == {"predict": 62, "vbd": 54, "last": 45, "update": 66, "root": 0}
+    runs = out["runs"]
+    assert len(runs) == 1 + iters * clusters + 2
+    assert runs[0][0] == 62 and runs[-1][0] == 66 and runs[-2][0] == 45
+    seen = {}
+    for i, (f, it, c, dev) in enumerate(runs):
+        if f == 54:
+            seen[(it, c)] = i
+            if it > 0:
+                assert seen[(it - 1, c)] < i
+    assert len(seen) == iters * clusters
+    devices = {dev for f, it, c, dev in runs}
+    assert devices == ({0} if mode == "sequence" else {0, 1})
