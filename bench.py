@@ -65,7 +65,7 @@ sys.path.insert(0, ROOT)
 METRIC = "frames/s to 1e-4 residual: batched+learned VBD vs plain CUDA VBD, 1 B200"
 UNIT = "frames/s"
 WORKLOADS = {
-    "c4": "c4: 64 batched grid cloths, side U{64..512}, wind per instance; batched+learned vs plain batched VBD, "
+    "c4": "c4: 64 batched grid cloths, side U{{64..512}}, wind per instance; batched+learned vs plain batched VBD, "
           "both iterated to a relative residual of {tol:g} (cap {cap} iterations, probes every {check})",
     "c3": "c3: 128x128 grid cloth, wind per frame; learned vs plain VBD, both iterated to a relative residual of "
           "{tol:g} (cap {cap} iterations, probes every {check})",
@@ -89,6 +89,8 @@ def parse():
     p.add_argument("--cap", type=int, default=200)
     p.add_argument("--check-every", type=int, default=10)
     p.add_argument("--train-steps", type=int, default=150000)
+    p.add_argument("--instances", type=int, default=0, help="only the first N instances (a small case for profiling)")
+    p.add_argument("--record-frames", type=int, default=30, help="recorded frames per trajectory (c4)")
     p.add_argument("--sweep-cap", type=int, default=400, help="iterations of the residual traces")
     p.add_argument("--trace-out", default="", help="write the full residual traces (JSON) here")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -386,10 +388,12 @@ def run_learned(args):
     wl = args.workload
     if wl == "c4":
         all_insts, prm = configs.c4()
-        traj, frames = 2, 30
+        traj, frames = 2, args.record_frames
     else:
         all_insts, prm = configs.c3()
         traj, frames = 20, 100
+    if args.instances:
+        all_insts = all_insts[:args.instances]
     insts = all_insts
     if world > 1:
         insts, _ = sharding.shard(all_insts, args.cap)
@@ -466,7 +470,7 @@ def run_learned(args):
     state_bytes = 2 * 3 * 4 * nv
 
     sweep, trace, timed_tols = None, None, None
-    if world == 1:
+    if world == 1 and args.sweep_cap > 0:
         points = sorted(set([0, 1, 2, 3, 5, 7, 10, 15, 20, 30, 40, 50, 70, 100, 150, 200, 300, 400, 600, 800, 1000,
                              1500, 2000, 3000, 4000, 5000]) | {args.sweep_cap})
         points = [p for p in points if p <= args.sweep_cap]
@@ -495,6 +499,7 @@ def run_learned(args):
                "dtype": "f32 (MLP bf16 / fp32 accumulate; residuals fp64)", "data": "synthetic",
                "config": {"workload": WORKLOADS[wl].format(tol=args.tol, cap=args.cap, check=args.check_every),
                           "instances": len(all_insts), "vertices": sum(i.num_verts for i in all_insts),
+                          "recorded_frames": traj * frames,
                           "tol": args.tol, "cap": args.cap, "check_every": args.check_every,
                           "parallelism": f"instance-shards{world}", "create_s": t_create,
                           "threads_per_vertex": info.threads_per_vertex, "block_size": info.block_size,

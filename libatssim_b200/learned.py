@@ -132,15 +132,19 @@ def fixed_tolerance_frames(cloth, insts, model, tol, cap, check_every, frames, w
         cloth.set_accel(wind_table(np.random.RandomState(seed0 + f), masses), stream=st)
         x0, v0 = cloth.state(stream=st)
         torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push("learned_frame")  # lets a profiler select these kernels
         ev[0].record(st)
         it_l, r_l, used = cloth.frame_warm_to_residual(model, tol, check_every=check_every, max_iterations=cap,
                                                        stream=st)
         ev[1].record(st)
+        torch.cuda.nvtx.range_pop()
         cloth.set_state(x0, v0, stream=st)
         torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push("plain_frame")
         ev[2].record(st)
         it_p, r_p = cloth.frame_to_residual(tol, check_every=check_every, max_iterations=cap, stream=st)
         ev[3].record(st)
+        torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
         if timed:
             out["learned_ms"].append(ev[0].elapsed_time(ev[1]))
