@@ -74,27 +74,5 @@ def build(verbose=False, ptxas_info=False):
     return LIB
 
 
-TEST_SOURCES = ["heft_case.cpp", "vbd_dag.cpp", "launch_modes.cpp", "example2_sequence.cpp"]
-
-
-def build_tests():
-    """C++ programs of tests/cpp linked against the library (boundary tests)."""
-    lib = build()
-    root = os.path.dirname(PKG)
-    out_dir = os.path.join(BUILD, "tests")
-    os.makedirs(out_dir, exist_ok=True)
-    outs = {}
-    for src in TEST_SOURCES:
-        path = os.path.join(root, "tests", "cpp", src)
-        exe = os.path.join(out_dir, src[:-4])
-        deps = [path, lib, os.path.join(root, "include", "ats_launcher.hpp"), os.path.join(root, "include", "ats_cloth.h")]
-        if _stale(exe, deps):
-            _run([CXX, "-O2", "-std=c++20", "-I" + os.path.join(root, "include"), "-o", exe, path,
-                  "-L" + LIBDIR, "-lats_b200", "-Wl,-rpath," + LIBDIR, "-lpthread"])
-        outs[src[:-4]] = exe
-    return outs
-
-
 if __name__ == "__main__":
     print(build(verbose=True, ptxas_info="--ptxas" in sys.argv))
-    print(build_tests())

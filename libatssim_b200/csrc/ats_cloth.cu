@@ -101,79 +101,97 @@ __global__ void update_kernel(const float4* __restrict__ x, float4* __restrict__
     x0[i] = make_float4(p.x, p.y, p.z, q.w);
 }
 
-// solve_stretch_mass_spring_template (xpbd_constraints.h:984-1059) for one colour.
-// Programmatic dependent launch: the constraint's ids, rest length, stiffness and the
-// endpoints' inverse masses (constant for the handle) are loaded before the wait on the
-// previous colour; positions and lambda after it.
-__global__ void xpbd_stretch_kernel(float4* __restrict__ x, const float4* __restrict__ vm, const int2* __restrict__ edge,
-                                    const float* __restrict__ rest, const float* __restrict__ kst,
-                                    float* __restrict__ lambda, int b, int e, float h) {
-    const int i = b + blockIdx.x * blockDim.x + threadIdx.x;
-    int2 ed = make_int2(0, 0);
-    float L = 0.f, k = 0.f, w0 = 0.f, w1 = 0.f;
-    if (i < e) {
-        ed = __ldg(&edge[i]);
-        L = __ldg(&rest[i]);
-        k = __ldg(&kst[i]);
-        w0 = __ldg(&vm[ed.x]).z;
-        w1 = __ldg(&vm[ed.y]).z;
-    }
-    grid_dependency_wait();
-    allow_dependent_launch();
-    if (i >= e) return;
-    float4 p0 = x[ed.x], p1 = x[ed.y];
-    float lam = lambda[i];
-    float3 d = make_float3(fs(p1.x, p0.x), fs(p1.y, p0.y), fs(p1.z, p0.z));
-    float lsq = fdot(d, d);
+// Position access of the XPBD bodies: plain loads / stores in the per-colour kernels
+// (each launch starts with a clean L1), L2-only ones in the persistent kernel, whose
+// blocks read vertices that other SMs wrote since the last grid barrier.
+struct PlainMem {
+    static __device__ __forceinline__ float4 ld(const float4* p) { return *p; }
+    static __device__ __forceinline__ void st(float4* p, float4 v) { *p = v; }
+};
+struct L2Mem {
+    static __device__ __forceinline__ float4 ld(const float4* p) { return __ldcg(p); }
+    static __device__ __forceinline__ void st(float4* p, float4 v) { __stcg(p, v); }
+};
+
+// The constant data of one stretch constraint: vertex ids, rest length, stiffness and
+// the endpoints' inverse masses.
+struct StretchConst {
+    int2 ed;
+    float L, k, w0, w1;
+};
+__device__ __forceinline__ StretchConst load_stretch(int i, const float4* __restrict__ vm, const int2* __restrict__ edge,
+                                                     const float* __restrict__ rest, const float* __restrict__ kst) {
+    StretchConst c;
+    c.ed = __ldg(&edge[i]);
+    c.L = __ldg(&rest[i]);
+    c.k = __ldg(&kst[i]);
+    c.w0 = __ldg(&vm[c.ed.x]).z;
+    c.w1 = __ldg(&vm[c.ed.y]).z;
+    return c;
+}
+
+// solve_stretch_mass_spring_template (xpbd_constraints.h:984-1059) for constraint i.
+template <class M>
+__device__ __forceinline__ void solve_stretch(float4* __restrict__ x, float* __restrict__ lambda, int i,
+                                              const StretchConst& c, float h) {
+    const float4 p0 = M::ld(&x[c.ed.x]), p1 = M::ld(&x[c.ed.y]);
+    const float lam = lambda[i];
+    const float3 d = make_float3(fs(p1.x, p0.x), fs(p1.y, p0.y), fs(p1.z, p0.z));
+    const float lsq = fdot(d, d);
     if ((double)lsq < 1e-8) return;
-    float l = sqrtf(lsq);
-    float C = fs(l, L);
-    float gx = -(d.x / l), gy = -(d.y / l), gz = -(d.z / l);
-    float alpha = k < kEps ? 1e9f : 1.f / fm(fm(k, h), h);
-    float denom = fa(alpha, fa(w0, w1));
-    float dl = fs(-C, fm(alpha, lam)) / denom;
+    const float l = sqrtf(lsq);
+    const float C = fs(l, c.L);
+    const float gx = -(d.x / l), gy = -(d.y / l), gz = -(d.z / l);
+    const float alpha = c.k < kEps ? 1e9f : 1.f / fm(fm(c.k, h), h);
+    const float denom = fa(alpha, fa(c.w0, c.w1));
+    const float dl = fs(-C, fm(alpha, lam)) / denom;
     lambda[i] = fa(lam, dl);
     if (denom != 0.f) {
-        float s0 = fm(dl, w0), s1 = fm(-dl, w1);
-        x[ed.x] = make_float4(fa(p0.x, fm(s0, gx)), fa(p0.y, fm(s0, gy)), fa(p0.z, fm(s0, gz)), p0.w);
-        x[ed.y] = make_float4(fa(p1.x, fm(s1, gx)), fa(p1.y, fm(s1, gy)), fa(p1.z, fm(s1, gz)), p1.w);
+        const float s0 = fm(dl, c.w0), s1 = fm(-dl, c.w1);
+        M::st(&x[c.ed.x], make_float4(fa(p0.x, fm(s0, gx)), fa(p0.y, fm(s0, gy)), fa(p0.z, fm(s0, gz)), p0.w));
+        M::st(&x[c.ed.y], make_float4(fa(p1.x, fm(s1, gx)), fa(p1.y, fm(s1, gy)), fa(p1.z, fm(s1, gz)), p1.w));
     }
 }
 
+// The constant data of one bending constraint: vertex ids, the 10 unique entries of
+// the symmetric Q and k_b, and the inverse masses.
+struct BendConst {
+    int4 id;
+    float4 qa, qb, qc;
+    float w[4];
+};
+__device__ __forceinline__ BendConst load_bend(int i, const float4* __restrict__ vm, const int4* __restrict__ idx,
+                                               const float4* __restrict__ q) {
+    BendConst c;
+    c.id = __ldg(&idx[i]);
+    c.qa = __ldg(&q[3 * i]);
+    c.qb = __ldg(&q[3 * i + 1]);
+    c.qc = __ldg(&q[3 * i + 2]);
+    c.w[0] = __ldg(&vm[c.id.x]).z;
+    c.w[1] = __ldg(&vm[c.id.y]).z;
+    c.w[2] = __ldg(&vm[c.id.z]).z;
+    c.w[3] = __ldg(&vm[c.id.w]).z;
+    return c;
+}
+
 // solve_bending_quadratic_template (xpbd_constraints.h:1170-1229, core :1062-1126,
-// get_delta_xpbd_4 :211-236) for one colour. q holds the 10 unique entries of the
-// symmetric Q, then k_b.
-__global__ void xpbd_bending_kernel(float4* __restrict__ x, const float4* __restrict__ vm, const int4* __restrict__ idx,
-                                    const float4* __restrict__ q, float* __restrict__ lambda, int b, int e, float h) {
-    const int i = b + blockIdx.x * blockDim.x + threadIdx.x;
-    // constant data before the wait on the previous colour (as xpbd_stretch_kernel)
-    int4 id = make_int4(0, 0, 0, 0);
-    float4 qa = make_float4(0.f, 0.f, 0.f, 0.f), qb = qa, qc = qa;
-    float w[4] = {0.f, 0.f, 0.f, 0.f};
-    if (i < e) {
-        id = __ldg(&idx[i]);
-        qa = __ldg(&q[3 * i]);
-        qb = __ldg(&q[3 * i + 1]);
-        qc = __ldg(&q[3 * i + 2]);
-        w[0] = __ldg(&vm[id.x]).z;
-        w[1] = __ldg(&vm[id.y]).z;
-        w[2] = __ldg(&vm[id.z]).z;
-        w[3] = __ldg(&vm[id.w]).z;
-    }
-    grid_dependency_wait();
-    allow_dependent_launch();
-    if (i >= e) return;
+// get_delta_xpbd_4 :211-236) for constraint i.
+template <class M>
+__device__ __forceinline__ void solve_bend(float4* __restrict__ x, float* __restrict__ lambda, int i,
+                                           const BendConst& c, float h) {
     float Q[4][4];
-    Q[0][0] = qa.x; Q[0][1] = Q[1][0] = qa.y; Q[0][2] = Q[2][0] = qa.z; Q[0][3] = Q[3][0] = qa.w;
-    Q[1][1] = qb.x; Q[1][2] = Q[2][1] = qb.y; Q[1][3] = Q[3][1] = qb.z; Q[2][2] = qb.w;
-    Q[2][3] = Q[3][2] = qc.x; Q[3][3] = qc.y;
-    const float kb = qc.z;
-    const int vid[4] = {id.x, id.y, id.z, id.w};
+    Q[0][0] = c.qa.x; Q[0][1] = Q[1][0] = c.qa.y; Q[0][2] = Q[2][0] = c.qa.z; Q[0][3] = Q[3][0] = c.qa.w;
+    Q[1][1] = c.qb.x; Q[1][2] = Q[2][1] = c.qb.y; Q[1][3] = Q[3][1] = c.qb.z; Q[2][2] = c.qb.w;
+    Q[2][3] = Q[3][2] = c.qc.x; Q[3][3] = c.qc.y;
+    const float kb = c.qc.z;
+    const int vid[4] = {c.id.x, c.id.y, c.id.z, c.id.w};
     float3 p[4];
+    float pw[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-        float4 t = x[vid[j]];
+        const float4 t = M::ld(&x[vid[j]]);
         p[j] = make_float3(t.x, t.y, t.z);
+        pw[j] = t.w;
     }
     // C = 1/2 sum_ij Q_ij <x_i, x_j>
     float sum = 0.f;
@@ -181,7 +199,7 @@ __global__ void xpbd_bending_kernel(float4* __restrict__ x, const float4* __rest
     for (int ii = 0; ii < 4; ++ii)
 #pragma unroll
         for (int jj = 0; jj < 4; ++jj) sum = fa(sum, fm(Q[ii][jj], fdot(p[ii], p[jj])));
-    float C = fm(0.5f, sum);
+    const float C = fm(0.5f, sum);
     // gradient_i = sum_j Q_ij x_j (the negated force of the reference)
     float3 g[4];
     float denom = 0.f;
@@ -195,19 +213,155 @@ __global__ void xpbd_bending_kernel(float4* __restrict__ x, const float4* __rest
             gz = fa(gz, fm(Q[ii][jj], p[jj].z));
         }
         g[ii] = make_float3(gx, gy, gz);
-        denom = fa(denom, fm(w[ii], fdot(g[ii], g[ii])));
+        denom = fa(denom, fm(c.w[ii], fdot(g[ii], g[ii])));
     }
-    float alpha = kb < kEps ? 1e12f : 1.f / fm(fm(kb, h), h);
+    const float alpha = kb < kEps ? 1e12f : 1.f / fm(fm(kb, h), h);
     denom = fa(denom, alpha);
-    float lam = lambda[i];
-    float dl = fs(-C, fm(alpha, lam)) / denom;
+    const float lam = lambda[i];
+    const float dl = fs(-C, fm(alpha, lam)) / denom;
     lambda[i] = fa(lam, dl);
     if (denom != 0.f) {
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            float s = fm(dl, w[j]);
-            float4 t = x[vid[j]];
-            x[vid[j]] = make_float4(fa(p[j].x, fm(s, g[j].x)), fa(p[j].y, fm(s, g[j].y)), fa(p[j].z, fm(s, g[j].z)), t.w);
+            const float s = fm(dl, c.w[j]);
+            M::st(&x[vid[j]],
+                  make_float4(fa(p[j].x, fm(s, g[j].x)), fa(p[j].y, fm(s, g[j].y)), fa(p[j].z, fm(s, g[j].z)), pw[j]));
+        }
+    }
+}
+
+// One stretch colour. Programmatic dependent launch: the constraint's constant data is
+// loaded before the wait on the previous colour; positions and lambda after it.
+__global__ void xpbd_stretch_kernel(float4* __restrict__ x, const float4* __restrict__ vm, const int2* __restrict__ edge,
+                                    const float* __restrict__ rest, const float* __restrict__ kst,
+                                    float* __restrict__ lambda, int b, int e, float h) {
+    const int i = b + blockIdx.x * blockDim.x + threadIdx.x;
+    StretchConst c = {};
+    if (i < e) c = load_stretch(i, vm, edge, rest, kst);
+    grid_dependency_wait();
+    allow_dependent_launch();
+    if (i < e) solve_stretch<PlainMem>(x, lambda, i, c, h);
+}
+
+// One bending colour (as xpbd_stretch_kernel).
+__global__ void xpbd_bending_kernel(float4* __restrict__ x, const float4* __restrict__ vm, const int4* __restrict__ idx,
+                                    const float4* __restrict__ q, float* __restrict__ lambda, int b, int e, float h) {
+    const int i = b + blockIdx.x * blockDim.x + threadIdx.x;
+    BendConst c = {};
+    if (i < e) c = load_bend(i, vm, idx, q);
+    grid_dependency_wait();
+    allow_dependent_launch();
+    if (i < e) solve_bend<PlainMem>(x, lambda, i, c, h);
+}
+
+// Grid-wide barrier of the persistent XPBD kernel, whose blocks are co-resident (a
+// cooperative launch). bar[0] counts arrivals, bar[1] is the generation. Thread 0 of
+// every block reads the generation, publishes the block's writes (device-scope fence)
+// and arrives; the last arrival resets the count and advances the generation, the
+// others wait for that. The wait is bounded: after kBarrierSpins polls it sets *err
+// and every block leaves the kernel at its next barrier. Returns false on error.
+constexpr unsigned kBarrierSpins = 1u << 24;
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, int* err, unsigned nblocks) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned* gen = bar + 1;
+        const unsigned my_gen = *gen;
+        __threadfence();
+        const unsigned arrived = atomicAdd(bar, 1u);
+        if (arrived == nblocks - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            unsigned spins = 0;
+            while (*gen == my_gen) {
+                if (++spins > kBarrierSpins || *(volatile int*)err) {
+                    atomicExch(err, 1);
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+        s_ok = *(volatile int*)err == 0;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+constexpr int kXpbdLoopThreads = 640;  // one block per SM, up to 96 registers a thread
+
+struct XpbdLoopArgs {
+    float4* x;
+    const float4* vm;
+    const int2* edge;
+    const float* rest;
+    const float* kst;
+    float* slambda;
+    const int4* bidx;
+    const float4* bq;
+    float* blambda;
+    const int* scolor;  // n_scolors + 1 offsets
+    const int* bcolor;  // n_bcolors + 1 offsets
+    int nsc, nbc, iterations;
+    float h;
+    unsigned* bar;
+    int* err;
+};
+
+// `iterations` XPBD iterations (every stretch colour, then every bending colour, as
+// the per-colour launches run them) in one cooperative launch: each colour is a
+// grid-stride loop, colours are separated by grid_barrier. Each thread loads the
+// constant data of its first constraint of the next colour before the barrier, so
+// only the position gather waits for the previous colour. Same arithmetic, same
+// results as the per-colour kernels.
+__global__ void __launch_bounds__(kXpbdLoopThreads, 1) xpbd_loop_kernel(XpbdLoopArgs a) {
+    const int stride = gridDim.x * blockDim.x;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int phases = a.nsc + a.nbc;
+    if (phases == 0) return;
+    auto range = [&](int ph, int& b, int& e) {
+        if (ph < a.nsc) {
+            b = __ldg(&a.scolor[ph]);
+            e = __ldg(&a.scolor[ph + 1]);
+        } else {
+            b = __ldg(&a.bcolor[ph - a.nsc]);
+            e = __ldg(&a.bcolor[ph - a.nsc + 1]);
+        }
+    };
+    StretchConst sc = {};
+    BendConst bc = {};
+    int b, e;
+    range(0, b, e);
+    if (b + t < e) {
+        if (a.nsc > 0) sc = load_stretch(b + t, a.vm, a.edge, a.rest, a.kst);
+        else bc = load_bend(b + t, a.vm, a.bidx, a.bq);
+    }
+    for (int it = 0; it < a.iterations; ++it) {
+        for (int ph = 0; ph < phases; ++ph) {
+            range(ph, b, e);
+            const bool stretch = ph < a.nsc;
+            int i = b + t;
+            if (i < e) {
+                if (stretch) solve_stretch<L2Mem>(a.x, a.slambda, i, sc, a.h);
+                else solve_bend<L2Mem>(a.x, a.blambda, i, bc, a.h);
+                for (i += stride; i < e; i += stride) {
+                    if (stretch) solve_stretch<L2Mem>(a.x, a.slambda, i, load_stretch(i, a.vm, a.edge, a.rest, a.kst), a.h);
+                    else solve_bend<L2Mem>(a.x, a.blambda, i, load_bend(i, a.vm, a.bidx, a.bq), a.h);
+                }
+            }
+            // the next colour's first constraint of this thread, ahead of the barrier
+            const int nph = ph + 1 < phases ? ph + 1 : 0;
+            if (it + 1 < a.iterations || nph != 0) {
+                int nb, ne;
+                range(nph, nb, ne);
+                if (nb + t < ne) {
+                    if (nph < a.nsc) sc = load_stretch(nb + t, a.vm, a.edge, a.rest, a.kst);
+                    else bc = load_bend(nb + t, a.vm, a.bidx, a.bq);
+                }
+            }
+            if (!grid_barrier(a.bar, a.err, gridDim.x)) return;
         }
     }
 }
@@ -858,8 +1012,48 @@ int launch_xpbd_bending(ats_cloth* c, int color, cudaStream_t st) {
     return ATS_OK;
 }
 
+// `iterations` XPBD iterations as one cooperative launch of xpbd_loop_kernel (one
+// block per SM), the barrier state reset on the stream first.
+int launch_xpbd_loop(ats_cloth* c, int iterations, cudaStream_t st) {
+    XpbdLoopArgs a;
+    a.x = c->x.p;
+    a.vm = c->vm.p;
+    a.edge = (const int2*)c->xs_edge.p;
+    a.rest = c->xs_rest.p;
+    a.kst = c->xs_k.p;
+    a.slambda = c->xs_lambda.p;
+    a.bidx = (const int4*)c->xb_idx.p;
+    a.bq = (const float4*)c->xb_q.p;
+    a.blambda = c->xb_lambda.p;
+    a.scolor = c->xs_color_d.p;
+    a.bcolor = c->xb_color_d.p;
+    a.nsc = c->L.n_scolors;
+    a.nbc = c->L.n_bcolors;
+    a.iterations = iterations;
+    a.h = c->h;
+    a.bar = c->loop_bar.p;
+    a.err = c->loop_err.p;
+    ATS_CUDA(cudaMemsetAsync(c->loop_bar.p, 0, 2 * sizeof(unsigned), st));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(c->xpbd_loop_blocks);
+    cfg.blockDim = dim3(kXpbdLoopThreads);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    ATS_CUDA(cudaLaunchKernelEx(&cfg, xpbd_loop_kernel, a));
+    count_launch(st);
+    return ATS_OK;
+}
+
 int enqueue_iterations(ats_cloth* c, int solver, int iterations, cudaStream_t st, const int* active) {
     int r;
+    if (solver == ATS_SOLVER_XPBD && c->xpbd_loop_blocks > 0 && iterations > 0 &&
+        c->L.n_scolors + c->L.n_bcolors > 0)
+        return launch_xpbd_loop(c, iterations, st);
     for (int it = 0; it < iterations; ++it) {
         if (solver == ATS_SOLVER_VBD) {
             for (int col = 0; col < c->L.n_vcolors; ++col)
@@ -1288,6 +1482,23 @@ int ats_cloth_create(const ats_instance_desc* inst, int ninst, const ats_solver_
     if ((r = upload(c->xb_idx, L.xb_idx, L.xb_idx.size() / 4)) || (r = upload(c->xb_q, L.xb_q, L.xb_q.size() / 4)))
         return r;
     ATS_CUDA(c->xb_lambda.alloc(L.xb_idx.size() / 4));
+    // the persistent XPBD kernel: colour offsets on the device, barrier state, and one
+    // 1024-thread block per SM when the device runs cooperative launches of it
+    if ((r = upload(c->xs_color_d, L.xs_color, L.xs_color.size())) ||
+        (r = upload(c->xb_color_d, L.xb_color, L.xb_color.size())))
+        return r;
+    ATS_CUDA(c->loop_bar.alloc(2));
+    ATS_CUDA(c->loop_err.alloc(1));
+    ATS_CUDA(cudaMemset(c->loop_bar.p, 0, 2 * sizeof(unsigned)));
+    ATS_CUDA(cudaMemset(c->loop_err.p, 0, sizeof(int)));
+    {
+        int coop = 0, sms = 0, per_sm = 0;
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c->device);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, xpbd_loop_kernel, kXpbdLoopThreads, 0) != cudaSuccess)
+            per_sm = 0;
+        c->xpbd_loop_blocks = coop && per_sm >= 1 ? sms : 0;
+    }
     if ((r = upload(c->en_edge, L.en_edge, L.en_rest.size())) || (r = upload(c->en_rest, L.en_rest, L.en_rest.size())) ||
         (r = upload(c->en_k, L.en_k, L.en_k.size())) || (r = upload(c->en_bend, L.en_bend, L.en_kb.size())) ||
         (r = upload(c->en_q, L.en_q, L.en_q.size())) || (r = upload(c->en_kb, L.en_kb, L.en_kb.size())))
@@ -1380,6 +1591,19 @@ int ats_set_positions(ats_cloth* c, const float* x, ats_stream stream) {
     return ATS_OK;
 }
 
+// A grid barrier of the persistent XPBD kernel that ran out of polls leaves loop_err
+// set (the kernel returned early); the next state read reports it once and clears it.
+static int check_loop_error(ats_cloth* c, cudaStream_t st) {
+    if (!c->loop_err.p) return ATS_OK;
+    ATS_CUDA(cudaMemcpyAsync(c->host_flag, c->loop_err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    ATS_CUDA(cudaStreamSynchronize(st));
+    if (*c->host_flag == 0) return ATS_OK;
+    ATS_CUDA(cudaMemsetAsync(c->loop_err.p, 0, sizeof(int), st));
+    ATS_CUDA(cudaStreamSynchronize(st));
+    set_error("XPBD persistent kernel: a grid barrier wait expired; the frame stopped early");
+    return ATS_ERR_TIMEOUT;
+}
+
 static int read_back(ats_cloth* c, const float4* src, float* dst, float* staging, cudaStream_t st) {
     const int n = c->L.nv;
     gather_state_kernel<<<(n + 255) / 256, 256, 0, st>>>(src, c->to_caller.p, staging, n); count_launch(st);
@@ -1426,7 +1650,7 @@ int ats_get_state(ats_cloth* c, float* x, float* v, ats_stream stream) {
     if (!r && v) r = read_back(c, c->vel.p, v, c->io_v.p, st);
     if (r) return r;
     ATS_CUDA(cudaStreamSynchronize(st));
-    return ATS_OK;
+    return check_loop_error(c, st);
 }
 
 int ats_get_positions(ats_cloth* c, float* x, ats_stream stream) {

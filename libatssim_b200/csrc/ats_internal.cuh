@@ -74,6 +74,10 @@ struct ats_cloth {
     DevBuf<int4> xb_idx;
     DevBuf<float4> xb_q;
     DevBuf<float> xb_lambda;
+    DevBuf<int> xs_color_d, xb_color_d;  // XPBD colour offsets, for the persistent kernel
+    DevBuf<unsigned> loop_bar;           // its grid barrier: arrivals, generation
+    DevBuf<int> loop_err;                // set when a barrier wait ran out
+    int xpbd_loop_blocks = 0;            // co-resident blocks of the persistent kernel (0: per-colour launches)
     DevBuf<int2> en_edge;
     DevBuf<float> en_rest, en_k, en_q, en_kb;
     DevBuf<int4> en_bend;

@@ -923,6 +923,44 @@ int ato_frame_to_residual(void* h, double tol, int check_every, int max_iteratio
     return used;
 }
 
+// The frame as separate steps, for a scheduler that runs each task on its own
+// device: ato_frame_begin (the frame-start bookkeeping of ato_frame), ato_predict
+// (Core::predict_position), ato_vbd_color (one colour of solve_constraints_VBD),
+// ato_update (Core::update_velocity, then the frame-end state), and access to the
+// current iterate x (3 floats per vertex).
+void ato_frame_begin(void* h) {
+    Scene* s = (Scene*)h;
+    s->x_frame_start = s->x_frame_end;
+    s->v_frame_start = s->v_frame_end;
+    s->x_start = s->x_frame_start;
+    s->v_start = s->v_frame_start;
+    s->x = s->x_frame_start;
+    s->v = s->v_frame_start;
+}
+void ato_predict(void* h) { predict_position(*(Scene*)h); }
+void ato_vbd_color(void* h, int c) {
+    Scene* s = (Scene*)h;
+    if (c >= 0 && (size_t)c < s->vert_colors.size()) vbd_color(*s, (uint)c);
+}
+void ato_update(void* h) {
+    Scene* s = (Scene*)h;
+    update_velocity(*s);
+    s->x_frame_end = s->x;
+    s->v_frame_end = s->v;
+}
+void ato_get_x(void* h, float* x) {
+    Scene* s = (Scene*)h;
+    for (uint i = 0; i < s->nv; ++i) {
+        x[3 * i] = s->x[i].x;
+        x[3 * i + 1] = s->x[i].y;
+        x[3 * i + 2] = s->x[i].z;
+    }
+}
+void ato_set_x(void* h, const float* x) {
+    Scene* s = (Scene*)h;
+    for (uint i = 0; i < s->nv; ++i) s->x[i] = v3(x[3 * i], x[3 * i + 1], x[3 * i + 2]);
+}
+
 // Runs `frames` frames back to back (no logging), for the CPU baseline timing.
 void ato_run_frames(void* h, int solver, int frames) {
     for (int f = 0; f < frames; ++f) ato_frame(h, solver, nullptr, 0, nullptr);

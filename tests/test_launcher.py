@@ -16,8 +16,10 @@ GOLD = os.path.join(os.path.dirname(__file__), "golden")
 
 @pytest.fixture(scope="module")
 def programs(ats):
-    from libatssim_b200 import build
-    return build.build_tests()
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "cpp"))
+    from build_programs import build_programs
+    return build_programs()
 
 
 def heft_input(d):
@@ -50,22 +52,55 @@ def test_heft_rejects_cycles(programs):
     assert "cycle" in r.stderr
 
 
-@pytest.mark.gpu
-@pytest.mark.parametrize("mode", ["gpu", "hetero", "fake", "profiled"])
-def test_vbd_task_graph_through_scheduler(programs, mode):
-    r = subprocess.run([programs["vbd_dag"], "32", "8", "4", mode], capture_output=True, text=True, timeout=300)
+def _vbd_dag(programs, mode, n=24, iters=6, frames=3):
+    r = subprocess.run([programs["vbd_dag"], str(n), str(iters), str(frames), mode], capture_output=True, text=True,
+                       timeout=300)
     assert r.returncode == 0, r.stderr
     lines = r.stdout.strip().splitlines()
-    if mode == "profiled":
-        prof = json.loads(lines[0])["profiled"]
-        # one measured row per distinct (function id, colour); both devices implement every task
-        assert len(prof) == 3 + 4 and all(c > 0 for row in prof for c in row[2:])
-    out = json.loads(lines[-1])
-    assert out["max_abs_diff"] == 0.0
-    assert out["max_displacement"] > 1e-3
-    # predict + 8 x 4 colours + last node + update + root + terminal, all on the B200
-    assert out["tasks"] == 1 + 8 * 4 + 2 + 2
-    assert out["tasks_on_gpu"] >= 8 * 4
+    return json.loads(lines[-1]), lines
+
+
+@pytest.mark.gpu
+def test_vbd_task_graph_single_device_modes(programs):
+    """Every task on the B200 (the CUDA solver through the C ABI) gives exactly the
+    frames of ats_frame; every task on the host (the oracle's per-step entry points)
+    gives exactly the oracle's frames."""
+    gpu, _ = _vbd_dag(programs, "gpu")
+    assert gpu["status"] == 0 and gpu["rel_l2_vs_gpu_alone"] == 0.0
+    assert gpu["max_displacement"] > 1e-3
+    cpu, _ = _vbd_dag(programs, "cpu")
+    assert cpu["status"] == 0 and cpu["rel_l2_vs_oracle_alone"] == 0.0
+    # 2 cloths x (predict + 6 x 4 colours + last node + update) + root + terminal
+    assert gpu["tasks"] == 2 * (1 + 6 * 4 + 2) + 2
+
+
+@pytest.mark.gpu
+def test_vbd_task_graph_split_between_cpu_and_b200(programs):
+    """The HEFT schedule puts colour sweeps on both the host (oracle) and the B200
+    (CUDA). Hetero runs both devices at once, ordered by CUDA events and host
+    counters; FakeHetero runs the same schedule one task at a time. Their positions
+    are bit-identical, and close to either device alone."""
+    fake, _ = _vbd_dag(programs, "fake")
+    het, _ = _vbd_dag(programs, "hetero")
+    for out in (fake, het):
+        assert out["status"] == 0
+        assert out["sweeps_on_cpu"] > 0 and out["sweeps_on_gpu"] > 0
+        assert out["cross_device_waits"] > 0
+        assert out["rel_l2_vs_gpu_alone"] < 1e-4 and out["rel_l2_vs_oracle_alone"] < 1e-4
+    assert het["digest"] == fake["digest"]
+    # the Hetero launch measured every launch event (GPU by CUDA events) for the refit
+    assert het["measured_events"] == het["launch_events"]
+
+
+@pytest.mark.gpu
+def test_vbd_task_graph_profiled_costs(programs):
+    out, lines = _vbd_dag(programs, "profiled")
+    prof = json.loads(lines[0])["profiled"]
+    # one measured row per distinct (function id, colour) on both devices
+    assert len(prof) == 3 + 4 and all(c >= 0 for row in prof for c in row[2:])
+    sweeps = [row for row in prof if row[0] == "id_vbd_all_in_one"]
+    assert all(row[2] > 0 and row[3] > 0 for row in sweeps)
+    assert out["status"] == 0 and out["rel_l2_vs_gpu_alone"] < 1e-4
 
 
 def test_launch_modes_on_host_devices(programs):

@@ -413,3 +413,29 @@ def test_irregular_meshes_match_oracle(ats, oracle, mesh):
     for _ in range(10):
         cx.frame(ats.SOLVER_XPBD)
     assert rel_l2(cx.state()[0], sx.state()[0]) < 1e-6
+
+
+@pytest.mark.parametrize("n", [32, 200])
+def test_xpbd_persistent_frame_equals_per_colour_launches(ats, n):
+    """XPBD frames run their iterations as one cooperative launch (every colour a
+    grid-stride loop, colours separated by a grid barrier); the per-colour entry points
+    launch one kernel per colour. Both evaluate the same constraint bodies in the same
+    colour order, so the positions are bit-identical."""
+    inst = configs.grid_instance(n)
+    prm = dict(implicit_dt=1.0 / 60.0, num_substep=1, iterations=12, damping=2.0)
+    a = ats.Cloth([inst], **prm)
+    b = ats.Cloth([inst], **prm)
+    for f in range(4):
+        a.frame(ats.SOLVER_XPBD, graph=(f % 2 == 1))
+        b.predict()
+        b.xpbd_reset()
+        for _ in range(prm["iterations"]):
+            for c in range(b.info.num_stretch_colors):
+                b.xpbd_stretch_color(c)
+            for c in range(b.info.num_bending_colors):
+                b.xpbd_bending_color(c)
+        b.update_velocity()
+    xa, va = a.state()
+    xb, vb = b.state()
+    assert np.array_equal(xa, xb) and np.array_equal(va, vb)
+    assert np.linalg.norm(xa - inst.positions) > 1e-3
