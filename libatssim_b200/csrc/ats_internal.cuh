@@ -97,6 +97,7 @@ struct ats_cloth {
     DevBuf<float4> y_buf;
     DevBuf<double> pot_y, pot_guess, pot_vx, pot_vy;
     DevBuf<int> guess_used;
+    DevBuf<int> tc_err;  // set by the tensor-core inference kernel when a completion wait ran out
     cudaGraphExec_t warm_graph = nullptr;  // captured warm-started frame (ats_frame_warm)
     const void* warm_key_mlp = nullptr;
     int warm_key_iters = -1, warm_key_fallback = -1;

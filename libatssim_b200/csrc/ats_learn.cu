@@ -25,6 +25,7 @@
 
 #include "ats_gelu.cuh"
 #include "ats_internal.cuh"
+#include "ats_umma.cuh"
 
 namespace ats {
 namespace {
@@ -563,6 +564,173 @@ __global__ void __launch_bounds__(kThreads, 3) infer_warp_kernel(FeatArgs fa, co
     }
 }
 
+// Inference on the 5th-generation tensor cores: one CTA of 128 threads per tile of 128
+// vertices (the MMA's M), persistent over tiles. Thread r gathers vertex r's features
+// into shared memory; one thread issues each layer as tcgen05.mma (BF16 operands from
+// shared memory, FP32 accumulator in TMEM: layer 1 K = 32 as 2 steps of 16, the others
+// K = 64 as 4); completion arrives on an mbarrier; every thread then reads its own row
+// of the accumulator (tcgen05.ld, warp w owns TMEM lanes 32w..32w+31), adds the bias,
+// applies the polynomial GELU in packed FP32 and writes the BF16 activations back as
+// the next layer's A operand. TMEM columns: layers 1 and 3 at 0..63, 2 at 64..127, the
+// output layer (N = 16, 3 used) at 64..79. Same quantisation points as the training
+// forward (features and activations rounded to BF16, FP32 accumulation); the bias is
+// added after the products instead of before, a different FP32 summation order.
+constexpr int kTcRows = 128;
+constexpr uint32_t kTcCols = 128;
+constexpr uint32_t kTcWaitPolls = 1u << 24;
+struct __align__(128) TcSmem {
+    uint8_t w1[kHid * kInP * 2];      // W1^T, 64 x 32, K-major core matrices
+    uint8_t w2[kHid * kHid * 2];      // W2^T, 64 x 64
+    uint8_t w3[kHid * kHid * 2];      // W3^T
+    uint8_t w4[kOutP * kHid * 2];     // W4^T, 16 x 64 (rows 3..15 zero)
+    uint8_t a1[kTcRows * kInP * 2];   // features of the tile, 128 x 32
+    uint8_t ah[kTcRows * kHid * 2];   // hidden activations, 128 x 64
+    float b[3 * kHid + kOutP];
+    float nrm[kNorm];
+    uint64_t mbar;
+    uint32_t tmem;
+};
+constexpr size_t kTcSmem = sizeof(TcSmem);
+static_assert(offsetof(TcSmem, w2) % 128 == 0 && offsetof(TcSmem, w3) % 128 == 0 && offsetof(TcSmem, w4) % 128 == 0 &&
+                  offsetof(TcSmem, a1) % 128 == 0 && offsetof(TcSmem, ah) % 128 == 0 && offsetof(TcSmem, mbar) % 8 == 0,
+              "operand tiles 128-byte aligned");
+static_assert(kTcSmem <= 56 * 1024, "at most 4 CTAs (4 x 128 TMEM columns) per SM");
+
+// Rows of a packed [rows][K] BF16 matrix (global) into the K-major core-matrix layout.
+__device__ __forceinline__ void tc_stage(uint8_t* dst, const __nv_bfloat16* src, int rows, int K) {
+    const int chunks = rows * (K / 8);
+    for (int i = threadIdx.x; i < chunks; i += blockDim.x) {
+        const int r = i / (K / 8), c = i % (K / 8);
+        *reinterpret_cast<uint4*>(dst + umma::kmajor_offset(r, 8 * c, K)) =
+            *reinterpret_cast<const uint4*>(src + (size_t)r * K + 8 * c);
+    }
+}
+
+// One layer: D[tmem col dcol] = A (128 x K) * W^T (N x K)^T, issued by thread 0 after
+// the CTA's shared-memory writes are visible to the tensor core; returns false (the
+// same on every thread) if the completion wait ran out.
+template <int K, int N>
+__device__ __forceinline__ bool tc_layer(TcSmem& S, const uint8_t* a, const uint8_t* w, uint32_t dcol,
+                                         uint32_t& phase) {
+    umma::fence_proxy_async();
+    umma::fence_before_sync();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        umma::fence_after_sync();
+        constexpr uint32_t sbo = (K / 8) * 128;
+        const uint32_t a0 = umma::smem_u32(a), w0 = umma::smem_u32(w);
+#pragma unroll
+        for (int s = 0; s < K / 16; ++s)
+            umma::mma_bf16(S.tmem + dcol, umma::desc_kmajor(a0 + 256 * s, 128, sbo),
+                           umma::desc_kmajor(w0 + 256 * s, 128, sbo), umma::idesc_bf16_f32(kTcRows, N), s > 0);
+        umma::mma_commit(&S.mbar);
+    }
+    const bool ok = umma::mbar_wait(&S.mbar, phase, kTcWaitPolls);
+    phase ^= 1u;
+    umma::fence_after_sync();
+    __syncwarp();
+    return __syncthreads_and(ok) != 0;
+}
+
+// Row r of a hidden layer: TMEM (64 FP32) + bias -> GELU -> BF16 -> activation tile.
+__device__ __forceinline__ void tc_hidden_epilogue(TcSmem& S, uint32_t dcol, const float* bias) {
+    const int r = threadIdx.x;
+    const uint32_t t = S.tmem + ((uint32_t)(r & ~31) << 16) + dcol;
+    float lo[32], hi[32];
+    umma::tmem_ld32(t, lo);
+    umma::tmem_ld32(t + 32, hi);
+    umma::tmem_ld_wait();
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        uint32_t q[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int n = 8 * c + 2 * j;
+            const float z0 = (n < 32 ? lo[n] : hi[n - 32]) + bias[n];
+            const float z1 = (n + 1 < 32 ? lo[n + 1] : hi[n + 1 - 32]) + bias[n + 1];
+            const float2 g = gelu2(make_float2(z0, z1));
+            q[j] = pack_f2(g.x, g.y);
+        }
+        *reinterpret_cast<uint4*>(S.ah + umma::kmajor_offset(r, 8 * c, kHid)) = make_uint4(q[0], q[1], q[2], q[3]);
+    }
+}
+
+__global__ void __launch_bounds__(kTcRows, 1) infer_tc_kernel(FeatArgs fa, const __nv_bfloat16* __restrict__ wpack,
+                                                              const float* __restrict__ master,
+                                                              const float* __restrict__ nrm, float4* __restrict__ x,
+                                                              float s, int* __restrict__ err) {
+    extern __shared__ __align__(128) uint8_t tc_smem_raw[];
+    TcSmem& S = *reinterpret_cast<TcSmem*>(tc_smem_raw);
+    const int r = threadIdx.x, warp = r >> 5;
+    tc_stage(S.w1, wpack + kP1, kHid, kInP);
+    tc_stage(S.w2, wpack + kP2, kHid, kHid);
+    tc_stage(S.w3, wpack + kP3, kHid, kHid);
+    tc_stage(S.w4, wpack + kP4, kOutP, kHid);
+    for (int i = r; i < kHid; i += kTcRows) {
+        S.b[i] = master[kB1 + i];
+        S.b[kHid + i] = master[kB2 + i];
+        S.b[2 * kHid + i] = master[kB3 + i];
+    }
+    for (int i = r; i < kOutP; i += kTcRows) S.b[3 * kHid + i] = i < kOut ? master[kB4 + i] : 0.f;
+    for (int i = r; i < kNorm; i += kTcRows) S.nrm[i] = nrm[i];
+    if (warp == 0) umma::tmem_alloc(&S.tmem, kTcCols);
+    if (r == 0) umma::mbar_init(&S.mbar, 1);
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    uint32_t phase = 0;
+    bool ok = true;
+    const int ntiles = (fa.nv + kTcRows - 1) / kTcRows;
+    for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+        const int v = tile * kTcRows + r;
+        {
+            float f[kIn];
+            if (v < fa.nv) vertex_features(fa, v, f);
+            uint32_t q[kInP / 2];
+#pragma unroll
+            for (int k = 0; k < kIn / 2; ++k)
+                q[k] = v < fa.nv ? pack_f2((f[2 * k] - S.nrm[kNormInMean + 2 * k]) * S.nrm[kNormInScale + 2 * k],
+                                           (f[2 * k + 1] - S.nrm[kNormInMean + 2 * k + 1]) *
+                                               S.nrm[kNormInScale + 2 * k + 1])
+                                 : 0u;
+#pragma unroll
+            for (int k = kIn / 2; k < kInP / 2; ++k) q[k] = 0u;
+#pragma unroll
+            for (int c = 0; c < kInP / 8; ++c)
+                *reinterpret_cast<uint4*>(S.a1 + umma::kmajor_offset(r, 8 * c, kInP)) =
+                    make_uint4(q[4 * c], q[4 * c + 1], q[4 * c + 2], q[4 * c + 3]);
+        }
+        if (!(ok = tc_layer<kInP, kHid>(S, S.a1, S.w1, 0, phase))) break;
+        tc_hidden_epilogue(S, 0, S.b);
+        if (!(ok = tc_layer<kHid, kHid>(S, S.ah, S.w2, 64, phase))) break;
+        tc_hidden_epilogue(S, 64, S.b + kHid);
+        if (!(ok = tc_layer<kHid, kHid>(S, S.ah, S.w3, 0, phase))) break;
+        tc_hidden_epilogue(S, 0, S.b + 2 * kHid);
+        if (!(ok = tc_layer<kHid, kOutP>(S, S.ah, S.w4, 64, phase))) break;
+        float o[16];
+        umma::tmem_ld16(S.tmem + ((uint32_t)(r & ~31) << 16) + 64, o);
+        umma::tmem_ld_wait();
+        if (v < fa.nv && fa.vm[v].y == 0.f) {
+            float4 p = x[v];
+            p.x += s * (S.nrm[kNormOutMean + 0] + S.nrm[kNormOutStd + 0] * (o[0] + S.b[3 * kHid + 0]));
+            p.y += s * (S.nrm[kNormOutMean + 1] + S.nrm[kNormOutStd + 1] * (o[1] + S.b[3 * kHid + 1]));
+            p.z += s * (S.nrm[kNormOutMean + 2] + S.nrm[kNormOutStd + 2] * (o[2] + S.b[3 * kHid + 2]));
+            x[v] = p;
+        }
+    }
+    if (!ok) {
+        if (r == 0) atomicExch(err, 1);
+        // an MMA may still be in flight: give it one more bounded wait before freeing TMEM
+        umma::mbar_wait(&S.mbar, phase ^ 1u, kTcWaitPolls);
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        umma::fence_after_sync();
+        umma::tmem_free(S.tmem, kTcCols);
+    }
+}
+
 __global__ void copy4_kernel(const float4* __restrict__ src, float4* __restrict__ dst, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) dst[i] = src[i];
@@ -631,6 +799,7 @@ int ensure_partials(ats_mlp* m, int ctas) {
 }
 
 int g_infer_ctas = 148;  // resident CTAs of infer_warp_kernel on the device (set_smem_limits)
+int g_tc_ctas = 148;     // CTAs of infer_tc_kernel: resident ones, at most 4 per SM (TMEM)
 
 // Kernel attributes and launch shapes, set once before any launch or capture.
 int set_smem_limits() {
@@ -642,6 +811,12 @@ int set_smem_limits() {
         ATS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         ATS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, infer_warp_kernel, kThreads, 0));
         g_infer_ctas = std::max(1, sms) * std::max(1, resident);
+        ATS_CUDA(cudaFuncSetAttribute(infer_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
+        int tc_resident = 0;
+        ATS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tc_resident, infer_tc_kernel, kTcRows, kTcSmem));
+        // every resident CTA holds kTcCols of the SM's 512 TMEM columns
+        tc_resident = std::min(tc_resident, (int)(512 / kTcCols));
+        g_tc_ctas = std::max(1, sms) * std::max(1, tc_resident);
     }
     ATS_CUDA(cudaFuncSetAttribute(train_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmem));
     ATS_CUDA(cudaFuncSetAttribute(infer_samples_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmem));
@@ -695,7 +870,24 @@ int ensure_learn_buffers(ats_cloth* c) {
     if (!c->pot_vy.p) ATS_CUDA(c->pot_vy.alloc(nv));
     if (!c->pot_guess.p) ATS_CUDA(c->pot_guess.alloc(c->L.ninst));
     if (!c->guess_used.p) ATS_CUDA(c->guess_used.alloc(c->L.ninst));
+    if (!c->tc_err.p) {
+        ATS_CUDA(c->tc_err.alloc(1));
+        ATS_CUDA(cudaMemset(c->tc_err.p, 0, sizeof(int)));
+    }
     return ATS_OK;
+}
+
+// The inference kernel's error flag, read (and cleared) after a synchronisation.
+int check_tc_error(ats_cloth* c, cudaStream_t st) {
+    if (!c->tc_err.p) return ATS_OK;
+    int flag = 0;
+    ATS_CUDA(cudaMemcpyAsync(&flag, c->tc_err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    ATS_CUDA(cudaStreamSynchronize(st));
+    if (!flag) return ATS_OK;
+    ATS_CUDA(cudaMemsetAsync(c->tc_err.p, 0, sizeof(int), st));
+    ATS_CUDA(cudaStreamSynchronize(st));
+    set_error("warm-start inference: a tensor-core completion wait expired; the guess is incomplete");
+    return ATS_ERR_TIMEOUT;
 }
 
 // after predict: save y, x = guess, then (G(guess), G(y) and the per-instance fallback)
@@ -706,10 +898,10 @@ int enqueue_warm_start(ats_cloth* c, const ats_mlp* m, int fallback, cudaStream_
     copy4_kernel<<<(nv + 255) / 256, 256, 0, st>>>(c->x.p, c->y_buf.p, nv); count_launch(st);
     ATS_CUDA(cudaGetLastError());
     {
-        const int tiles = (nv + kWarpRows - 1) / kWarpRows;
-        const int grid = std::max(1, std::min((tiles + 3) / 4, g_infer_ctas));
-        infer_warp_kernel<<<grid, kThreads, 0, st>>>(feat_args(c), m->wpack.p, m->master.p, m->nrm.p, c->x.p,
-                                                     9.8f * c->h * c->h); count_launch(st);
+        const int tiles = (nv + kTcRows - 1) / kTcRows;
+        const int grid = std::max(1, std::min(tiles, g_tc_ctas));
+        infer_tc_kernel<<<grid, kTcRows, kTcSmem, st>>>(feat_args(c), m->wpack.p, m->master.p, m->nrm.p, c->x.p,
+                                                        9.8f * c->h * c->h, c->tc_err.p); count_launch(st);
     }
     ATS_CUDA(cudaGetLastError());
     if (fallback) {
@@ -1092,6 +1284,7 @@ int ats_warm_start(ats_cloth* c, const ats_mlp* m, int fallback, int* used, ats_
             for (int i = 0; i < c->L.ninst; ++i) used[i] = 1;
         }
         ATS_CUDA(cudaStreamSynchronize(st));
+        return check_tc_error(c, st);
     }
     return ATS_OK;
 }
@@ -1159,7 +1352,7 @@ int ats_frame_warm_to_residual(ats_cloth* c, const ats_mlp* m, int fallback, dou
     cudaStream_t st = S(stream);
     int r = frame_to_residual_impl(c, tol, tols, first_check, check_every, max_iterations, iterations, residual, st,
                                    [&](cudaStream_t s) { return enqueue_warm_start(c, m, fallback, s); });
-    if (r) return r;
+    if (r || (r = check_tc_error(c, st))) return r;
     if (used) {
         if (fallback) {
             ATS_CUDA(cudaMemcpyAsync(used, c->guess_used.p, c->L.ninst * sizeof(int), cudaMemcpyDeviceToHost, st));

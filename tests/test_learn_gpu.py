@@ -165,11 +165,14 @@ def test_learned_warm_start_reaches_plain_residual_in_fewer_iterations(ats):
     assert np.median(needed) < iters, needed
 
 
-def test_warp_tiled_inference_equals_tile_forward(ats):
-    """The frame's inference kernel (register-resident activations, one warp per 16
-    vertices) against ats_mlp_infer (the shared-memory tile forward checked against
-    the oracle): same BF16 rounding points and mma order, so the same guess."""
-    inst = configs.grid_instance(40)
+@pytest.mark.parametrize("n", [40, 181])
+def test_tensor_core_inference_matches_tile_forward(ats, n):
+    """The frame's inference kernel (tcgen05 MMA, FP32 accumulators in tensor memory,
+    128 vertices per tile) against ats_mlp_infer (the shared-memory tile forward that
+    is checked against the oracle). Same BF16 quantisation points; the FP32 sums are
+    ordered differently (bias after the products), which can move a BF16 rounding, so
+    the guesses agree to a tolerance. 181^2 vertices exercise full and partial tiles."""
+    inst = configs.grid_instance(n)
     cloth = ats.Cloth([inst], implicit_dt=1.0 / 60.0, num_substep=1, iterations=10, damping=2.0)
     for _ in range(4):
         cloth.frame()
@@ -187,8 +190,15 @@ def test_warp_tiled_inference_equals_tile_forward(ats):
     order = cloth.vertex_order()
     rows = np.argsort(order)[np.sort(order[free])]
     s = 9.8 / 3600.0
-    expect = y[rows] + np.float32(s) * m.infer(f)
-    assert np.allclose(guess[rows], expect, rtol=0, atol=1e-7)
+    out = m.infer(f)
+    expect = y[rows] + np.float32(s) * out
+    got = (guess[rows] - y[rows]) / np.float32(s)
+    err = np.abs(got - out)
+    scale = np.max(np.abs(out))
+    assert np.linalg.norm(got - out) <= 2e-3 * np.linalg.norm(out), np.linalg.norm(got - out) / np.linalg.norm(out)
+    assert np.max(err) <= 2e-2 * scale, (np.max(err), scale)
+    assert np.median(err) <= 1e-3 * scale
+    assert np.allclose(guess[rows], expect, rtol=0, atol=1e-5)
     pinned = inst.fixed.astype(bool)
     assert np.array_equal(guess[pinned], y[pinned])
 
