@@ -9,11 +9,15 @@
 // The implementations only record which task ran where; the program prints one JSON
 // line: the launch order (function id, iteration, cluster), the device of each run, the
 // scheduled makespan and the launch status. Arguments: iterations clusters mode
-// (mode: sequence | hetero | fake).
+// (mode: sequence | hetero | fake | timeout). In "timeout" the device implementation
+// of the first vbd task sleeps 300 ms while the launch's waits are limited to 50 ms:
+// the Hetero launch must end with LaunchWaitTimeout instead of waiting.
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 #include "ats_launcher.hpp"
@@ -28,7 +32,13 @@ int main(int argc, char** argv) {
     const char* mode_name = argc > 3 ? argv[3] : "sequence";
     std::vector<Run> runs;
     std::mutex mu;
+    const bool slow = !std::strcmp(mode_name, "timeout");
+    bool slept = false;
     auto fn_dispatch = [&](unsigned device, const Launcher::LaunchParam& param) {
+        if (slow && device == 1 && param.function_id == Launcher::id_vbd_all_in_one && !slept) {
+            slept = true;  // only the device thread reaches this
+            std::this_thread::sleep_for(std::chrono::milliseconds(300));
+        }
         std::lock_guard<std::mutex> lock(mu);
         runs.push_back({(unsigned)param.function_id, param.iter_idx, param.cluster_idx, device});
     };
@@ -116,7 +126,8 @@ int main(int argc, char** argv) {
         };
     };
     auto mode = Launcher::Scheduler::LaunchModeSequeceHetero;
-    if (!std::strcmp(mode_name, "hetero")) mode = Launcher::Scheduler::LaunchModeHetero;
+    if (!std::strcmp(mode_name, "hetero") || slow) mode = Launcher::Scheduler::LaunchModeHetero;
+    if (slow) scheduler.set_wait_timeout_ms(50.0);
     if (!std::strcmp(mode_name, "fake")) mode = Launcher::Scheduler::LaunchModeFakeHetero;
     scheduler.set_device_sync(Launcher::DeviceTypeGpu, [] {});  // host-only devices: nothing to drain
     scheduler.launch(mode, fn_task_to_param, false);

@@ -165,3 +165,15 @@ def test_example2_scheduler_sequence(programs, mode):
     assert len(seen) == iters * clusters
     devices = {dev for f, it, c, dev in runs}
     assert devices == ({0} if mode == "sequence" else {0, 1})
+
+
+def test_hetero_launch_wait_is_bounded(programs):
+    """A device task that takes longer than the launch's wait limit ends the Hetero
+    launch with LaunchWaitTimeout (status 1) and a message, instead of blocking: the
+    failure is made on the host (a slow implementation), not on a GPU."""
+    r = subprocess.run([programs["example2_sequence"], "3", "4", "timeout"], capture_output=True, text=True,
+                       timeout=60)
+    assert r.returncode == 0, r.stderr
+    out = json.loads(r.stdout.strip().splitlines()[-1])
+    assert out["status"] == 1
+    assert "in time" in r.stderr or "too long" in r.stderr
