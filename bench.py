@@ -7,8 +7,10 @@ Headline workload (the default, a step = one simulated frame of the whole batch)
       60 recorded plain frames of the batch (seeds 0..59; 150k Adam steps).
       Two forms, each iterated to the SAME fixed relative residual
       r = ||grad G(x)|| / ||grad G(y)|| <= --tol (1e-4) with an iteration cap
-      (--cap 200), probes every --check-every (10) iterations, converged instances
-      skipped:
+      (--cap 200), converged instances skipped; residual probes on the extrapolated
+      schedule (--probe-policy 1: the first two after 10 and 20 iterations
+      (--check-every), then after half the iterations the residual's contraction
+      predicts are still needed, or at the cap when it stalls):
         learned  predict, the network's guess (potential fallback per instance), VBD;
         plain    predict, VBD (the reference's method, batched).
       Both run from the same frame-start state each frame (held-out wind seeds
@@ -66,9 +68,9 @@ METRIC = "frames/s to 1e-4 residual: batched+learned VBD vs plain CUDA VBD, 1 B2
 UNIT = "frames/s"
 WORKLOADS = {
     "c4": "c4: 64 batched grid cloths, side U{{64..512}}, wind per instance; batched+learned vs plain batched VBD, "
-          "both iterated to a relative residual of {tol:g} (cap {cap} iterations, probes every {check})",
+          "both iterated to a relative residual of {tol:g} (cap {cap} iterations, probes from every {check})",
     "c3": "c3: 128x128 grid cloth, wind per frame; learned vs plain VBD, both iterated to a relative residual of "
-          "{tol:g} (cap {cap} iterations, probes every {check})",
+          "{tol:g} (cap {cap} iterations, probes from every {check})",
     "c1": "c1: 512x512 grid cloth, plain VBD, 50 iterations x 4 colours per frame",
     "c2": "c2: 256 batched grid cloths, side U{16..256}, plain VBD, 50 iterations per frame",
 }
@@ -88,6 +90,8 @@ def parse():
     p.add_argument("--tol", type=float, default=1e-4)
     p.add_argument("--cap", type=int, default=200)
     p.add_argument("--check-every", type=int, default=10)
+    p.add_argument("--probe-policy", type=int, default=1, choices=[0, 1],
+                   help="residual probes: 0 every check-every iterations, 1 extrapolated from the contraction")
     p.add_argument("--train-steps", type=int, default=150000)
     p.add_argument("--instances", type=int, default=0, help="only the first N instances (a small case for profiling)")
     p.add_argument("--record-frames", type=int, default=30, help="recorded frames per trajectory (c4)")
@@ -190,7 +194,7 @@ def c4_cpu_sample():
     return insts[0], prm, sum(i.num_verts for i in insts)
 
 
-def cpu_to_tolerance_frames(threads, frames, tol, cap, check_every, approach=2):
+def cpu_to_tolerance_frames(threads, frames, tol, cap, check_every, policy, approach=2):
     """Seconds per frame of the oracle's plain VBD frame iterated to `tol` (cap
     iterations, probes every check_every) on the c4 sample, after `approach` plain
     50-iteration frames from rest; winds as instance 0 of the GPU run's frames."""
@@ -209,7 +213,7 @@ def cpu_to_tolerance_frames(threads, frames, tol, cap, check_every, approach=2):
     for f in range(frames):
         s.set_gravity(configs.wind_accel(np.random.RandomState(10010 + f), total))
         t = time.perf_counter()
-        it, r = s.frame_to_residual(tol, check_every=check_every, max_iterations=cap)
+        it, r = s.frame_to_residual(tol, check_every=check_every, max_iterations=cap, policy=policy)
         times.append(time.perf_counter() - t)
         iters.append(it)
         res.append(r)
@@ -250,19 +254,21 @@ def run_reference(args):
             print(json.dumps({"impl": "reference", "unavailable": "c3 reference arm not provided; use c4"}))
             return
         t_all, it_all, r_all = cpu_to_tolerance_frames(threads, args.warmup + args.steps, args.tol, args.cap,
-                                                       args.check_every)
+                                                       args.check_every, args.probe_policy)
         t_all = t_all[args.warmup:]
-        t_one, _, _ = cpu_to_tolerance_frames(1, 5, args.tol, args.cap, args.check_every)
+        t_one, _, _ = cpu_to_tolerance_frames(1, 5, args.tol, args.cap, args.check_every, args.probe_policy)
         inst, _, total_v = c4_cpu_sample()
         scale = total_v / inst.num_verts
         per_frame = float(np.median(t_all)) * scale
         one = float(np.median(t_one)) * scale
         sample = (f"one frame of c4 instance 0 ({inst.num_verts} of {total_v} vertices) per step, plain VBD to "
-                  f"{args.tol:g} (cap {args.cap}, probes every {args.check_every}), scaled by vertex count; "
+                  f"{args.tol:g} (cap {args.cap}, probe policy {args.probe_policy}, check every {args.check_every}), "
+                  f"scaled by vertex count; "
                   f"reached tol in {float(np.mean(r_all <= args.tol)):.2f} of frames, mean iterations "
                   f"{float(np.mean(it_all)):.0f}")
         config = {"workload": WORKLOADS["c4"].format(tol=args.tol, cap=args.cap, check=args.check_every),
-                  "vertices": total_v, "tol": args.tol, "cap": args.cap, "check_every": args.check_every}
+                  "vertices": total_v, "tol": args.tol, "cap": args.cap, "check_every": args.check_every,
+                  "probe_policy": args.probe_policy}
         metric = METRIC
     else:
         t_all, nv_s, nv_t = cpu_plain_fixed_frames(threads, args.warmup + args.steps, wl)
@@ -403,6 +409,7 @@ def run_learned(args):
     cloth = ats.Cloth(insts, **prm)
     t_create = time.perf_counter() - t0
     tuned = cloth.autotune(iterations=20, stream=stream)
+    cloth.set_probe_policy(args.probe_policy)
     info = cloth.info
     nv = info.num_verts
     # training data: plain frames of this rank's instances
@@ -501,6 +508,7 @@ def run_learned(args):
                           "instances": len(all_insts), "vertices": sum(i.num_verts for i in all_insts),
                           "recorded_frames": traj * frames,
                           "tol": args.tol, "cap": args.cap, "check_every": args.check_every,
+                          "probe_policy": ["fixed", "extrapolated"][args.probe_policy],
                           "parallelism": f"instance-shards{world}", "create_s": t_create,
                           "threads_per_vertex": info.threads_per_vertex, "block_size": info.block_size,
                           "autotuned": list(tuned),
@@ -544,7 +552,8 @@ def run_learned(args):
             out["extras"] = extras
     if rank == 0 and world == 1 and not args.no_cpu_baseline and wl == "c4":
         threads = os.cpu_count() or 1
-        t_cpu, it_cpu, r_cpu = cpu_to_tolerance_frames(threads, 3, args.tol, args.cap, args.check_every)
+        t_cpu, it_cpu, r_cpu = cpu_to_tolerance_frames(threads, 3, args.tol, args.cap, args.check_every,
+                                                       args.probe_policy)
         inst0, _, total_v = c4_cpu_sample()
         per_frame = float(np.median(t_cpu)) * total_v / inst0.num_verts
         out["cpu_baseline"] = {"value": 1.0 / per_frame, "unit": UNIT, "cores": threads, "kind": "port",

@@ -212,6 +212,17 @@ int ats_frame_to_residual(ats_cloth* cloth, double tol, int check_every, int max
 int ats_frame_to_residuals(ats_cloth* cloth, const double* tols, const int* first_check, int check_every,
                            int max_iterations, int* iterations, double* residual, ats_stream stream);
 
+/* Probe schedule of the residual-driven frames of this handle (ats_frame_to_residual(s),
+ * ats_frame_warm_to_residual). 0 (default): every check_every iterations after an
+ * instance's first probe, and at max_iterations. 1 (extrapolated): the first two probes
+ * as policy 0; after that, from the residual's contraction per iteration between the
+ * last two probes, the next probe comes after half of the iterations still predicted
+ * to reach the tolerance (at least check_every, rounded up to a multiple of it), or at
+ * max_iterations when the residual did not fall. Probes then follow the distance to the
+ * tolerance instead of a fixed period; an instance can stop up to that gap after it
+ * crossed the tolerance. The reference has no residual-driven frames. */
+int ats_set_probe_policy(ats_cloth* cloth, int policy);
+
 /* Times `iterations` VBD iterations (three times, taking the fastest) for every
  * lanes-per-vertex (1, 2, 4, 8) and block size (64, 128, 256) on this handle's own
  * mesh, keeps the fastest and

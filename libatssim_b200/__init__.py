@@ -140,6 +140,7 @@ _SIGNATURES = {
                                    _dp, _ip, _vp],
     "ats_frame_to_residuals": [_vp, _dp, _ip, ctypes.c_int, ctypes.c_int, _ip, _dp, _vp],
     "ats_kernel_launches": [ctypes.POINTER(ctypes.c_longlong)],
+    "ats_set_probe_policy": [_vp, ctypes.c_int],
     "ats_energy_noalloc": [_vp, _vp, _vp, _vp, _vp, ctypes.c_int, _vp, _vp, ctypes.c_int, _vp, _vp, ctypes.c_int,
                            ctypes.c_float, ctypes.c_float, _fp, ctypes.c_float, _vp, _vp],
 }
@@ -470,6 +471,11 @@ class Cloth:
 
     def record_end(self, dataset, stream=None):
         _check(lib().ats_record_frame_end(self.h, dataset.h, _stream(stream)))
+
+    def set_probe_policy(self, policy):
+        """Probe schedule of the residual-driven frames: 0 fixed period, 1 extrapolated
+        from the residual's contraction (ats_set_probe_policy)."""
+        _check(lib().ats_set_probe_policy(self.h, int(policy)))
 
     def frame_to_residual(self, tol, check_every=10, max_iterations=1000, first_check=None, stream=None):
         """One frame iterated until every instance reaches ||grad G|| <= tol ||grad G(y)||

@@ -748,23 +748,28 @@ __global__ void __launch_bounds__(kSegChunks) segment_final_kernel(const double*
     if (threadIdx.x == 0) out[blockIdx.x] = take_sqrt ? sqrt(s) : s;
 }
 
-// Residual bookkeeping of ats_frame_to_residual, one block: the first call after
-// predict stores ||grad G(y)|| per instance; later calls deactivate an instance once
-// ||grad G(x)|| <= tol ||grad G(y)|| or its iteration cap is reached; n_active
-// receives the number of instances still iterating.
 // Bookkeeping of the residual-driven frame (one block). The probe schedule lives on the
 // device, so that the same captured chunk graph serves every probe point: pts[0..n-1]
-// are the iteration counts at which probes run and pts[n] = max_iters; *pidx is the
+// are the iteration counts at which probes may run and pts[n] = max_iters; *pidx is the
 // index of the probe point just reached (advanced here, once per call).
 // init: norm0 = ||grad G(y)||, every instance with a nonzero gradient active, *pidx = 0.
 // Otherwise, after done = pts[*pidx] iterations: every active instance has iters = done;
 // an instance probed now (due) stops when ||grad G|| <= tols[i] ||grad G(y)|| or
-// done >= max_iters. Then due is set for the next point `next`: active instances with
-// next == max_iters, or next >= first[i] and (next - first[i]) a multiple of step.
+// done >= max_iters. Then due is set for the next point `next`, by the probe policy:
+//   0 (fixed)        next == max_iters, or next >= first[i] and (next - first[i]) a
+//                    multiple of step;
+//   1 (extrapolated) next == max_iters, or next >= next_due[i]. After the first probe
+//                    next_due = that point + step; after later ones the contraction per
+//                    iteration since the previous probe, rho, predicts the iterations
+//                    still needed, log(tol / r) / log(rho), and the next probe comes after
+//                    half of them (at least step, rounded up to a multiple of it); without
+//                    progress (rho >= 1) it comes at the cap. A flat residual curve is
+//                    then probed a few times per frame instead of every step.
 __global__ void __launch_bounds__(256) residual_check_kernel(const double* norm, double* norm0, int* active, int* iters,
                                                             int* n_active, int* due, int ninst, int init,
                                                             const int* pts, int* pidx, int step, const int* first,
-                                                            int max_iters, const double* tols) {
+                                                            int max_iters, const double* tols, int policy,
+                                                            int* next_due, int* last_it, double* last_res) {
     __shared__ int count[256];
     const int p = init ? 0 : *pidx;
     const int done = init ? 0 : pts[p];
@@ -775,12 +780,37 @@ __global__ void __launch_bounds__(256) residual_check_kernel(const double* norm,
             norm0[i] = norm[i];
             active[i] = norm[i] > 0.0 && max_iters > 0 ? 1 : 0;
             iters[i] = 0;
+            next_due[i] = first[i];
+            last_it[i] = 0;
+            last_res[i] = 1.0;
         } else if (active[i]) {
             iters[i] = done;
-            if (due[i] && (norm[i] <= tols[i] * norm0[i] || done >= max_iters)) active[i] = 0;
+            if (due[i]) {
+                const double r = norm0[i] > 0.0 ? norm[i] / norm0[i] : 0.0;
+                if (norm[i] <= tols[i] * norm0[i] || done >= max_iters) {
+                    active[i] = 0;
+                } else if (policy == 1) {
+                    int gap = step;
+                    if (last_it[i] > 0) {
+                        gap = max_iters - done;
+                        if (r < last_res[i] && r > 0.0 && tols[i] > 0.0) {
+                            const double rho = pow(r / last_res[i], 1.0 / (double)(done - last_it[i]));
+                            const double need = log(tols[i] / r) / log(rho);  // > 0: r > tol, rho < 1
+                            if (need < (double)(max_iters - done)) {
+                                const int half = (int)ceil(0.5 * need);
+                                gap = ((max(half, step) + step - 1) / step) * step;
+                            }
+                        }
+                    }
+                    next_due[i] = min(done + gap, max_iters);
+                    last_it[i] = done;
+                    last_res[i] = r;
+                }
+            }
         }
         const int f = first[i];
-        due[i] = active[i] && (next >= max_iters || (next >= f && (next - f) % step == 0)) ? 1 : 0;
+        const bool sched = policy == 1 ? next >= next_due[i] : (next >= f && (next - f) % step == 0);
+        due[i] = active[i] && (next >= max_iters || sched) ? 1 : 0;
         c += active[i];
     }
     count[threadIdx.x] = c;
@@ -1244,7 +1274,8 @@ int enqueue_potential(ats_cloth* c, double* g, cudaStream_t st) {
 // tolerances and first probes are read from device memory), so a dozen graphs serve
 // every frame; they are dropped with the frame graphs (ats_autotune).
 int piece_graph(ats_cloth* c, int k, int step, int max_iterations, cudaGraphExec_t* out) {
-    const auto key = std::make_tuple(k, step, max_iterations);
+    const int policy = k > 0 ? 0 : c->probe_policy;  // baked into the probe pieces
+    const auto key = std::make_tuple(k, step, max_iterations, policy);
     auto it = c->chunk_graphs.find(key);
     if (it != c->chunk_graphs.end()) {
         *out = it->second;
@@ -1262,7 +1293,8 @@ int piece_graph(ats_cloth* c, int k, int step, int max_iterations, cudaGraphExec
             residual_check_kernel<<<1, 256, 0, cs>>>(c->red_out.p, c->norm0.p, c->active.p, c->iters.p,
                                                       c->n_active.p, c->due.p, c->L.ninst, 0, c->probe_points.p,
                                                       c->probe_idx.p, step, c->first_check.p, max_iterations,
-                                                      c->tols.p); count_launch(cs);
+                                                      c->tols.p, policy, c->next_due.p, c->last_it.p,
+                                                      c->last_res.p); count_launch(cs);
             if (cudaGetLastError() != cudaSuccess) r = ATS_ERR_CUDA;
             if (!r) r = enqueue_compaction(c, cs);
         }
@@ -1314,6 +1346,9 @@ int frame_to_residual_impl(ats_cloth* c, double tol, const double* tols, const i
     if (!c->tols.p) ATS_CUDA(c->tols.alloc(ni));
     if (!c->due.p) ATS_CUDA(c->due.alloc(ni));
     if (!c->first_check.p) ATS_CUDA(c->first_check.alloc(ni));
+    if (!c->next_due.p) ATS_CUDA(c->next_due.alloc(ni));
+    if (!c->last_it.p) ATS_CUDA(c->last_it.alloc(ni));
+    if (!c->last_res.p) ATS_CUDA(c->last_res.alloc(ni));
     if (!c->probe_idx.p) ATS_CUDA(c->probe_idx.alloc(1));
     std::vector<double> tv(ni);
     std::vector<int> fv(ni);
@@ -1354,7 +1389,8 @@ int frame_to_residual_impl(ats_cloth* c, double tol, const double* tols, const i
         if (after_predict && (r = after_predict(st))) return r;
         residual_check_kernel<<<1, 256, 0, st>>>(c->red_out.p, c->norm0.p, c->active.p, c->iters.p, c->n_active.p,
                                                   c->due.p, ni, 1, c->probe_points.p, c->probe_idx.p, check_every,
-                                                  c->first_check.p, max_iterations, c->tols.p); count_launch(st);
+                                                  c->first_check.p, max_iterations, c->tols.p, c->probe_policy,
+                                                  c->next_due.p, c->last_it.p, c->last_res.p); count_launch(st);
         ATS_CUDA(cudaGetLastError());
         if ((r = enqueue_compaction(c, st))) return r;
         list_sweep_ctas(c->L.tpv, c->block);  // occupancy query before any capture
@@ -1397,6 +1433,15 @@ int frame_to_residual_impl(ats_cloth* c, double tol, const double* tols, const i
 extern "C" {
 
 const char* ats_last_error(void) { return g_last_error.c_str(); }
+
+int ats_set_probe_policy(ats_cloth* c, int policy) {
+    if (!c || (policy != 0 && policy != 1)) {
+        set_error("ats_set_probe_policy: need a handle and policy 0 (fixed) or 1 (extrapolated)");
+        return ATS_ERR_INVALID;
+    }
+    c->probe_policy = policy;
+    return ATS_OK;
+}
 
 int ats_kernel_launches(long long* count) {
     if (!count) {

@@ -88,8 +88,11 @@ struct ats_cloth {
     // scratch of the FP64 reductions
     DevBuf<double> partial, seg_partial, red_out, g2, norm0, tols;
     DevBuf<int> active, iters, n_active, due, first_check;  // ats_frame_to_residual bookkeeping
+    DevBuf<int> next_due, last_it;                          // its extrapolated probe schedule
+    DevBuf<double> last_res;
+    int probe_policy = 0;                                   // 0 fixed, 1 extrapolated (ats_set_probe_policy)
     DevBuf<int> probe_points, probe_idx;                     // its probe schedule, on the device
-    std::map<std::tuple<int, int, int>, cudaGraphExec_t> chunk_graphs;  // residual-frame pieces
+    std::map<std::tuple<int, int, int, int>, cudaGraphExec_t> chunk_graphs;  // residual-frame pieces
     int* host_flag = nullptr;             // pinned copy of n_active
     // learned warm start (uploaded at create; the rest allocated on first use)
     DevBuf<int> feat_nb, inst_eseg, inst_bseg, free_list;

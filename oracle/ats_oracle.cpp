@@ -885,11 +885,15 @@ void ato_frame(void* h, int solver, double* energy_log, int with_bending, double
 // residual-driven frame (the reference defines no residual; it is the norm of the
 // incremental-potential gradient over free vertices, relative to its value at the
 // inertial prediction y). Per substep: predict; r0 = ||grad G(y)||; VBD iterations
-// (example2:1481-1509), probed after every check_every iterations and at
-// max_iterations; the substep stops once ||grad G(x)|| <= tol * r0 (or at once when
-// r0 == 0); then the velocity update. Returns the iterations of the last substep;
-// *rel_out (nullable) receives its last probed relative residual.
-int ato_frame_to_residual(void* h, double tol, int check_every, int max_iterations, double* rel_out) {
+// (example2:1481-1509) with probes; the substep stops once ||grad G(x)|| <= tol * r0 (or
+// at once when r0 == 0) or at max_iterations; then the velocity update. Probes:
+// policy 0 after every check_every iterations and at max_iterations; policy 1 (the
+// GPU's extrapolated schedule) the first two as policy 0, then after half of the
+// iterations that the contraction per iteration between the last two probes predicts
+// are still needed (at least check_every, rounded up to a multiple of it), or at
+// max_iterations when the residual did not fall. Returns the iterations of the last
+// substep; *rel_out (nullable) receives its last probed relative residual.
+int ato_frame_to_residual(void* h, double tol, int check_every, int max_iterations, int policy, double* rel_out) {
     Scene* s = (Scene*)h;
     s->x_frame_start = s->x_frame_end;
     s->v_frame_start = s->v_frame_end;
@@ -905,14 +909,30 @@ int ato_frame_to_residual(void* h, double tol, int check_every, int max_iteratio
         const double r0 = grad_norm_pool(*s, s->x);
         used = 0;
         rel = r0 > 0.0 ? 1.0 : 0.0;
-        if (r0 > 0.0) {
-            while (used < max_iterations) {
-                const int chunk = std::min(check_every, max_iterations - used);
-                for (int it = 0; it < chunk; ++it)
-                    for (uint c = 0; c < s->vert_colors.size(); ++c) vbd_color(*s, c);
-                used += chunk;
-                rel = grad_norm_pool(*s, s->x) / r0;
-                if (rel <= tol) break;
+        int next_due = check_every, last_it = 0;
+        double last_res = 1.0;
+        while (r0 > 0.0 && used < max_iterations) {
+            const int target = std::min(policy == 1 ? next_due : used + check_every, max_iterations);
+            for (; used < target; ++used)
+                for (uint c = 0; c < s->vert_colors.size(); ++c) vbd_color(*s, c);
+            rel = grad_norm_pool(*s, s->x) / r0;
+            if (rel <= tol || used >= max_iterations) break;
+            if (policy == 1) {
+                int gap = check_every;
+                if (last_it > 0) {
+                    gap = max_iterations - used;
+                    if (rel < last_res && rel > 0.0 && tol > 0.0) {
+                        const double rho = std::pow(rel / last_res, 1.0 / (double)(used - last_it));
+                        const double need = std::log(tol / rel) / std::log(rho);
+                        if (need < (double)(max_iterations - used)) {
+                            const int half = (int)std::ceil(0.5 * need);
+                            gap = ((std::max(half, check_every) + check_every - 1) / check_every) * check_every;
+                        }
+                    }
+                }
+                next_due = std::min(used + gap, max_iterations);
+                last_it = used;
+                last_res = rel;
             }
         }
         update_velocity(*s);

@@ -62,7 +62,7 @@ def lib():
         L.ato_set_gravity.argtypes = [P, ctypes.c_float, ctypes.c_float, ctypes.c_float]
         L.ato_frame.argtypes = [P, ctypes.c_int, dp, ctypes.c_int, dp]
         L.ato_run_frames.argtypes = [P, ctypes.c_int, ctypes.c_int]
-        L.ato_frame_to_residual.argtypes = [P, ctypes.c_double, ctypes.c_int, ctypes.c_int, dp]
+        L.ato_frame_to_residual.argtypes = [P, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp]
         L.ato_frame_to_residual.restype = ctypes.c_int
         L.ato_energy_of.argtypes = [P, fp, ctypes.c_int]
         L.ato_energy_of.restype = ctypes.c_double
@@ -181,11 +181,13 @@ class Scene:
                         _p(r, ctypes.c_double) if r is not None else None)
         return e, r
 
-    def frame_to_residual(self, tol, check_every=10, max_iterations=1000):
+    def frame_to_residual(self, tol, check_every=10, max_iterations=1000, policy=0):
         """One VBD frame iterated until ||grad G(x)|| <= tol ||grad G(y)||, probed every
-        check_every iterations and at max_iterations -> (iterations, relative residual)."""
+        check_every iterations (policy 0) or on the extrapolated schedule (policy 1), and
+        at max_iterations -> (iterations, relative residual)."""
         r = ctypes.c_double(0.0)
-        it = lib().ato_frame_to_residual(self.h, float(tol), int(check_every), int(max_iterations), ctypes.byref(r))
+        it = lib().ato_frame_to_residual(self.h, float(tol), int(check_every), int(max_iterations), int(policy),
+                                         ctypes.byref(r))
         return int(it), float(r.value)
 
     def run(self, frames, solver="vbd"):

@@ -99,3 +99,23 @@ def test_residual_structure_of_a_hanging_cloth(oracle):
     # most of it, the largest 10 only a few percent
     top = np.sort(g1)[::-1] / g1.sum()
     assert top[:10].sum() < 0.1 and top[:1000].sum() > 0.8, (top[:10].sum(), top[:1000].sum())
+
+
+def test_extrapolated_probe_schedule(oracle):
+    """Policy 1 probes after 4 and 8 iterations, then by the residual's contraction: a
+    loose tolerance stops as with the fixed schedule's first probes; an unreachable one
+    runs to the cap either way with the same positions (probes never change the
+    iterate)."""
+    inst, s = _scene(oracle)
+    s.frame()
+    x, v = s.state()
+    out = {}
+    for policy in (0, 1):
+        for tol in (10.0, 1e-9):
+            s.set_state(x, v)
+            it, r = s.frame_to_residual(tol, check_every=4, max_iterations=60, policy=policy)
+            out[(policy, tol)] = (it, r, s.state()[0])
+    assert out[(0, 10.0)][0] == out[(1, 10.0)][0] == 4
+    assert out[(0, 1e-9)][0] == out[(1, 1e-9)][0] == 60
+    assert np.array_equal(out[(0, 1e-9)][2], out[(1, 1e-9)][2])
+    assert out[(0, 1e-9)][1] == out[(1, 1e-9)][1]

@@ -171,17 +171,20 @@ def test_wind_per_instance_batched(ats, oracle):
     cloth.close()
 
 
-def test_frame_to_residual_matches_oracle(ats, oracle):
+@pytest.mark.parametrize("policy", [0, 1])
+def test_frame_to_residual_matches_oracle(ats, oracle, policy):
     """The residual-driven frame: the same stopping iteration as the oracle's
-    to-residual frame (probes every 5 iterations) and the same positions."""
+    to-residual frame (probes every 5 iterations, or the extrapolated schedule) and the
+    same positions."""
     inst = configs.grid_instance(48)
     prm = dict(implicit_dt=1.0 / 60.0, num_substep=1, iterations=50, damping=2.0)
     cloth = ats.Cloth([inst], **prm)
+    cloth.set_probe_policy(policy)
     s = scene(oracle, inst, prm)
     agree = 0
     for f in range(12):
         it_g, r_g = cloth.frame_to_residual(0.3, check_every=5, max_iterations=200)
-        it_o, r_o = s.frame_to_residual(0.3, check_every=5, max_iterations=200)
+        it_o, r_o = s.frame_to_residual(0.3, check_every=5, max_iterations=200, policy=policy)
         # the probes sum FP32 force terms in FP64, the oracle is FP64 throughout: near
         # the threshold they may stop one probe apart
         assert abs(int(it_g[0]) - it_o) <= 5, (f, it_g, it_o)
