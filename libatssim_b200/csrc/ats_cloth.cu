@@ -101,18 +101,6 @@ __global__ void update_kernel(const float4* __restrict__ x, float4* __restrict__
     x0[i] = make_float4(p.x, p.y, p.z, q.w);
 }
 
-// Position access of the XPBD bodies: plain loads / stores in the per-colour kernels
-// (each launch starts with a clean L1), L2-only ones in the persistent kernel, whose
-// blocks read vertices that other SMs wrote since the last grid barrier.
-struct PlainMem {
-    static __device__ __forceinline__ float4 ld(const float4* p) { return *p; }
-    static __device__ __forceinline__ void st(float4* p, float4 v) { *p = v; }
-};
-struct L2Mem {
-    static __device__ __forceinline__ float4 ld(const float4* p) { return __ldcg(p); }
-    static __device__ __forceinline__ void st(float4* p, float4 v) { __stcg(p, v); }
-};
-
 // The constant data of one stretch constraint: vertex ids, rest length, stiffness and
 // the endpoints' inverse masses.
 struct StretchConst {
@@ -291,6 +279,25 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, int* err, unsigned n
 }
 
 constexpr int kXpbdLoopThreads = 640;  // one block per SM, up to 96 registers a thread
+
+// `iterations` VBD iterations of every instance in one cooperative launch: each colour
+// is a grid-stride loop of warps over the colour's slices (sweep_slice, the body of
+// the list sweep, with L2-only position access), colours are separated by
+// grid_barrier. The same per-vertex arithmetic as the one-wave and list sweeps, so the
+// same positions. The autotuner keeps it only where it measures faster.
+template <int TPV, int RE, int RB>
+__global__ void __launch_bounds__(256) vbd_loop_kernel(SweepArgs a, const int* __restrict__ color_slices, int ncolors,
+                                                       int iterations, unsigned* bar, int* err) {
+    const int lane = threadIdx.x & 31;
+    const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
+    const int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    for (int it = 0; it < iterations; ++it)
+        for (int c = 0; c < ncolors; ++c) {
+            const int b = __ldg(&color_slices[c]), e = __ldg(&color_slices[c + 1]);
+            for (int slice = b + w; slice < e; slice += nwarps) sweep_slice<TPV, RE, RB, L2Mem>(a, slice, lane);
+            if (!grid_barrier(bar, err, gridDim.x)) return;
+        }
+}
 
 struct XpbdLoopArgs {
     float4* x;
@@ -1079,8 +1086,73 @@ int launch_xpbd_loop(ats_cloth* c, int iterations, cudaStream_t st) {
     return ATS_OK;
 }
 
+// Co-resident blocks of vbd_loop_kernel at (lanes per vertex, block size), all SMs,
+// queried outside any capture (at autotune time); 0 when cooperative launch is
+// unavailable.
+int vbd_loop_blocks(int tpv, int block, int device) {
+    int coop = 0, sms = 0, per_sm = 0;
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    cudaError_t e;
+    switch (tpv) {
+        case 1: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, vbd_loop_kernel<1, 6, 6>, block, 0); break;
+        case 2: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, vbd_loop_kernel<2, 3, 3>, block, 0); break;
+        case 4: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, vbd_loop_kernel<4, 2, 2>, block, 0); break;
+        default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, vbd_loop_kernel<8, 1, 1>, block, 0); break;
+    }
+    return coop && e == cudaSuccess && per_sm > 0 ? sms * per_sm : 0;
+}
+
+int launch_vbd_loop(ats_cloth* c, int iterations, cudaStream_t st) {
+    SweepArgs a;
+    a.x = c->x.p;
+    a.x0 = c->x0.p;
+    a.vel = c->vel.p;
+    a.vm = c->vm.p;
+    a.st_iw = c->st_iw.p;
+    a.st_rest = c->st_rest.p;
+    a.slices = c->slices.p;
+    a.slice_inst = c->slice_inst.p;
+    a.inst = c->inst.p;
+    a.active = nullptr;
+    a.list = nullptr;
+    a.list_count = nullptr;
+    a.slice_begin = 0;
+    a.slice_end = (int)c->slices.n;
+    a.h = c->h;
+    a.h2inv = c->h2inv;
+    ATS_CUDA(cudaMemsetAsync(c->loop_bar.p, 0, 2 * sizeof(unsigned), st));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(c->vbd_loop_blocks);
+    cfg.blockDim = dim3(c->block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const int* cs = c->color_slices.p;
+    const int nc = c->L.n_vcolors;
+    cudaError_t e;
+    switch (c->L.tpv) {
+        case 1: e = cudaLaunchKernelEx(&cfg, vbd_loop_kernel<1, 6, 6>, a, cs, nc, iterations, c->loop_bar.p, c->loop_err.p); break;
+        case 2: e = cudaLaunchKernelEx(&cfg, vbd_loop_kernel<2, 3, 3>, a, cs, nc, iterations, c->loop_bar.p, c->loop_err.p); break;
+        case 4: e = cudaLaunchKernelEx(&cfg, vbd_loop_kernel<4, 2, 2>, a, cs, nc, iterations, c->loop_bar.p, c->loop_err.p); break;
+        default: e = cudaLaunchKernelEx(&cfg, vbd_loop_kernel<8, 1, 1>, a, cs, nc, iterations, c->loop_bar.p, c->loop_err.p); break;
+    }
+    if (e != cudaSuccess) {
+        set_error(std::string("vbd loop launch: ") + cudaGetErrorString(e));
+        return ATS_ERR_CUDA;
+    }
+    count_launch(st);
+    return ATS_OK;
+}
+
 int enqueue_iterations(ats_cloth* c, int solver, int iterations, cudaStream_t st, const int* active) {
     int r;
+    if (solver == ATS_SOLVER_VBD && !active && c->vbd_loop_blocks > 0 && iterations > 0 && c->L.n_vcolors > 0)
+        return launch_vbd_loop(c, iterations, st);
     if (solver == ATS_SOLVER_XPBD && c->xpbd_loop_blocks > 0 && iterations > 0 &&
         c->L.n_scolors + c->L.n_bcolors > 0)
         return launch_xpbd_loop(c, iterations, st);
@@ -1433,6 +1505,21 @@ int frame_to_residual_impl(ats_cloth* c, double tol, const double* tols, const i
 extern "C" {
 
 const char* ats_last_error(void) { return g_last_error.c_str(); }
+
+int ats_set_sweep_form(ats_cloth* c, int form) {
+    if (!c || (form != 0 && form != 1)) {
+        set_error("ats_set_sweep_form: need a handle and form 0 (a launch per colour) or 1 (persistent)");
+        return ATS_ERR_INVALID;
+    }
+    int blocks = 0;
+    if (form == 1 && (blocks = vbd_loop_blocks(c->L.tpv, c->block, c->device)) == 0) {
+        set_error("ats_set_sweep_form: the device cannot run the persistent sweep cooperatively");
+        return ATS_ERR_INVALID;
+    }
+    c->vbd_loop_blocks = blocks;
+    c->drop_graphs();  // captured frames hold the other form
+    return ATS_OK;
+}
 
 int ats_set_probe_policy(ats_cloth* c, int policy) {
     if (!c || (policy != 0 && policy != 1)) {
@@ -1828,6 +1915,27 @@ int ats_autotune(ats_cloth* c, int iterations, ats_stream stream, int* out_tpv, 
     int best_tpv = c->L.tpv, best_block = c->block;
     std::string err;
     int r = ATS_OK;
+    c->vbd_loop_blocks = 0;  // the one-wave launches first
+    // the fastest of three timings of `iterations` iterations (short runs are noisy)
+    auto time_iterations = [&](float& ms) -> int {
+        int rr;
+        if ((rr = enqueue_iterations(c, ATS_SOLVER_VBD, 1, st))) return rr;  // warm-up
+        ms = 1e30f;
+        for (int rep = 0; rep < 3; ++rep) {
+            cudaEventRecord(e0, st);
+            if ((rr = enqueue_iterations(c, ATS_SOLVER_VBD, iterations, st))) return rr;
+            cudaEventRecord(e1, st);
+            cudaError_t ce = cudaEventSynchronize(e1);
+            if (ce != cudaSuccess) {
+                set_error(std::string("ats_autotune: ") + cudaGetErrorString(ce));
+                return ATS_ERR_CUDA;
+            }
+            float t = 0.f;
+            cudaEventElapsedTime(&t, e0, e1);
+            ms = std::min(ms, t);
+        }
+        return ATS_OK;
+    };
     for (int tpv : tpvs) {
         if (!build_slices(c->L, tpv, err) || (r = upload_stencil(c))) {
             if (!r) {
@@ -1838,24 +1946,8 @@ int ats_autotune(ats_cloth* c, int iterations, ats_stream stream, int* out_tpv, 
         }
         for (int b : blocks) {
             c->block = b;
-            if ((r = enqueue_iterations(c, ATS_SOLVER_VBD, 1, st))) break;  // warm-up
-            // the fastest of three timings (short runs are noisy)
             float ms = 1e30f;
-            for (int rep = 0; rep < 3 && !r; ++rep) {
-                cudaEventRecord(e0, st);
-                if ((r = enqueue_iterations(c, ATS_SOLVER_VBD, iterations, st))) break;
-                cudaEventRecord(e1, st);
-                cudaError_t ce = cudaEventSynchronize(e1);
-                if (ce != cudaSuccess) {
-                    set_error(std::string("ats_autotune: ") + cudaGetErrorString(ce));
-                    r = ATS_ERR_CUDA;
-                    break;
-                }
-                float t = 0.f;
-                cudaEventElapsedTime(&t, e0, e1);
-                ms = std::min(ms, t);
-            }
-            if (r) break;
+            if ((r = time_iterations(ms))) break;
             if (ms < best) {
                 best = ms;
                 best_tpv = tpv;
@@ -1864,8 +1956,6 @@ int ats_autotune(ats_cloth* c, int iterations, ats_stream stream, int* out_tpv, 
         }
         if (r) break;
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     if (!r && (!build_slices(c->L, best_tpv, err) || (r = upload_stencil(c)))) {
         if (!r) {
             set_error("ats_autotune: " + err);
@@ -1873,6 +1963,18 @@ int ats_autotune(ats_cloth* c, int iterations, ats_stream stream, int* out_tpv, 
         }
     }
     c->block = best_block;
+    // then the persistent form at the chosen shape: kept where it is faster
+    if (!r) {
+        const int loop_blocks = vbd_loop_blocks(c->L.tpv, c->block, c->device);
+        if (loop_blocks > 0) {
+            c->vbd_loop_blocks = loop_blocks;
+            float ms = 1e30f;
+            r = time_iterations(ms);
+            if (r || ms >= best) c->vbd_loop_blocks = 0;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
     c->prm.threads_per_vertex = c->L.tpv;
     c->prm.block_size = best_block;
     c->drop_graphs();

@@ -78,6 +78,7 @@ struct ats_cloth {
     DevBuf<unsigned> loop_bar;           // its grid barrier: arrivals, generation
     DevBuf<int> loop_err;                // set when a barrier wait ran out
     int xpbd_loop_blocks = 0;            // co-resident blocks of the persistent kernel (0: per-colour launches)
+    int vbd_loop_blocks = 0;             // the same for VBD iterations (0: one launch per colour; set by autotune)
     DevBuf<int2> en_edge;
     DevBuf<float> en_rest, en_k, en_q, en_kb;
     DevBuf<int4> en_bend;

@@ -25,6 +25,18 @@ namespace ats {
 
 constexpr float kEps = 1.19209290E-7f;  // src/SharedDefine/constant_value.h:9
 
+// Position access of the sweep and XPBD bodies: plain loads / stores in kernels that
+// end at each colour (a launch starts with a clean L1), L2-only ones in the persistent
+// kernels, whose blocks read vertices that other SMs wrote since the last grid barrier.
+struct PlainMem {
+    static __device__ __forceinline__ float4 ld(const float4* p) { return *p; }
+    static __device__ __forceinline__ void st(float4* p, float4 v) { *p = v; }
+};
+struct L2Mem {
+    static __device__ __forceinline__ float4 ld(const float4* p) { return __ldcg(p); }
+    static __device__ __forceinline__ void st(float4* p, float4 v) { __stcg(p, v); }
+};
+
 struct SweepArgs {
     float4* __restrict__ x;
     const float4* __restrict__ x0;
@@ -94,7 +106,7 @@ __device__ __forceinline__ void vbd_bend(float4 xv, float4 xu, float w, float& f
 // The per-vertex part of a sweep, shared by both sweep kernels: the RE + RB gathered
 // neighbours (rows beyond them go through loops), the lane reduction, inertia and the
 // guarded 3x3 solve; the leader lane of a vertex writes x.
-template <int TPV, int RE, int RB>
+template <int TPV, int RE, int RB, class M = PlainMem>
 __device__ __forceinline__ void sweep_vertex(const SweepArgs& a, int v, bool leader, int base, int bbase, int erows,
                                              int brows, float4 xv, const float4 (&xe)[RE], const float (&le)[RE],
                                              const float (&we)[RE], const float4 (&xb)[RB], const float (&wb)[RB],
@@ -105,14 +117,14 @@ __device__ __forceinline__ void sweep_vertex(const SweepArgs& a, int v, bool lea
     for (int r = 0; r < RE; ++r) vbd_edge(xv, xe[r], le[r], we[r], ks, fx, fy, fz, h00, h01, h02, h11, h12, h22);
     for (int r = RE; r < erows; ++r) {
         const int2 iw = __ldg(&a.st_iw[base + r * 32]);
-        vbd_edge(xv, a.x[iw.x], __ldg(&a.st_rest[base + r * 32]), __int_as_float(iw.y), ks, fx, fy, fz, h00, h01, h02,
+        vbd_edge(xv, M::ld(&a.x[iw.x]), __ldg(&a.st_rest[base + r * 32]), __int_as_float(iw.y), ks, fx, fy, fz, h00, h01, h02,
                  h11, h12, h22);
     }
 #pragma unroll
     for (int r = 0; r < RB; ++r) vbd_bend(xv, xb[r], wb[r], fx, fy, fz);
     for (int r = RB; r < brows; ++r) {
         const int2 iw = __ldg(&a.st_iw[bbase + r * 32]);
-        vbd_bend(xv, a.x[iw.x], __int_as_float(iw.y), fx, fy, fz);
+        vbd_bend(xv, M::ld(&a.x[iw.x]), __int_as_float(iw.y), fx, fy, fz);
     }
     // reduce the TPV lanes of a vertex
 #pragma unroll
@@ -154,7 +166,7 @@ __device__ __forceinline__ void sweep_vertex(const SweepArgs& a, int v, bool lea
         xn.x = fmaf(fmaf(c00, fx, fmaf(c01, fy, __fmul_rn(c02, fz))), id, xv.x);
         xn.y = fmaf(fmaf(c01, fx, fmaf(c11, fy, __fmul_rn(c12, fz))), id, xv.y);
         xn.z = fmaf(fmaf(c02, fx, fmaf(c12, fy, __fmul_rn(c22, fz))), id, xv.z);
-        a.x[v] = xn;
+        M::st(&a.x[v], xn);
     }
 }
 
@@ -250,6 +262,62 @@ __global__ void __launch_bounds__(256) vbd_sweep_kernel(SweepArgs a) {
 // listed per colour by the compaction after each probe (order within a colour does not
 // matter: its vertices are independent). A grid of resident size strides over the
 // list, so a converged instance costs nothing, not even a CTA launch.
+// One slice of a sweep: every vertex of the slice (its constant data, then all
+// neighbour positions at once, then the solve). M chooses how positions are accessed.
+template <int TPV, int RE, int RB, class M>
+__device__ __forceinline__ void sweep_slice(const SweepArgs& a, int slice, int lane) {
+    const int4 sd = __ldg(&a.slices[slice]);
+    const int rows = sd.w & 0xffff, erows = sd.w >> 16, brows = rows - erows;
+    const int k = lane / TPV;
+    const bool leader = k < sd.y && (lane % TPV) == 0;
+    const int v = sd.x + min(k, sd.y - 1);
+    const int base = sd.z + lane;
+    const int bbase = base + erows * 32;
+    int ue[RE], ub[RB];
+    float we[RE], le[RE], wb[RB];
+#pragma unroll
+    for (int r = 0; r < RE; ++r) {
+        ue[r] = v;
+        we[r] = 0.f;
+        le[r] = -1.f;
+        if (r < erows) {
+            const int2 iw = __ldg(&a.st_iw[base + r * 32]);
+            ue[r] = iw.x;
+            we[r] = __int_as_float(iw.y);
+            le[r] = __ldg(&a.st_rest[base + r * 32]);
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < RB; ++r) {
+        ub[r] = v;
+        wb[r] = 0.f;
+        if (r < brows) {
+            const int2 iw = __ldg(&a.st_iw[bbase + r * 32]);
+            ub[r] = iw.x;
+            wb[r] = __int_as_float(iw.y);
+        }
+    }
+    const float4 mv = __ldg(&a.vm[v]);
+    const float4 ip = __ldg(&a.inst[__float_as_int(mv.w)]);
+    const float4 xv = M::ld(&a.x[v]);
+    float4 xe[RE], xb[RB];
+#pragma unroll
+    for (int r = 0; r < RE; ++r) xe[r] = M::ld(&a.x[ue[r]]);
+#pragma unroll
+    for (int r = 0; r < RB; ++r) xb[r] = M::ld(&a.x[ub[r]]);
+    float4 p0 = make_float4(0.f, 0.f, 0.f, 0.f), vv = p0;
+    if (leader) {
+        p0 = a.x0[v];
+        vv = a.vel[v];
+    }
+    sweep_vertex<TPV, RE, RB, M>(a, v, leader, base, bbase, erows, brows, xv, xe, le, we, xb, wb, ip.w, ip, mv, p0,
+                                 vv);
+}
+
+// The sweep of a residual-driven frame: only the slices of instances still iterating,
+// listed per colour by the compaction after each probe (order within a colour does not
+// matter: its vertices are independent). A grid of resident size strides over the
+// list, so a converged instance costs nothing, not even a CTA launch.
 template <int TPV, int RE, int RB>
 __global__ void __launch_bounds__(256) vbd_sweep_list_kernel(SweepArgs a) {
     grid_dependency_wait();  // the list and the positions come from the kernels before
@@ -257,55 +325,8 @@ __global__ void __launch_bounds__(256) vbd_sweep_list_kernel(SweepArgs a) {
     const int lane = threadIdx.x & 31;
     const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
     const int count = *a.list_count;
-    for (int idx = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); idx < count; idx += nwarps) {
-        const int slice = a.list[idx];
-        const int4 sd = __ldg(&a.slices[slice]);
-        const int rows = sd.w & 0xffff, erows = sd.w >> 16, brows = rows - erows;
-        const int k = lane / TPV;
-        const bool leader = k < sd.y && (lane % TPV) == 0;
-        const int v = sd.x + min(k, sd.y - 1);
-        const int base = sd.z + lane;
-        const int bbase = base + erows * 32;
-        int ue[RE], ub[RB];
-        float we[RE], le[RE], wb[RB];
-#pragma unroll
-        for (int r = 0; r < RE; ++r) {
-            ue[r] = v;
-            we[r] = 0.f;
-            le[r] = -1.f;
-            if (r < erows) {
-                const int2 iw = __ldg(&a.st_iw[base + r * 32]);
-                ue[r] = iw.x;
-                we[r] = __int_as_float(iw.y);
-                le[r] = __ldg(&a.st_rest[base + r * 32]);
-            }
-        }
-#pragma unroll
-        for (int r = 0; r < RB; ++r) {
-            ub[r] = v;
-            wb[r] = 0.f;
-            if (r < brows) {
-                const int2 iw = __ldg(&a.st_iw[bbase + r * 32]);
-                ub[r] = iw.x;
-                wb[r] = __int_as_float(iw.y);
-            }
-        }
-        const float4 mv = __ldg(&a.vm[v]);
-        const float4 ip = __ldg(&a.inst[__float_as_int(mv.w)]);
-        const float4 xv = a.x[v];
-        float4 xe[RE], xb[RB];
-#pragma unroll
-        for (int r = 0; r < RE; ++r) xe[r] = a.x[ue[r]];
-#pragma unroll
-        for (int r = 0; r < RB; ++r) xb[r] = a.x[ub[r]];
-        float4 p0 = make_float4(0.f, 0.f, 0.f, 0.f), vv = p0;
-        if (leader) {
-            p0 = a.x0[v];
-            vv = a.vel[v];
-        }
-        sweep_vertex<TPV, RE, RB>(a, v, leader, base, bbase, erows, brows, xv, xe, le, we, xb, wb, ip.w, ip, mv, p0,
-                                  vv);
-    }
+    for (int idx = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); idx < count; idx += nwarps)
+        sweep_slice<TPV, RE, RB, PlainMem>(a, a.list[idx], lane);
 }
 
 }  // namespace ats
