@@ -1,6 +1,6 @@
 """Builds the C++ driver programs of tests/cpp against libats_b200.so (test
-infrastructure). vbd_dag also links the CPU oracle, whose per-step entry points are
-its host implementation of the VBD tasks."""
+infrastructure). vbd_dag and async_dag also link the CPU oracle, whose per-step entry
+points are their host implementation of the VBD tasks."""
 import os
 import subprocess
 import sys
@@ -9,8 +9,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
-SOURCES = ["heft_case.cpp", "vbd_dag.cpp", "launch_modes.cpp", "example2_sequence.cpp"]
-WITH_ORACLE = {"vbd_dag.cpp"}
+SOURCES = ["heft_case.cpp", "vbd_dag.cpp", "async_dag.cpp", "launch_modes.cpp", "example2_sequence.cpp"]
+WITH_ORACLE = {"vbd_dag.cpp", "async_dag.cpp"}
 
 
 def _stale(out, deps):
