@@ -94,6 +94,8 @@ typedef struct ats_cloth_info {
     int block_size;
     int stencil_slots;      /* stencil entries stored (incl. padding) */
     long long device_bytes; /* device memory held by the handle */
+    int vbd_form;           /* fixed-iteration VBD iterations: 0 a launch per colour, 1 persistent */
+    int xpbd_form;          /* XPBD iterations: 0 a launch per colour, 1 persistent */
 } ats_cloth_info;
 
 /* ---------------------------------------------------------------- host-only mesh helpers */
@@ -212,14 +214,15 @@ int ats_frame_to_residual(ats_cloth* cloth, double tol, int check_every, int max
 int ats_frame_to_residuals(ats_cloth* cloth, const double* tols, const int* first_check, int check_every,
                            int max_iterations, int* iterations, double* residual, ats_stream stream);
 
-/* Form of the VBD iterations of fixed-iteration frames and ats_vbd_iterations:
- * 0 one launch per colour (one wave, constant data loaded while the previous colour
- * drains); 1 persistent: all iterations in one cooperative launch, each colour a
- * grid-stride loop over its slices, a bounded grid barrier between colours. Both give
- * the same positions. ats_autotune chooses; this call overrides it (drops captured
- * frame graphs). Fails with ATS_ERR_INVALID if the device cannot run form 1. The
+/* Form of the iterations of fixed-iteration frames (and ats_vbd_iterations) for one
+ * solver: 0 one launch per colour (the next colour's constant data loads while the
+ * previous one drains); 1 persistent: all iterations in one cooperative launch, each
+ * colour a grid-stride loop, a bounded grid barrier between colours. Both give the
+ * same positions. A new handle starts with form 0 for both solvers; ats_autotune times
+ * both forms and keeps the faster; this call overrides it (and drops captured frame
+ * graphs). Fails with ATS_ERR_INVALID if the device cannot run form 1. The
  * residual-driven frames always use their persistent list sweep. */
-int ats_set_sweep_form(ats_cloth* cloth, int form);
+int ats_set_sweep_form(ats_cloth* cloth, int solver, int form);
 
 /* Probe schedule of the residual-driven frames of this handle (ats_frame_to_residual(s),
  * ats_frame_warm_to_residual). 0 (default): every check_every iterations after an
@@ -234,9 +237,9 @@ int ats_set_probe_policy(ats_cloth* cloth, int policy);
 
 /* Times `iterations` VBD iterations (three times, taking the fastest) for every
  * lanes-per-vertex (1, 2, 4, 8) and block size (64, 128, 256) on this handle's own
- * mesh, keeps the fastest, then times the persistent form of the fixed-iteration sweep
- * (ats_set_sweep_form) at that shape and keeps it where it is faster; reports the
- * shape. The iterate x is restored afterwards; captured frame graphs are dropped (they
+ * mesh, keeps the fastest, then times the persistent form of the fixed-iteration VBD
+ * and XPBD iterations (ats_set_sweep_form) and keeps each where it is faster; reports
+ * the shape (ats_cloth_query reports the forms). The iterate x is restored afterwards; captured frame graphs are dropped (they
  * are re-captured on next use). Synchronises `stream`. */
 int ats_autotune(ats_cloth* cloth, int iterations, ats_stream stream, int* tpv, int* block_size);
 

@@ -66,6 +66,8 @@ class ClothInfo(ctypes.Structure):
         ("block_size", ctypes.c_int),
         ("stencil_slots", ctypes.c_int),
         ("device_bytes", ctypes.c_longlong),
+        ("vbd_form", ctypes.c_int),
+        ("xpbd_form", ctypes.c_int),
     ]
 
 
@@ -141,7 +143,7 @@ _SIGNATURES = {
     "ats_frame_to_residuals": [_vp, _dp, _ip, ctypes.c_int, ctypes.c_int, _ip, _dp, _vp],
     "ats_kernel_launches": [ctypes.POINTER(ctypes.c_longlong)],
     "ats_set_probe_policy": [_vp, ctypes.c_int],
-    "ats_set_sweep_form": [_vp, ctypes.c_int],
+    "ats_set_sweep_form": [_vp, ctypes.c_int, ctypes.c_int],
     "ats_energy_noalloc": [_vp, _vp, _vp, _vp, _vp, ctypes.c_int, _vp, _vp, ctypes.c_int, _vp, _vp, ctypes.c_int,
                            ctypes.c_float, ctypes.c_float, _fp, ctypes.c_float, _vp, _vp],
 }
@@ -473,10 +475,13 @@ class Cloth:
     def record_end(self, dataset, stream=None):
         _check(lib().ats_record_frame_end(self.h, dataset.h, _stream(stream)))
 
-    def set_sweep_form(self, form):
-        """VBD iterations of fixed-iteration frames: 0 one launch per colour, 1 one
-        persistent cooperative launch (ats_set_sweep_form)."""
-        _check(lib().ats_set_sweep_form(self.h, int(form)))
+    def set_sweep_form(self, form, solver=SOLVER_VBD):
+        """Iterations of fixed-iteration frames of `solver`: 0 one launch per colour, 1
+        one persistent cooperative launch (ats_set_sweep_form)."""
+        _check(lib().ats_set_sweep_form(self.h, int(solver), int(form)))
+        info = ClothInfo()
+        _check(lib().ats_cloth_query(self.h, ctypes.byref(info)))
+        self.info = info
 
     def set_probe_policy(self, policy):
         """Probe schedule of the residual-driven frames: 0 fixed period, 1 extrapolated

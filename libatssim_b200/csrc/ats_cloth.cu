@@ -242,19 +242,25 @@ __global__ void xpbd_bending_kernel(float4* __restrict__ x, const float4* __rest
     if (i < e) solve_bend<PlainMem>(x, lambda, i, c, h);
 }
 
-// Grid-wide barrier of the persistent XPBD kernel, whose blocks are co-resident (a
+// Grid-wide barrier of the persistent kernels, whose blocks are co-resident (a
 // cooperative launch). bar[0] counts arrivals, bar[1] is the generation. Thread 0 of
 // every block reads the generation, publishes the block's writes (device-scope fence)
 // and arrives; the last arrival resets the count and advances the generation, the
-// others wait for that. The wait is bounded: after kBarrierSpins polls it sets *err
-// and every block leaves the kernel at its next barrier. Returns false on error.
+// others poll it with acquire loads (back to back for the first kBarrierFastPolls,
+// then with a short sleep). The wait is bounded: after kBarrierSpins polls it sets
+// *err, and every block leaves the kernel at its next barrier. Returns false on error.
 constexpr unsigned kBarrierSpins = 1u << 24;
+constexpr unsigned kBarrierFastPolls = 1u << 12;
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
 __device__ __forceinline__ bool grid_barrier(unsigned* bar, int* err, unsigned nblocks) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
-        volatile unsigned* gen = bar + 1;
-        const unsigned my_gen = *gen;
+        const unsigned my_gen = ld_acquire_gpu(bar + 1);
         __threadfence();
         const unsigned arrived = atomicAdd(bar, 1u);
         if (arrived == nblocks - 1) {
@@ -263,12 +269,13 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, int* err, unsigned n
             atomicAdd(bar + 1, 1u);
         } else {
             unsigned spins = 0;
-            while (*gen == my_gen) {
-                if (++spins > kBarrierSpins || *(volatile int*)err) {
+            while (ld_acquire_gpu(bar + 1) == my_gen) {
+                ++spins;
+                if ((spins & 1023u) == 0 && (spins > kBarrierSpins || *(volatile int*)err)) {
                     atomicExch(err, 1);
                     break;
                 }
-                __nanosleep(32);
+                if (spins > kBarrierFastPolls) __nanosleep(64);
             }
         }
         __threadfence();
@@ -1506,17 +1513,19 @@ extern "C" {
 
 const char* ats_last_error(void) { return g_last_error.c_str(); }
 
-int ats_set_sweep_form(ats_cloth* c, int form) {
-    if (!c || (form != 0 && form != 1)) {
-        set_error("ats_set_sweep_form: need a handle and form 0 (a launch per colour) or 1 (persistent)");
+int ats_set_sweep_form(ats_cloth* c, int solver, int form) {
+    if (!c || (form != 0 && form != 1) || (solver != ATS_SOLVER_VBD && solver != ATS_SOLVER_XPBD)) {
+        set_error("ats_set_sweep_form: need a handle, a solver and form 0 (a launch per colour) or 1 (persistent)");
         return ATS_ERR_INVALID;
     }
-    int blocks = 0;
-    if (form == 1 && (blocks = vbd_loop_blocks(c->L.tpv, c->block, c->device)) == 0) {
-        set_error("ats_set_sweep_form: the device cannot run the persistent sweep cooperatively");
+    const int blocks = form == 0 ? 0
+                                 : solver == ATS_SOLVER_VBD ? vbd_loop_blocks(c->L.tpv, c->block, c->device)
+                                                            : c->xpbd_loop_capable;
+    if (form == 1 && blocks == 0) {
+        set_error("ats_set_sweep_form: the device cannot run the persistent form cooperatively");
         return ATS_ERR_INVALID;
     }
-    c->vbd_loop_blocks = blocks;
+    (solver == ATS_SOLVER_VBD ? c->vbd_loop_blocks : c->xpbd_loop_blocks) = blocks;
     c->drop_graphs();  // captured frames hold the other form
     return ATS_OK;
 }
@@ -1629,7 +1638,8 @@ int ats_cloth_create(const ats_instance_desc* inst, int ninst, const ats_solver_
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, xpbd_loop_kernel, kXpbdLoopThreads, 0) != cudaSuccess)
             per_sm = 0;
-        c->xpbd_loop_blocks = coop && per_sm >= 1 ? sms : 0;
+        c->xpbd_loop_capable = coop && per_sm >= 1 ? sms : 0;
+        c->xpbd_loop_blocks = 0;  // per-colour launches until ats_autotune or ats_set_sweep_form chooses
     }
     if ((r = upload(c->en_edge, L.en_edge, L.en_rest.size())) || (r = upload(c->en_rest, L.en_rest, L.en_rest.size())) ||
         (r = upload(c->en_k, L.en_k, L.en_k.size())) || (r = upload(c->en_bend, L.en_bend, L.en_kb.size())) ||
@@ -1681,6 +1691,8 @@ int ats_cloth_query(const ats_cloth* c, ats_cloth_info* info) {
     info->block_size = c->block;
     info->stencil_slots = (int)c->L.st_rest.size();
     info->device_bytes = (long long)c->device_bytes();
+    info->vbd_form = c->vbd_loop_blocks > 0 ? 1 : 0;
+    info->xpbd_form = c->xpbd_loop_blocks > 0 ? 1 : 0;
     return ATS_OK;
 }
 
@@ -1972,6 +1984,29 @@ int ats_autotune(ats_cloth* c, int iterations, ats_stream stream, int* out_tpv, 
             r = time_iterations(ms);
             if (r || ms >= best) c->vbd_loop_blocks = 0;
         }
+    }
+    // XPBD iterations: per-colour launches against the persistent kernel (the fastest of
+    // three timings each); lambda is reset afterwards by every frame, x restored below
+    if (!r && c->xpbd_loop_capable > 0 && c->L.n_scolors + c->L.n_bcolors > 0) {
+        float t_form[2] = {1e30f, 1e30f};
+        for (int form = 0; form < 2 && !r; ++form) {
+            c->xpbd_loop_blocks = form ? c->xpbd_loop_capable : 0;
+            if ((r = enqueue_iterations(c, ATS_SOLVER_XPBD, 1, st))) break;
+            for (int rep = 0; rep < 3; ++rep) {
+                cudaEventRecord(e0, st);
+                if ((r = enqueue_iterations(c, ATS_SOLVER_XPBD, iterations, st))) break;
+                cudaEventRecord(e1, st);
+                if (cudaEventSynchronize(e1) != cudaSuccess) {
+                    set_error("ats_autotune: XPBD timing failed");
+                    r = ATS_ERR_CUDA;
+                    break;
+                }
+                float t = 0.f;
+                cudaEventElapsedTime(&t, e0, e1);
+                t_form[form] = std::min(t_form[form], t);
+            }
+        }
+        c->xpbd_loop_blocks = !r && t_form[1] < t_form[0] ? c->xpbd_loop_capable : 0;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

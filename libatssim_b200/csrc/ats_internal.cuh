@@ -77,7 +77,8 @@ struct ats_cloth {
     DevBuf<int> xs_color_d, xb_color_d;  // XPBD colour offsets, for the persistent kernel
     DevBuf<unsigned> loop_bar;           // its grid barrier: arrivals, generation
     DevBuf<int> loop_err;                // set when a barrier wait ran out
-    int xpbd_loop_blocks = 0;            // co-resident blocks of the persistent kernel (0: per-colour launches)
+    int xpbd_loop_capable = 0;           // co-resident blocks of the persistent XPBD kernel (0: unavailable)
+    int xpbd_loop_blocks = 0;            // the blocks XPBD frames launch it with (0: per-colour launches)
     int vbd_loop_blocks = 0;             // the same for VBD iterations (0: one launch per colour; set by autotune)
     DevBuf<int2> en_edge;
     DevBuf<float> en_rest, en_k, en_q, en_kb;

@@ -425,6 +425,8 @@ def test_xpbd_persistent_frame_equals_per_colour_launches(ats, n):
     prm = dict(implicit_dt=1.0 / 60.0, num_substep=1, iterations=12, damping=2.0)
     a = ats.Cloth([inst], **prm)
     b = ats.Cloth([inst], **prm)
+    a.set_sweep_form(1, ats.SOLVER_XPBD)
+    assert a.info.xpbd_form == 1
     for f in range(4):
         a.frame(ats.SOLVER_XPBD, graph=(f % 2 == 1))
         b.predict()
@@ -453,6 +455,7 @@ def test_persistent_vbd_frames_equal_per_colour_launches(ats, n):
     b = ats.Cloth([inst], **prm)
     a.set_sweep_form(1)
     b.set_sweep_form(0)
+    assert a.info.vbd_form == 1 and b.info.vbd_form == 0
     for f in range(4):
         a.frame(graph=(f % 2 == 1))
         b.frame(graph=(f % 2 == 1))
