@@ -6,9 +6,11 @@
 //   features (24): h v / s, (y - x0) / s, and for the 6 edge neighbours in rest
 //   directions (+x, +x+z, +z, -x, -x-z, -z) (x0_u - x0_v) / rest length (0 if none)
 //   output (3):    (x* - y) / s,   guess = y + s * output   (pinned vertices keep y)
-// Network 24 -> 64 -> 64 -> 64 -> 3, GELU (polynomial form, ats_gelu.cuh), BF16 weights and activations, FP32
-// accumulation on the tensor cores (mma.sync m16n8k16 bf16). Training: MSE on the
-// solved positions of recorded frames, Adam, deterministic per-CTA gradient partials.
+// Network 24 -> 64 -> 64 -> 64 -> 3, GELU (polynomial form, ats_gelu.cuh), BF16 weights
+// and activations, FP32 accumulation on the tensor cores: inference by tcgen05 MMA with
+// TMEM accumulators (infer_tc_kernel), training by mma.sync m16n8k16 (train_tile_kernel).
+// Training: MSE on the solved positions of recorded frames, Adam, deterministic per-CTA
+// gradient partials.
 // Fallback: per instance, the guess is kept only if the FP64 incremental potential
 // G(guess) <= G(y) (Energy::compute_energy_* terms, xpbd_constraints.h:2079-2214).
 
@@ -393,175 +395,9 @@ __global__ void __launch_bounds__(kThreads) infer_samples_kernel(const float* __
                 out[(size_t)(base + i) * kOut + k] = S.nrm[kNormOutMean + k] + S.nrm[kNormOutStd + k] * S.y[i][k];
 }
 
-// Inference, one warp per 32 vertices, activations kept in registers: the FP32
-// accumulators of a 64-wide layer (8 n-tiles of m16n8) are exactly the A fragments of
-// the next layer's four k16 steps once rounded to BF16 pairs, so only the features go
-// through shared memory. The warp's two m16 halves share every B fragment. Weights sit
-// in shared memory in padded rows (80 B / 144 B): the 8 row addresses of an ldmatrix
-// land in 8 different 16-byte bank groups, so fragment loads are conflict-free.
-// Persistent CTAs, as many as are resident. Same quantisation points and the same mma
-// order as forward(): identical outputs.
-constexpr int kWarpRows = 32;       // two m16 halves; every lane gathers one vertex's features
-constexpr int kRowX = kInP + 8;     // 40 bf16 = 80 B
-constexpr int kRowH = kHid + 8;     // 72 bf16 = 144 B
-struct __align__(16) WarpScratch {
-    __nv_bfloat16 x[kWarpRows][kRowX];
-    float out[kWarpRows][4];
-};
-struct __align__(16) InferSmem {
-    __nv_bfloat16 w1[kHid][kRowX];
-    __nv_bfloat16 w2[kHid][kRowH];
-    __nv_bfloat16 w3[kHid][kRowH];
-    __nv_bfloat16 w4[8][kRowH];  // output rows 0..2 used, 3..7 zero
-    float b[3 * kHid + 8];
-    float nrm[kNorm];
-    WarpScratch ws[kThreads / 32];
-};
-static_assert(sizeof(InferSmem) <= 48 * 1024, "static shared memory");
-static_assert(offsetof(InferSmem, w2) % 16 == 0 && offsetof(InferSmem, w3) % 16 == 0 &&
-                  offsetof(InferSmem, w4) % 16 == 0 && offsetof(InferSmem, ws) % 16 == 0,
-              "ldmatrix rows must be 16-byte aligned");
-
 __device__ __forceinline__ uint32_t pack_f2(float lo, float hi) {
     const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
     return *reinterpret_cast<const uint32_t*>(&v);
-}
-
-// four 8x8 BF16 matrices; lanes 8i..8i+7 give the row addresses of matrix i
-__device__ __forceinline__ void ldsm_x4(uint32_t r[4], const __nv_bfloat16* p) {
-    const uint32_t a = (uint32_t)__cvta_generic_to_shared(p);
-    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-                 : "r"(a)
-                 : "memory");
-}
-
-// acc[nt][4] (FP32, bias included) of a 64-wide layer -> GELU -> A fragments a[ks][4]
-// of the next layer; adjacent columns (2t, 2t+1) go through one packed GELU
-__device__ __forceinline__ void hidden_epilogue(const float acc[8][4], uint32_t a[4][4]) {
-#pragma unroll
-    for (int ks = 0; ks < 4; ++ks) {
-        const float2 h0 = gelu2(make_float2(acc[2 * ks][0], acc[2 * ks][1]));
-        const float2 h1 = gelu2(make_float2(acc[2 * ks][2], acc[2 * ks][3]));
-        const float2 h2 = gelu2(make_float2(acc[2 * ks + 1][0], acc[2 * ks + 1][1]));
-        const float2 h3 = gelu2(make_float2(acc[2 * ks + 1][2], acc[2 * ks + 1][3]));
-        a[ks][0] = pack_f2(h0.x, h0.y);
-        a[ks][1] = pack_f2(h1.x, h1.y);
-        a[ks][2] = pack_f2(h2.x, h2.y);
-        a[ks][3] = pack_f2(h3.x, h3.y);
-    }
-}
-
-// acc[h][nt] = bias + A_h (16 x 16 KS) * W^T for n-tiles 0..NT-1; W rows [n][k] with
-// stride ROW
-template <int KS, int NT, int ROW>
-__device__ __forceinline__ void warp_layer2(const uint32_t a[2][4][4], const __nv_bfloat16* W, const float* bias,
-                                            int lane, float acc[2][NT][4]) {
-#pragma unroll
-    for (int nt = 0; nt < NT; ++nt) {
-        uint32_t b[KS][2];
-#pragma unroll
-        for (int p = 0; p < KS / 2; ++p) {
-            uint32_t r[4];
-            ldsm_x4(r, W + (8 * nt + (lane & 7)) * ROW + 32 * p + (lane >> 3) * 8);
-            b[2 * p][0] = r[0];
-            b[2 * p][1] = r[1];
-            b[2 * p + 1][0] = r[2];
-            b[2 * p + 1][1] = r[3];
-        }
-        const float b0 = bias[8 * nt + 2 * (lane & 3)], b1 = bias[8 * nt + 2 * (lane & 3) + 1];
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            acc[h][nt][0] = acc[h][nt][2] = b0;
-            acc[h][nt][1] = acc[h][nt][3] = b1;
-#pragma unroll
-            for (int ks = 0; ks < KS; ++ks)
-                mma16816(acc[h][nt], a[h][ks][0], a[h][ks][1], a[h][ks][2], a[h][ks][3], b[ks][0], b[ks][1]);
-        }
-    }
-}
-
-__global__ void __launch_bounds__(kThreads, 3) infer_warp_kernel(FeatArgs fa, const __nv_bfloat16* __restrict__ wpack,
-                                                                 const float* __restrict__ master,
-                                                                 const float* __restrict__ nrm, float4* __restrict__ x,
-                                                                 float s) {
-    __shared__ InferSmem S;
-    for (int i = threadIdx.x; i < kNorm; i += kThreads) S.nrm[i] = nrm[i];
-    const uint32_t* wp = reinterpret_cast<const uint32_t*>(wpack);
-    for (int i = threadIdx.x; i < kHid * (kInP / 2); i += kThreads)
-        reinterpret_cast<uint32_t*>(&S.w1[i / (kInP / 2)][0])[i % (kInP / 2)] = wp[kP1 / 2 + i];
-    for (int i = threadIdx.x; i < kHid * (kHid / 2); i += kThreads) {
-        reinterpret_cast<uint32_t*>(&S.w2[i / (kHid / 2)][0])[i % (kHid / 2)] = wp[kP2 / 2 + i];
-        reinterpret_cast<uint32_t*>(&S.w3[i / (kHid / 2)][0])[i % (kHid / 2)] = wp[kP3 / 2 + i];
-    }
-    for (int i = threadIdx.x; i < 8 * (kHid / 2); i += kThreads)
-        reinterpret_cast<uint32_t*>(&S.w4[i / (kHid / 2)][0])[i % (kHid / 2)] = wp[kP4 / 2 + i];
-    for (int i = threadIdx.x; i < kHid; i += kThreads) {
-        S.b[i] = master[kB1 + i];
-        S.b[kHid + i] = master[kB2 + i];
-        S.b[2 * kHid + i] = master[kB3 + i];
-    }
-    for (int i = threadIdx.x; i < 8; i += kThreads) S.b[3 * kHid + i] = i < kOut ? master[kB4 + i] : 0.f;
-    __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-    WarpScratch& W = S.ws[warp];
-    const int ntiles = (fa.nv + kWarpRows - 1) / kWarpRows;
-    for (int tile = blockIdx.x * (kThreads / 32) + warp; tile < ntiles; tile += gridDim.x * (kThreads / 32)) {
-        const int v = tile * kWarpRows + lane;
-        {
-            float f[kIn];
-            if (v < fa.nv) vertex_features(fa, v, f);
-            uint32_t q[kInP / 2];
-#pragma unroll
-            for (int k = 0; k < kIn / 2; ++k)
-                q[k] = v < fa.nv ? pack_f2((f[2 * k] - S.nrm[kNormInMean + 2 * k]) * S.nrm[kNormInScale + 2 * k],
-                                           (f[2 * k + 1] - S.nrm[kNormInMean + 2 * k + 1]) *
-                                               S.nrm[kNormInScale + 2 * k + 1])
-                                 : 0u;
-#pragma unroll
-            for (int k = kIn / 2; k < kInP / 2; ++k) q[k] = 0u;
-            uint4* row = reinterpret_cast<uint4*>(&W.x[lane][0]);
-#pragma unroll
-            for (int j = 0; j < kInP / 8; ++j) row[j] = make_uint4(q[4 * j], q[4 * j + 1], q[4 * j + 2], q[4 * j + 3]);
-        }
-        __syncwarp();
-        uint32_t a[2][4][4];
-#pragma unroll
-        for (int h = 0; h < 2; ++h)
-#pragma unroll
-            for (int ks = 0; ks < 2; ++ks)
-                ldsm_x4(a[h][ks], &W.x[16 * h + (lane & 8) + (lane & 7)][16 * ks + ((lane >> 4) << 3)]);
-        float acc[2][8][4];
-        warp_layer2<2, 8, kRowX>(a, &S.w1[0][0], S.b, lane, acc);
-        hidden_epilogue(acc[0], a[0]);
-        hidden_epilogue(acc[1], a[1]);
-        warp_layer2<4, 8, kRowH>(a, &S.w2[0][0], S.b + kHid, lane, acc);
-        hidden_epilogue(acc[0], a[0]);
-        hidden_epilogue(acc[1], a[1]);
-        warp_layer2<4, 8, kRowH>(a, &S.w3[0][0], S.b + 2 * kHid, lane, acc);
-        hidden_epilogue(acc[0], a[0]);
-        hidden_epilogue(acc[1], a[1]);
-        float o[2][1][4];
-        warp_layer2<4, 1, kRowH>(a, &S.w4[0][0], S.b + 3 * kHid, lane, o);  // output columns 0..7 (0..2 used)
-        if (t < 2) {
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                W.out[16 * h + g][2 * t] = o[h][0][0];
-                W.out[16 * h + g][2 * t + 1] = o[h][0][1];
-                W.out[16 * h + g + 8][2 * t] = o[h][0][2];
-                W.out[16 * h + g + 8][2 * t + 1] = o[h][0][3];
-            }
-        }
-        __syncwarp();
-        if (v < fa.nv && fa.vm[v].y == 0.f) {
-            float4 p = x[v];
-            p.x += s * (S.nrm[kNormOutMean + 0] + S.nrm[kNormOutStd + 0] * W.out[lane][0]);
-            p.y += s * (S.nrm[kNormOutMean + 1] + S.nrm[kNormOutStd + 1] * W.out[lane][1]);
-            p.z += s * (S.nrm[kNormOutMean + 2] + S.nrm[kNormOutStd + 2] * W.out[lane][2]);
-            x[v] = p;
-        }
-        __syncwarp();
-    }
 }
 
 // Inference on the 5th-generation tensor cores: one CTA of 128 threads per tile of 128
@@ -798,7 +634,6 @@ int ensure_partials(ats_mlp* m, int ctas) {
     return ATS_OK;
 }
 
-int g_infer_ctas = 148;  // resident CTAs of infer_warp_kernel on the device (set_smem_limits)
 int g_tc_ctas = 148;     // CTAs of infer_tc_kernel: resident ones, at most 4 per SM (TMEM)
 
 // Kernel attributes and launch shapes, set once before any launch or capture.
@@ -806,11 +641,9 @@ int set_smem_limits() {
     static bool done = false;
     if (done) return ATS_OK;
     {
-        int dev = 0, sms = 0, resident = 0;
+        int dev = 0, sms = 0;
         ATS_CUDA(cudaGetDevice(&dev));
         ATS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        ATS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, infer_warp_kernel, kThreads, 0));
-        g_infer_ctas = std::max(1, sms) * std::max(1, resident);
         ATS_CUDA(cudaFuncSetAttribute(infer_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
         int tc_resident = 0;
         ATS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tc_resident, infer_tc_kernel, kTcRows, kTcSmem));
