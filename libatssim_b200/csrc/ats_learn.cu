@@ -645,6 +645,10 @@ int set_smem_limits() {
         ATS_CUDA(cudaGetDevice(&dev));
         ATS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         ATS_CUDA(cudaFuncSetAttribute(infer_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
+        // the whole L1 / shared split as shared memory: four 48 KB CTAs per SM (with the
+        // default split the runtime sized the SM for one)
+        ATS_CUDA(cudaFuncSetAttribute(infer_tc_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                      (int)cudaSharedmemCarveoutMaxShared));
         int tc_resident = 0;
         ATS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tc_resident, infer_tc_kernel, kTcRows, kTcSmem));
         // every resident CTA holds kTcCols of the SM's 512 TMEM columns
@@ -652,6 +656,8 @@ int set_smem_limits() {
         g_tc_ctas = std::max(1, sms) * std::max(1, tc_resident);
     }
     ATS_CUDA(cudaFuncSetAttribute(train_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmem));
+    ATS_CUDA(cudaFuncSetAttribute(train_tile_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  (int)cudaSharedmemCarveoutMaxShared));
     ATS_CUDA(cudaFuncSetAttribute(infer_samples_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmem));
     done = true;
     return ATS_OK;
