@@ -419,9 +419,10 @@ def run_learned(args):
     rec_iters = prm["iterations"]
     stream = torch.cuda.current_stream()
     t0 = time.perf_counter()
-    cloth = ats.Cloth(insts, **prm)
+    cloth = ats.Cloth(insts, threads_per_vertex=args.tpv, block_size=args.block, **prm)
     t_create = time.perf_counter() - t0
-    tuned = cloth.autotune(iterations=20, stream=stream)
+    # the autotuned shape unless one is given (--tpv / --block, for shape sweeps)
+    tuned = cloth.autotune(iterations=20, stream=stream) if not (args.tpv or args.block) else (args.tpv, args.block)
     cloth.set_probe_policy(args.probe_policy)
     info = cloth.info
     nv = info.num_verts
