@@ -68,6 +68,7 @@ class ClothInfo(ctypes.Structure):
         ("device_bytes", ctypes.c_longlong),
         ("vbd_form", ctypes.c_int),
         ("xpbd_form", ctypes.c_int),
+        ("list_form", ctypes.c_int),
     ]
 
 
@@ -144,6 +145,7 @@ _SIGNATURES = {
     "ats_kernel_launches": [ctypes.POINTER(ctypes.c_longlong)],
     "ats_set_probe_policy": [_vp, ctypes.c_int],
     "ats_set_sweep_form": [_vp, ctypes.c_int, ctypes.c_int],
+    "ats_set_list_sweep": [_vp, ctypes.c_int],
     "ats_energy_noalloc": [_vp, _vp, _vp, _vp, _vp, ctypes.c_int, _vp, _vp, ctypes.c_int, _vp, _vp, ctypes.c_int,
                            ctypes.c_float, ctypes.c_float, _fp, ctypes.c_float, _vp, _vp],
 }
@@ -479,6 +481,13 @@ class Cloth:
         """Iterations of fixed-iteration frames of `solver`: 0 one launch per colour, 1
         one persistent cooperative launch (ats_set_sweep_form)."""
         _check(lib().ats_set_sweep_form(self.h, int(solver), int(form)))
+        info = ClothInfo()
+        _check(lib().ats_cloth_query(self.h, ctypes.byref(info)))
+        self.info = info
+
+    def set_list_sweep(self, pipelined):
+        """Sweep of the residual-driven frames: 0 plain, 1 pipelined (ats_set_list_sweep)."""
+        _check(lib().ats_set_list_sweep(self.h, int(pipelined)))
         info = ClothInfo()
         _check(lib().ats_cloth_query(self.h, ctypes.byref(info)))
         self.info = info

@@ -258,10 +258,6 @@ __global__ void __launch_bounds__(256) vbd_sweep_kernel(SweepArgs a) {
     sweep_vertex<TPV, RE, RB>(a, v, leader, base, bbase, erows, brows, xv, xe, le, we, xb, wb, ks, ip, mv, p0, vv);
 }
 
-// The sweep of a residual-driven frame: only the slices of instances still iterating,
-// listed per colour by the compaction after each probe (order within a colour does not
-// matter: its vertices are independent). A grid of resident size strides over the
-// list, so a converged instance costs nothing, not even a CTA launch.
 // One slice of a sweep: every vertex of the slice (its constant data, then all
 // neighbour positions at once, then the solve). M chooses how positions are accessed.
 template <int TPV, int RE, int RB, class M>
@@ -312,6 +308,133 @@ __device__ __forceinline__ void sweep_slice(const SweepArgs& a, int slice, int l
     }
     sweep_vertex<TPV, RE, RB, M>(a, v, leader, base, bbase, erows, brows, xv, xe, le, we, xb, wb, ip.w, ip, mv, p0,
                                  vv);
+}
+
+// ---------------------------------------------------------------- pipelined list sweep
+// A warp's slices are independent of one another inside a colour: a slice reads its own
+// vertices' records, its stencil and the positions of neighbours of other colours, none
+// of which this colour writes. So while a warp computes one slice, the constant data of
+// its next slice (stencil rows, rest lengths, the lanes' own vertex records) is already
+// on its way into shared memory by cp.async, and the descriptor of the slice after that
+// is loading into registers. Every lane stages and later reads only its own entries.
+template <int RE, int RB>
+struct SliceStage {
+    int2 iw[RE + RB][32];  // stencil rows: {neighbour, bending weight}
+    float rest[RE][32];    // rest lengths of the edge rows
+    float4 vm[32], x0[32], vel[32];
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+template <int TPV, int RE, int RB>
+__device__ __forceinline__ void stage_slice(SliceStage<RE, RB>& S, const SweepArgs& a, int4 sd, int lane) {
+    const int rows = sd.w & 0xffff, erows = sd.w >> 16, brows = rows - erows;
+    const int v = sd.x + min(lane / TPV, sd.y - 1);
+    const int base = sd.z + lane, bbase = base + erows * 32;
+#pragma unroll
+    for (int r = 0; r < RE; ++r)
+        if (r < erows) {
+            cp_async8(&S.iw[r][lane], &a.st_iw[base + r * 32]);
+            cp_async4(&S.rest[r][lane], &a.st_rest[base + r * 32]);
+        }
+#pragma unroll
+    for (int r = 0; r < RB; ++r)
+        if (r < brows) cp_async8(&S.iw[RE + r][lane], &a.st_iw[bbase + r * 32]);
+    cp_async16(&S.vm[lane], &a.vm[v]);
+    cp_async16(&S.x0[lane], &a.x0[v]);
+    cp_async16(&S.vel[lane], &a.vel[v]);
+}
+
+// sweep_slice with the constant data from a staged slice
+template <int TPV, int RE, int RB>
+__device__ __forceinline__ void sweep_staged(const SweepArgs& a, const SliceStage<RE, RB>& S, int4 sd, int lane) {
+    const int rows = sd.w & 0xffff, erows = sd.w >> 16, brows = rows - erows;
+    const int k = lane / TPV;
+    const bool leader = k < sd.y && (lane % TPV) == 0;
+    const int v = sd.x + min(k, sd.y - 1);
+    const int base = sd.z + lane;
+    const int bbase = base + erows * 32;
+    int ue[RE], ub[RB];
+    float we[RE], le[RE], wb[RB];
+#pragma unroll
+    for (int r = 0; r < RE; ++r) {
+        ue[r] = v;
+        we[r] = 0.f;
+        le[r] = -1.f;
+        if (r < erows) {
+            const int2 iw = S.iw[r][lane];
+            ue[r] = iw.x;
+            we[r] = __int_as_float(iw.y);
+            le[r] = S.rest[r][lane];
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < RB; ++r) {
+        ub[r] = v;
+        wb[r] = 0.f;
+        if (r < brows) {
+            const int2 iw = S.iw[RE + r][lane];
+            ub[r] = iw.x;
+            wb[r] = __int_as_float(iw.y);
+        }
+    }
+    const float4 mv = S.vm[lane];
+    const float4 ip = __ldg(&a.inst[__float_as_int(mv.w)]);
+    const float4 xv = a.x[v];
+    float4 xe[RE], xb[RB];
+#pragma unroll
+    for (int r = 0; r < RE; ++r) xe[r] = a.x[ue[r]];
+#pragma unroll
+    for (int r = 0; r < RB; ++r) xb[r] = a.x[ub[r]];
+    sweep_vertex<TPV, RE, RB, PlainMem>(a, v, leader, base, bbase, erows, brows, xv, xe, le, we, xb, wb, ip.w, ip, mv,
+                                        S.x0[lane], S.vel[lane]);
+}
+
+// The list sweep, software-pipelined across each warp's slices (two shared-memory
+// stages per warp, dynamic shared memory 2 * warps per block * sizeof(SliceStage)).
+template <int TPV, int RE, int RB>
+__global__ void __launch_bounds__(256) vbd_sweep_pipe_kernel(SweepArgs a) {
+    extern __shared__ __align__(16) unsigned char pipe_smem[];
+    grid_dependency_wait();  // the list and the positions come from the kernels before
+    allow_dependent_launch();
+    const int lane = threadIdx.x & 31;
+    SliceStage<RE, RB>* buf = reinterpret_cast<SliceStage<RE, RB>*>(pipe_smem) + 2 * (threadIdx.x >> 5);
+    const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
+    const int count = *a.list_count;
+    int idx = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (idx >= count) return;
+    int4 sd_cur = __ldg(&a.slices[a.list[idx]]);
+    stage_slice<TPV, RE, RB>(buf[0], a, sd_cur, lane);
+    cp_async_commit();
+    int4 sd_nxt = make_int4(0, 0, 0, 0);
+    if (idx + nwarps < count) sd_nxt = __ldg(&a.slices[a.list[idx + nwarps]]);
+    for (int it = 0; idx < count; idx += nwarps, ++it) {
+        const int cur = it & 1;
+        if (idx + nwarps < count) stage_slice<TPV, RE, RB>(buf[cur ^ 1], a, sd_nxt, lane);
+        cp_async_commit();  // empty when there is no next slice: the wait below stays uniform
+        int4 sd_after = make_int4(0, 0, 0, 0);
+        if (idx + 2 * nwarps < count) sd_after = __ldg(&a.slices[a.list[idx + 2 * nwarps]]);
+        cp_async_wait<1>();  // the current slice's stage has landed
+        sweep_staged<TPV, RE, RB>(a, buf[cur], sd_cur, lane);
+        __syncwarp();  // this stage is refilled two slices later
+        sd_cur = sd_nxt;
+        sd_nxt = sd_after;
+    }
+    cp_async_wait<0>();
 }
 
 // The sweep of a residual-driven frame: only the slices of instances still iterating,

@@ -466,3 +466,24 @@ def test_persistent_vbd_frames_equal_per_colour_launches(ats, n):
     a.vbd_iterations(3)
     b.vbd_iterations(3)
     assert np.array_equal(a.positions(), b.positions())
+
+
+@pytest.mark.parametrize("tpv", [1, 2, 4, 8])
+def test_pipelined_list_sweep_equals_plain(ats, tpv):
+    """The residual-driven frames' sweep, plain and pipelined (each warp stages its next
+    slice in shared memory while computing the current one): the same slices and the
+    same arithmetic, so bit-identical positions; with some instances stopping early."""
+    insts, prm = configs.c2(num_instances=5, seed=3, side_range=(20, 90))
+    a = ats.Cloth(insts, threads_per_vertex=tpv, block_size=128, **prm)
+    b = ats.Cloth(insts, threads_per_vertex=tpv, block_size=128, **prm)
+    a.set_list_sweep(0)
+    b.set_list_sweep(1)
+    assert a.info.list_form == 0 and b.info.list_form == 1
+    for f in range(4):
+        tol = 0.0 if f % 2 == 0 else 0.35
+        ia, ra = a.frame_to_residual(tol, check_every=5, max_iterations=15)
+        ib, rb = b.frame_to_residual(tol, check_every=5, max_iterations=15)
+        assert np.array_equal(ia, ib) and np.array_equal(ra, rb)
+    xa, va = a.state()
+    xb, vb = b.state()
+    assert np.array_equal(xa, xb) and np.array_equal(va, vb)
