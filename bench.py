@@ -99,6 +99,8 @@ def parse():
     p.add_argument("--trace-out", default="", help="write the full residual traces (JSON) here")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-extras", action="store_true")
+    p.add_argument("--list-sweep", type=int, default=-1, choices=[-1, 0, 1],
+                   help="sweep of the residual-driven frames: -1 the autotuner's choice, 0 plain, 1 pipelined")
     p.add_argument("--tpv", type=int, default=0)
     p.add_argument("--block", type=int, default=0)
     return p.parse_args()
@@ -424,6 +426,8 @@ def run_learned(args):
     # the autotuned shape unless one is given (--tpv / --block, for shape sweeps)
     tuned = cloth.autotune(iterations=20, stream=stream) if not (args.tpv or args.block) else (args.tpv, args.block)
     cloth.set_probe_policy(args.probe_policy)
+    if args.list_sweep >= 0:
+        cloth.set_list_sweep(args.list_sweep)
     info = cloth.info
     nv = info.num_verts
     # training data: plain frames of this rank's instances
@@ -552,7 +556,8 @@ def run_learned(args):
                             "frac": achieved / peak, "traffic": None,
                             "traffic_note": "not captured in this run; the committed ncu summaries under profiles/ "
                                             "hold the DRAM bytes of this kernel",
-                            "kernel": f"vbd_sweep_list_kernel<{info.threads_per_vertex}>",
+                            "kernel": ("vbd_sweep_pipe_kernel" if info.list_form else "vbd_sweep_list_kernel")
+                                      + f"<{info.threads_per_vertex}>",
                             "us_per_launch_upper_bound": per_launch * 1e3, "alg_bytes_per_launch": bytes_launch,
                             "timing": "50 listed iterations over all instances, CUDA events, predict/update/2 probes "
                                       "included", "peak_source": peak_src,

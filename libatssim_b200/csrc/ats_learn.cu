@@ -634,7 +634,7 @@ int ensure_partials(ats_mlp* m, int ctas) {
     return ATS_OK;
 }
 
-int g_tc_ctas = 148;     // CTAs of infer_tc_kernel: resident ones, at most 4 per SM (TMEM)
+int g_tc_ctas = 148;     // CTAs of infer_tc_kernel: up to 4 per SM (shared memory, TMEM)
 
 // Kernel attributes and launch shapes, set once before any launch or capture.
 int set_smem_limits() {
@@ -649,11 +649,15 @@ int set_smem_limits() {
         // default split the runtime sized the SM for one)
         ATS_CUDA(cudaFuncSetAttribute(infer_tc_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
                                       (int)cudaSharedmemCarveoutMaxShared));
-        int tc_resident = 0;
-        ATS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tc_resident, infer_tc_kernel, kTcRows, kTcSmem));
-        // every resident CTA holds kTcCols of the SM's 512 TMEM columns
-        tc_resident = std::min(tc_resident, (int)(512 / kTcCols));
-        g_tc_ctas = std::max(1, sms) * std::max(1, tc_resident);
+        // 4 CTAs per SM: registers (119 x 128), shared memory (48 KB each) and TMEM
+        // (4 x 128 of 512 columns) all admit four; the occupancy query reports one for
+        // this kernel, and CTAs beyond what is resident simply start later (each works
+        // alone on its tiles and frees its TMEM)
+        int smem_optin = 0;
+        ATS_CUDA(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+        const int by_smem = std::max(1, smem_optin / (int)(kTcSmem + 1024));
+        const int tc_resident = std::min(by_smem, (int)(512 / kTcCols));
+        g_tc_ctas = std::max(1, sms) * tc_resident;
     }
     ATS_CUDA(cudaFuncSetAttribute(train_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmem));
     ATS_CUDA(cudaFuncSetAttribute(train_tile_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
