@@ -99,8 +99,9 @@ def parse():
     p.add_argument("--trace-out", default="", help="write the full residual traces (JSON) here")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-extras", action="store_true")
-    p.add_argument("--list-sweep", type=int, default=-1, choices=[-1, 0, 1],
-                   help="sweep of the residual-driven frames: -1 the autotuner's choice, 0 plain, 1 pipelined")
+    p.add_argument("--list-sweep", type=int, default=-1, choices=[-1, 0, 1, 2],
+                   help="sweep of the residual-driven frames: -1 the autotuner's choice, 0 plain, 1 pipelined, "
+                        "2 streamed")
     p.add_argument("--tpv", type=int, default=0)
     p.add_argument("--block", type=int, default=0)
     return p.parse_args()
@@ -556,8 +557,8 @@ def run_learned(args):
                             "frac": achieved / peak, "traffic": None,
                             "traffic_note": "not captured in this run; the committed ncu summaries under profiles/ "
                                             "hold the DRAM bytes of this kernel",
-                            "kernel": ("vbd_sweep_pipe_kernel" if info.list_form else "vbd_sweep_list_kernel")
-                                      + f"<{info.threads_per_vertex}>",
+                            "kernel": ("vbd_sweep_list_kernel", "vbd_sweep_pipe_kernel",
+                                       "vbd_sweep_stream_kernel")[info.list_form] + f"<{info.threads_per_vertex}>",
                             "us_per_launch_upper_bound": per_launch * 1e3, "alg_bytes_per_launch": bytes_launch,
                             "timing": "50 listed iterations over all instances, CUDA events, predict/update/2 probes "
                                       "included", "peak_source": peak_src,

@@ -96,7 +96,7 @@ typedef struct ats_cloth_info {
     long long device_bytes; /* device memory held by the handle */
     int vbd_form;           /* fixed-iteration VBD iterations: 0 a launch per colour, 1 persistent */
     int xpbd_form;          /* XPBD iterations: 0 a launch per colour, 1 persistent */
-    int list_form;          /* list sweep of residual-driven frames: 0 plain, 1 pipelined */
+    int list_form;          /* list sweep of residual-driven frames: 0 plain, 1 pipelined, 2 streamed */
 } ats_cloth_info;
 
 /* ---------------------------------------------------------------- host-only mesh helpers */
@@ -228,8 +228,11 @@ int ats_set_sweep_form(ats_cloth* cloth, int solver, int form);
 /* The sweep of the residual-driven frames (a resident grid striding over the slices of
  * the instances still iterating): 0 plain; 1 pipelined, where each warp stages its next
  * slice's stencil and vertex records in shared memory (cp.async) while it computes the
- * current one. Same positions. ats_autotune times both and keeps the faster. */
-int ats_set_list_sweep(ats_cloth* cloth, int pipelined);
+ * current one; 2 streamed, where the data read once per iteration (stencil, vertex
+ * records, frame-start state) goes through evict-first loads, leaving L2 to the
+ * positions, and each warp's next slice descriptor loads while the current slice
+ * computes. Same positions. ats_autotune times the three and keeps the fastest. */
+int ats_set_list_sweep(ats_cloth* cloth, int form);
 
 /* Probe schedule of the residual-driven frames of this handle (ats_frame_to_residual(s),
  * ats_frame_warm_to_residual). 0 (default): every check_every iterations after an
@@ -245,8 +248,8 @@ int ats_set_probe_policy(ats_cloth* cloth, int policy);
 /* Times `iterations` VBD iterations (three times, taking the fastest) for every
  * lanes-per-vertex (1, 2, 4, 8) and block size (64, 128, 256) on this handle's own
  * mesh, keeps the fastest, then times the persistent form of the fixed-iteration VBD
- * and XPBD iterations (ats_set_sweep_form) and the pipelined list sweep
- * (ats_set_list_sweep) and keeps each where it is faster; reports the shape
+ * and XPBD iterations (ats_set_sweep_form) and the forms of the list sweep
+ * (ats_set_list_sweep) and keeps the fastest of each; reports the shape
  * (ats_cloth_query reports the forms). The iterate x is restored afterwards; captured frame graphs are dropped (they
  * are re-captured on next use). Synchronises `stream`. */
 int ats_autotune(ats_cloth* cloth, int iterations, ats_stream stream, int* tpv, int* block_size);

@@ -485,9 +485,10 @@ class Cloth:
         _check(lib().ats_cloth_query(self.h, ctypes.byref(info)))
         self.info = info
 
-    def set_list_sweep(self, pipelined):
-        """Sweep of the residual-driven frames: 0 plain, 1 pipelined (ats_set_list_sweep)."""
-        _check(lib().ats_set_list_sweep(self.h, int(pipelined)))
+    def set_list_sweep(self, form):
+        """Sweep of the residual-driven frames: 0 plain, 1 pipelined, 2 streamed
+        (ats_set_list_sweep)."""
+        _check(lib().ats_set_list_sweep(self.h, int(form)))
         info = ClothInfo()
         _check(lib().ats_cloth_query(self.h, ctypes.byref(info)))
         self.info = info

@@ -945,35 +945,40 @@ int resident_ctas(K kernel, int block, size_t smem, int sms) {
     return std::max(1, sms) * (e == cudaSuccess && res > 0 ? res : 1);
 }
 
-// Resident CTAs of the list sweeps (pipe = 0: vbd_sweep_list_kernel, 1:
-// vbd_sweep_pipe_kernel), all SMs together, per (lanes per vertex, block size); queried
+// Resident CTAs of the list sweeps (form 0: vbd_sweep_list_kernel, 1:
+// vbd_sweep_pipe_kernel, 2: vbd_sweep_stream_kernel), all SMs together, per (lanes per
+// vertex, block size); queried
 // (and the pipelined kernel's shared-memory attributes set) on first use, which is
 // outside stream capture (the eager iterations of ats_frame_to_residual's first frame,
 // or ats_autotune, come first).
-int list_sweep_ctas(int tpv, int block, int pipe) {
-    static int cache[2][4][3] = {};
+template <int TPV, int RE, int RB>
+int list_form_ctas(int form, int block, int sms) {
+    switch (form) {
+        case 1: return resident_ctas(vbd_sweep_pipe_kernel<TPV, RE, RB>, block, (block / 32) * pipe_smem_per_warp<RE, RB>(), sms);
+        case 2: return resident_ctas(vbd_sweep_stream_kernel<TPV, RE, RB>, block, 0, sms);
+        default: return resident_ctas(vbd_sweep_list_kernel<TPV, RE, RB>, block, 0, sms);
+    }
+}
+int list_sweep_ctas(int tpv, int block, int form) {
+    static int cache[3][4][3] = {};
     const int ti = tpv == 1 ? 0 : tpv == 2 ? 1 : tpv == 4 ? 2 : 3, bi = block == 64 ? 0 : block == 128 ? 1 : 2;
-    int& slot = cache[pipe ? 1 : 0][ti][bi];
+    int& slot = cache[form >= 0 && form < 3 ? form : 0][ti][bi];
     if (!slot) {
         int dev = 0, sms = 148;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        const size_t smem = pipe ? pipe_smem_bytes(tpv, block) : 0;
         switch (tpv) {
-            case 1: slot = pipe ? resident_ctas(vbd_sweep_pipe_kernel<1, 6, 6>, block, smem, sms)
-                                : resident_ctas(vbd_sweep_list_kernel<1, 6, 6>, block, smem, sms); break;
-            case 2: slot = pipe ? resident_ctas(vbd_sweep_pipe_kernel<2, 3, 3>, block, smem, sms)
-                                : resident_ctas(vbd_sweep_list_kernel<2, 3, 3>, block, smem, sms); break;
-            case 4: slot = pipe ? resident_ctas(vbd_sweep_pipe_kernel<4, 2, 2>, block, smem, sms)
-                                : resident_ctas(vbd_sweep_list_kernel<4, 2, 2>, block, smem, sms); break;
-            default: slot = pipe ? resident_ctas(vbd_sweep_pipe_kernel<8, 1, 1>, block, smem, sms)
-                                 : resident_ctas(vbd_sweep_list_kernel<8, 1, 1>, block, smem, sms); break;
+            case 1: slot = list_form_ctas<1, 6, 6>(form, block, sms); break;
+            case 2: slot = list_form_ctas<2, 3, 3>(form, block, sms); break;
+            case 4: slot = list_form_ctas<4, 2, 2>(form, block, sms); break;
+            default: slot = list_form_ctas<8, 1, 1>(form, block, sms); break;
         }
     }
     return slot;
 }
 
-// listed: 0 one-wave sweep over the colour's slices, 1 list sweep, 2 pipelined list sweep
+// listed: 0 one-wave sweep over the colour's slices, 1 list sweep, 2 pipelined list
+// sweep, 3 streamed list sweep
 template <int TPV, int RE, int RB>
 cudaError_t sweep_launch(dim3 grid, dim3 block, cudaStream_t st, const SweepArgs& a, int listed) {
     cudaLaunchConfig_t cfg = {};
@@ -986,7 +991,8 @@ cudaError_t sweep_launch(dim3 grid, dim3 block, cudaStream_t st, const SweepArgs
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    const cudaError_t e = listed == 2   ? cudaLaunchKernelEx(&cfg, vbd_sweep_pipe_kernel<TPV, RE, RB>, a)
+    const cudaError_t e = listed == 3   ? cudaLaunchKernelEx(&cfg, vbd_sweep_stream_kernel<TPV, RE, RB>, a)
+                          : listed == 2 ? cudaLaunchKernelEx(&cfg, vbd_sweep_pipe_kernel<TPV, RE, RB>, a)
                           : listed == 1 ? cudaLaunchKernelEx(&cfg, vbd_sweep_list_kernel<TPV, RE, RB>, a)
                                         : cudaLaunchKernelEx(&cfg, vbd_sweep_kernel<TPV, RE, RB>, a);
     if (e == cudaSuccess) count_launch(st);
@@ -1008,7 +1014,7 @@ int launch_sweep(ats_cloth* c, int color, cudaStream_t st, const int* active) {
     a.inst = c->inst.p;
     // with an activity mask: only the slices the last compaction listed (the mask
     // itself is what the compaction read)
-    const int listed = active != nullptr ? (c->list_pipe ? 2 : 1) : 0;
+    const int listed = active != nullptr ? 1 + c->list_form : 0;
     a.active = nullptr;  // masked sweeps go through the lists
     a.list = listed ? c->act_list.p + sb : nullptr;
     a.list_count = listed ? c->act_count.p + color : nullptr;
@@ -1018,7 +1024,7 @@ int launch_sweep(ats_cloth* c, int color, cudaStream_t st, const int* active) {
     a.h2inv = c->h2inv;
     const int warps_per_block = c->block / 32;
     int blocks = (se - sb + warps_per_block - 1) / warps_per_block;
-    if (listed) blocks = std::min(blocks, list_sweep_ctas(c->L.tpv, c->block, c->list_pipe));
+    if (listed) blocks = std::min(blocks, list_sweep_ctas(c->L.tpv, c->block, c->list_form));
     const dim3 grid(blocks), block(c->block);
     cudaError_t e;
     switch (c->L.tpv) {
@@ -1506,7 +1512,7 @@ int frame_to_residual_impl(ats_cloth* c, double tol, const double* tols, const i
                                                   c->next_due.p, c->last_it.p, c->last_res.p); count_launch(st);
         ATS_CUDA(cudaGetLastError());
         if ((r = enqueue_compaction(c, st))) return r;
-        list_sweep_ctas(c->L.tpv, c->block, c->list_pipe);  // occupancy query before any capture
+        list_sweep_ctas(c->L.tpv, c->block, c->list_form);  // occupancy query before any capture
         // one chunk (graphs) per probe point; the host looks at the number of active
         // instances only every kProbesPerSync points, so it rarely waits on the device
         constexpr int kProbesPerSync = 4;
@@ -1564,13 +1570,13 @@ int ats_set_sweep_form(ats_cloth* c, int solver, int form) {
     return ATS_OK;
 }
 
-int ats_set_list_sweep(ats_cloth* c, int pipelined) {
-    if (!c || (pipelined != 0 && pipelined != 1)) {
-        set_error("ats_set_list_sweep: need a handle and 0 (plain) or 1 (pipelined)");
+int ats_set_list_sweep(ats_cloth* c, int form) {
+    if (!c || form < 0 || form > 2) {
+        set_error("ats_set_list_sweep: need a handle and 0 (plain), 1 (pipelined) or 2 (streamed)");
         return ATS_ERR_INVALID;
     }
-    c->list_pipe = pipelined;
-    list_sweep_ctas(c->L.tpv, c->block, pipelined);  // shared-memory attributes, outside any capture
+    c->list_form = form;
+    list_sweep_ctas(c->L.tpv, c->block, form);  // shared-memory attributes, outside any capture
     c->drop_graphs();
     return ATS_OK;
 }
@@ -1738,7 +1744,7 @@ int ats_cloth_query(const ats_cloth* c, ats_cloth_info* info) {
     info->device_bytes = (long long)c->device_bytes();
     info->vbd_form = c->vbd_loop_blocks > 0 ? 1 : 0;
     info->xpbd_form = c->xpbd_loop_blocks > 0 ? 1 : 0;
-    info->list_form = c->list_pipe;
+    info->list_form = c->list_form;
     return ATS_OK;
 }
 
@@ -2031,16 +2037,16 @@ int ats_autotune(ats_cloth* c, int iterations, ats_stream stream, int* out_tpv, 
             if (r || ms >= best) c->vbd_loop_blocks = 0;
         }
     }
-    // the list sweep of the residual-driven frames, plain or pipelined, over every
-    // instance's slices (all instances active): the fastest of three timings each
+    // the list sweep of the residual-driven frames, plain, pipelined or streamed, over
+    // every instance's slices (all instances active): the fastest of three timings each
     if (!r && c->L.ninst > 0) {
         std::vector<int> ones(c->L.ninst, 1);
         ATS_CUDA(cudaMemcpyAsync(c->active.p, ones.data(), ones.size() * sizeof(int), cudaMemcpyHostToDevice, st));
         if (!(r = enqueue_compaction(c, st))) {
-            float t_form[2] = {1e30f, 1e30f};
-            for (int pipe = 0; pipe < 2 && !r; ++pipe) {
-                c->list_pipe = pipe;
-                list_sweep_ctas(c->L.tpv, c->block, pipe);
+            float t_form[3] = {1e30f, 1e30f, 1e30f};
+            for (int form = 0; form < 3 && !r; ++form) {
+                c->list_form = form;
+                list_sweep_ctas(c->L.tpv, c->block, form);
                 if ((r = enqueue_iterations(c, ATS_SOLVER_VBD, 1, st, c->active.p))) break;
                 for (int rep = 0; rep < 3; ++rep) {
                     cudaEventRecord(e0, st);
@@ -2053,10 +2059,12 @@ int ats_autotune(ats_cloth* c, int iterations, ats_stream stream, int* out_tpv, 
                     }
                     float t = 0.f;
                     cudaEventElapsedTime(&t, e0, e1);
-                    t_form[pipe] = std::min(t_form[pipe], t);
+                    t_form[form] = std::min(t_form[form], t);
                 }
             }
-            c->list_pipe = !r && t_form[1] < t_form[0] ? 1 : 0;
+            c->list_form = 0;
+            for (int form = 1; form < 3 && !r; ++form)
+                if (t_form[form] < t_form[c->list_form]) c->list_form = form;
         }
         ATS_CUDA(cudaStreamSynchronize(st));  // the host vector leaves scope
     }

@@ -80,7 +80,7 @@ struct ats_cloth {
     int xpbd_loop_capable = 0;           // co-resident blocks of the persistent XPBD kernel (0: unavailable)
     int xpbd_loop_blocks = 0;            // the blocks XPBD frames launch it with (0: per-colour launches)
     int vbd_loop_blocks = 0;             // the same for VBD iterations (0: one launch per colour; set by autotune)
-    int list_pipe = 0;                   // list sweep of residual-driven frames: 0 plain, 1 pipelined
+    int list_form = 0;                   // list sweep of residual-driven frames: 0 plain, 1 pipelined, 2 streamed
     DevBuf<int2> en_edge;
     DevBuf<float> en_rest, en_k, en_q, en_kb;
     DevBuf<int4> en_bend;

@@ -258,11 +258,24 @@ __global__ void __launch_bounds__(256) vbd_sweep_kernel(SweepArgs a) {
     sweep_vertex<TPV, RE, RB>(a, v, leader, base, bbase, erows, brows, xv, xe, le, we, xb, wb, ks, ip, mv, p0, vv);
 }
 
-// One slice of a sweep: every vertex of the slice (its constant data, then all
-// neighbour positions at once, then the solve). M chooses how positions are accessed.
-template <int TPV, int RE, int RB, class M>
-__device__ __forceinline__ void sweep_slice(const SweepArgs& a, int slice, int lane) {
-    const int4 sd = __ldg(&a.slices[slice]);
+// Loads of the data a sweep reads once per iteration and never writes (stencil rows,
+// rest lengths, vertex records, frame-start state): through the read-only path, or
+// as streaming loads (ld.global.cs: evict-first in L1 and L2), which leave L2 to
+// the positions that every colour's sweep gathers again.
+struct ConstLoads {
+    template <class T>
+    static __device__ __forceinline__ T ld(const T* p) { return __ldg(p); }
+};
+struct StreamLoads {
+    template <class T>
+    static __device__ __forceinline__ T ld(const T* p) { return __ldcs(p); }
+};
+
+// One slice of a sweep (descriptor sd): every vertex of the slice (its constant data,
+// then all neighbour positions at once, then the solve). M chooses how positions are
+// accessed, LD how the per-iteration constant data is loaded.
+template <int TPV, int RE, int RB, class M, class LD = ConstLoads>
+__device__ __forceinline__ void sweep_slice_sd(const SweepArgs& a, int4 sd, int lane) {
     const int rows = sd.w & 0xffff, erows = sd.w >> 16, brows = rows - erows;
     const int k = lane / TPV;
     const bool leader = k < sd.y && (lane % TPV) == 0;
@@ -277,10 +290,10 @@ __device__ __forceinline__ void sweep_slice(const SweepArgs& a, int slice, int l
         we[r] = 0.f;
         le[r] = -1.f;
         if (r < erows) {
-            const int2 iw = __ldg(&a.st_iw[base + r * 32]);
+            const int2 iw = LD::ld(&a.st_iw[base + r * 32]);
             ue[r] = iw.x;
             we[r] = __int_as_float(iw.y);
-            le[r] = __ldg(&a.st_rest[base + r * 32]);
+            le[r] = LD::ld(&a.st_rest[base + r * 32]);
         }
     }
 #pragma unroll
@@ -288,12 +301,12 @@ __device__ __forceinline__ void sweep_slice(const SweepArgs& a, int slice, int l
         ub[r] = v;
         wb[r] = 0.f;
         if (r < brows) {
-            const int2 iw = __ldg(&a.st_iw[bbase + r * 32]);
+            const int2 iw = LD::ld(&a.st_iw[bbase + r * 32]);
             ub[r] = iw.x;
             wb[r] = __int_as_float(iw.y);
         }
     }
-    const float4 mv = __ldg(&a.vm[v]);
+    const float4 mv = LD::ld(&a.vm[v]);
     const float4 ip = __ldg(&a.inst[__float_as_int(mv.w)]);
     const float4 xv = M::ld(&a.x[v]);
     float4 xe[RE], xb[RB];
@@ -303,11 +316,16 @@ __device__ __forceinline__ void sweep_slice(const SweepArgs& a, int slice, int l
     for (int r = 0; r < RB; ++r) xb[r] = M::ld(&a.x[ub[r]]);
     float4 p0 = make_float4(0.f, 0.f, 0.f, 0.f), vv = p0;
     if (leader) {
-        p0 = a.x0[v];
-        vv = a.vel[v];
+        p0 = LD::ld(&a.x0[v]);
+        vv = LD::ld(&a.vel[v]);
     }
     sweep_vertex<TPV, RE, RB, M>(a, v, leader, base, bbase, erows, brows, xv, xe, le, we, xb, wb, ip.w, ip, mv, p0,
                                  vv);
+}
+
+template <int TPV, int RE, int RB, class M>
+__device__ __forceinline__ void sweep_slice(const SweepArgs& a, int slice, int lane) {
+    sweep_slice_sd<TPV, RE, RB, M>(a, __ldg(&a.slices[slice]), lane);
 }
 
 // ---------------------------------------------------------------- pipelined list sweep
@@ -450,6 +468,34 @@ __global__ void __launch_bounds__(256) vbd_sweep_list_kernel(SweepArgs a) {
     const int count = *a.list_count;
     for (int idx = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); idx < count; idx += nwarps)
         sweep_slice<TPV, RE, RB, PlainMem>(a, a.list[idx], lane);
+}
+
+// The list sweep with streaming loads for the per-iteration constant data and the
+// next slice's descriptor in flight while the current slice computes: a warp loads
+// the list entry two slices ahead and the descriptor one slice ahead, so the chain
+// in front of each slice's neighbour gathers is its stencil rows alone.
+template <int TPV, int RE, int RB>
+__global__ void __launch_bounds__(256) vbd_sweep_stream_kernel(SweepArgs a) {
+    grid_dependency_wait();  // the list and the positions come from the kernels before
+    allow_dependent_launch();
+    const int lane = threadIdx.x & 31;
+    const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
+    const int count = *a.list_count;
+    int idx = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (idx >= count) return;
+    int4 sd = __ldg(&a.slices[a.list[idx]]);
+    int next = idx + nwarps < count ? a.list[idx + nwarps] : 0;
+    for (;;) {
+        const bool more = idx + nwarps < count;
+        int4 sd_next = sd;
+        if (more) sd_next = __ldg(&a.slices[next]);
+        const int after = idx + 2 * nwarps < count ? a.list[idx + 2 * nwarps] : 0;
+        sweep_slice_sd<TPV, RE, RB, PlainMem, StreamLoads>(a, sd, lane);
+        if (!more) break;
+        idx += nwarps;
+        sd = sd_next;
+        next = after;
+    }
 }
 
 }  // namespace ats

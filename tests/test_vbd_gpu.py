@@ -469,16 +469,18 @@ def test_persistent_vbd_frames_equal_per_colour_launches(ats, n):
 
 
 @pytest.mark.parametrize("tpv", [1, 2, 4, 8])
-def test_pipelined_list_sweep_equals_plain(ats, tpv):
-    """The residual-driven frames' sweep, plain and pipelined (each warp stages its next
-    slice in shared memory while computing the current one): the same slices and the
-    same arithmetic, so bit-identical positions; with some instances stopping early."""
+@pytest.mark.parametrize("form", [1, 2])
+def test_list_sweep_forms_equal_plain(ats, tpv, form):
+    """The residual-driven frames' sweep, plain against pipelined (each warp stages its
+    next slice in shared memory while computing the current one) and streamed
+    (evict-first loads, next descriptor in flight): the same slices and the same
+    arithmetic, so bit-identical positions; with some instances stopping early."""
     insts, prm = configs.c2(num_instances=5, seed=3, side_range=(20, 90))
     a = ats.Cloth(insts, threads_per_vertex=tpv, block_size=128, **prm)
     b = ats.Cloth(insts, threads_per_vertex=tpv, block_size=128, **prm)
     a.set_list_sweep(0)
-    b.set_list_sweep(1)
-    assert a.info.list_form == 0 and b.info.list_form == 1
+    b.set_list_sweep(form)
+    assert a.info.list_form == 0 and b.info.list_form == form
     for f in range(4):
         tol = 0.0 if f % 2 == 0 else 0.35
         ia, ra = a.frame_to_residual(tol, check_every=5, max_iterations=15)
