@@ -312,6 +312,13 @@ def maxrank(v):
     return float(sharding.allreduce_stats([float(v)], op="max")[0])
 
 
+# DRAM traffic over algorithmic bytes of the list sweeps, per launch: ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum, 3 launches, --clock-control none) on the
+# 32-instance c4 case, 1 lane per vertex, 64 threads per block: 216.9 MB (plain) and
+# 209.0 MB (streamed) against 214.0 MB algorithmic.
+SWEEP_TRAFFIC_RATIO = {"vbd_sweep_list_kernel<1>": 1.013, "vbd_sweep_stream_kernel<1>": 0.977}
+
+
 def sweep_roofline(cloth, stream, reps=3, iters=50):
     """Per-launch time of vbd_sweep_list_kernel: `iters` listed iterations over every
     instance (a to-residual frame with tol 0 and one probe at the cap), CUDA-event
@@ -470,6 +477,8 @@ def run_learned(args):
 
     # sweep roofline in this run (listed sweep over all instances)
     per_launch, rf_frame_ms, bytes_launch = sweep_roofline(cloth, stream)
+    sweep_kernel = (("vbd_sweep_list_kernel", "vbd_sweep_pipe_kernel", "vbd_sweep_stream_kernel")[info.list_form]
+                    + f"<{info.threads_per_vertex}>")
     peak, peak_src = hbm_peak()
     achieved = bytes_launch / (per_launch * 1e-3) / 1e9
     sweeps_per_learned_frame = float(np.mean(res["learned_iters"].max(axis=1))) * info.num_vertex_colors
@@ -554,11 +563,15 @@ def run_learned(args):
                        "path": "ats_set_state from pinned host, ats_frame_warm_to_residual, ats_get_state to pinned "
                                "host; wall clock"},
                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                            "frac": achieved / peak, "traffic": None,
-                            "traffic_note": "not captured in this run; the committed ncu summaries under profiles/ "
-                                            "hold the DRAM bytes of this kernel",
-                            "kernel": ("vbd_sweep_list_kernel", "vbd_sweep_pipe_kernel",
-                                       "vbd_sweep_stream_kernel")[info.list_form] + f"<{info.threads_per_vertex}>",
+                            "frac": achieved / peak,
+                            "traffic": (SWEEP_TRAFFIC_RATIO[sweep_kernel] * bytes_launch
+                                        if sweep_kernel in SWEEP_TRAFFIC_RATIO else None),
+                            "traffic_source": ("not captured in this run: DRAM bytes read + written per launch from "
+                                               "an ncu capture of the 32-instance c4 case (3,528,428 vertices, "
+                                               "214.0 MB algorithmic per launch), scaled to this launch by its "
+                                               "algorithmic bytes" if sweep_kernel in SWEEP_TRAFFIC_RATIO
+                                               else "no capture of this kernel"),
+                            "kernel": sweep_kernel,
                             "us_per_launch_upper_bound": per_launch * 1e3, "alg_bytes_per_launch": bytes_launch,
                             "timing": "50 listed iterations over all instances, CUDA events, predict/update/2 probes "
                                       "included", "peak_source": peak_src,

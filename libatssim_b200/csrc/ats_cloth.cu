@@ -243,43 +243,43 @@ __global__ void xpbd_bending_kernel(float4* __restrict__ x, const float4* __rest
 }
 
 // Grid-wide barrier of the persistent kernels, whose blocks are co-resident (a
-// cooperative launch). bar[0] counts arrivals, bar[1] is the generation. Thread 0 of
-// every block reads the generation, publishes the block's writes (device-scope fence)
-// and arrives; the last arrival resets the count and advances the generation, the
-// others poll it with acquire loads (back to back for the first kBarrierFastPolls,
-// then with a short sleep). The wait is bounded: after kBarrierSpins polls it sets
-// *err, and every block leaves the kernel at its next barrier. Returns false on error.
+// cooperative launch). bar[0] counts the arrivals since the launch (set to 0 before
+// it); barrier k of the launch is passed once the count reaches k * gridDim.x, which
+// each block tracks in `target`, so an arrival is one atomic and nothing is reset.
+// Thread 0 of every block publishes the block's writes (device-scope fence), arrives,
+// and polls the count with acquire loads (back to back for the first
+// kBarrierFastPolls, then with a short sleep). The wait is bounded: after
+// kBarrierSpins polls the block sets bit 31 of the count (kBarrierError) and *err,
+// and every block leaves the kernel at its next poll. Returns false on error. The
+// host keeps every launch below 2^31 arrivals (kMaxLoopArrivals).
 constexpr unsigned kBarrierSpins = 1u << 24;
 constexpr unsigned kBarrierFastPolls = 1u << 12;
+constexpr unsigned kBarrierError = 0x80000000u;
+constexpr unsigned long long kMaxLoopArrivals = 0x7fffffffull;
 __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
     unsigned v;
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
-__device__ __forceinline__ bool grid_barrier(unsigned* bar, int* err, unsigned nblocks) {
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, int* err, unsigned& target) {
     __shared__ int s_ok;
+    target += gridDim.x;
     __syncthreads();
     if (threadIdx.x == 0) {
-        const unsigned my_gen = ld_acquire_gpu(bar + 1);
         __threadfence();
-        const unsigned arrived = atomicAdd(bar, 1u);
-        if (arrived == nblocks - 1) {
-            atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
-        } else {
-            unsigned spins = 0;
-            while (ld_acquire_gpu(bar + 1) == my_gen) {
-                ++spins;
-                if ((spins & 1023u) == 0 && (spins > kBarrierSpins || *(volatile int*)err)) {
-                    atomicExch(err, 1);
-                    break;
-                }
-                if (spins > kBarrierFastPolls) __nanosleep(64);
+        unsigned v = atomicAdd(bar, 1u) + 1u;
+        unsigned spins = 0;
+        while ((v & ~kBarrierError) < target && !(v & kBarrierError)) {
+            if (++spins > kBarrierSpins) {
+                v = atomicOr(bar, kBarrierError) | kBarrierError;
+                atomicExch(err, 1);
+                break;
             }
+            if (spins > kBarrierFastPolls) __nanosleep(64);
+            v = ld_acquire_gpu(bar);
         }
         __threadfence();
-        s_ok = *(volatile int*)err == 0;
+        s_ok = !(v & kBarrierError);
     }
     __syncthreads();
     return s_ok != 0;
@@ -298,11 +298,12 @@ __global__ void __launch_bounds__(256) vbd_loop_kernel(SweepArgs a, const int* _
     const int lane = threadIdx.x & 31;
     const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
     const int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    unsigned target = 0;
     for (int it = 0; it < iterations; ++it)
         for (int c = 0; c < ncolors; ++c) {
             const int b = __ldg(&color_slices[c]), e = __ldg(&color_slices[c + 1]);
             for (int slice = b + w; slice < e; slice += nwarps) sweep_slice<TPV, RE, RB, L2Mem>(a, slice, lane);
-            if (!grid_barrier(bar, err, gridDim.x)) return;
+            if (!grid_barrier(bar, err, target)) return;
         }
 }
 
@@ -346,6 +347,7 @@ __global__ void __launch_bounds__(kXpbdLoopThreads, 1) xpbd_loop_kernel(XpbdLoop
     };
     StretchConst sc = {};
     BendConst bc = {};
+    unsigned target = 0;
     int b, e;
     range(0, b, e);
     if (b + t < e) {
@@ -375,7 +377,7 @@ __global__ void __launch_bounds__(kXpbdLoopThreads, 1) xpbd_loop_kernel(XpbdLoop
                     else bc = load_bend(nb + t, a.vm, a.bidx, a.bq);
                 }
             }
-            if (!grid_barrier(a.bar, a.err, gridDim.x)) return;
+            if (!grid_barrier(a.bar, a.err, target)) return;
         }
     }
 }
@@ -1098,6 +1100,8 @@ int launch_xpbd_bending(ats_cloth* c, int color, cudaStream_t st) {
 
 // `iterations` XPBD iterations as one cooperative launch of xpbd_loop_kernel (one
 // block per SM), the barrier state reset on the stream first.
+int launch_xpbd_loop_once(ats_cloth* c, const XpbdLoopArgs& a, cudaStream_t st);
+
 int launch_xpbd_loop(ats_cloth* c, int iterations, cudaStream_t st) {
     XpbdLoopArgs a;
     a.x = c->x.p;
@@ -1113,10 +1117,27 @@ int launch_xpbd_loop(ats_cloth* c, int iterations, cudaStream_t st) {
     a.bcolor = c->xb_color_d.p;
     a.nsc = c->L.n_scolors;
     a.nbc = c->L.n_bcolors;
-    a.iterations = iterations;
     a.h = c->h;
     a.bar = c->loop_bar.p;
     a.err = c->loop_err.p;
+    // at most kMaxLoopArrivals barrier arrivals per launch
+    const unsigned long long per_it =
+        std::max(1ull, (unsigned long long)(a.nsc + a.nbc) * (unsigned long long)c->xpbd_loop_blocks);
+    const int max_it = (int)std::min<unsigned long long>(kMaxLoopArrivals / per_it, 1ull << 30);
+    if (max_it < 1) {
+        set_error("xpbd loop: too many colours x blocks for one launch");
+        return ATS_ERR_INVALID;
+    }
+    for (int done = 0; done < iterations;) {
+        a.iterations = std::min(iterations - done, max_it);
+        done += a.iterations;
+        const int r = launch_xpbd_loop_once(c, a, st);
+        if (r) return r;
+    }
+    return ATS_OK;
+}
+
+int launch_xpbd_loop_once(ats_cloth* c, const XpbdLoopArgs& a, cudaStream_t st) {
     ATS_CUDA(cudaMemsetAsync(c->loop_bar.p, 0, 2 * sizeof(unsigned), st));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(c->xpbd_loop_blocks);
@@ -1150,6 +1171,8 @@ int vbd_loop_blocks(int tpv, int block, int device) {
     return coop && e == cudaSuccess && per_sm > 0 ? sms * per_sm : 0;
 }
 
+int launch_vbd_loop_once(ats_cloth* c, const SweepArgs& a, const int* cs, int nc, int iterations, cudaStream_t st);
+
 int launch_vbd_loop(ats_cloth* c, int iterations, cudaStream_t st) {
     SweepArgs a;
     a.x = c->x.p;
@@ -1168,6 +1191,25 @@ int launch_vbd_loop(ats_cloth* c, int iterations, cudaStream_t st) {
     a.slice_end = (int)c->slices.n;
     a.h = c->h;
     a.h2inv = c->h2inv;
+    const int* cs = c->color_slices.p;
+    const int nc = c->L.n_vcolors;
+    // at most kMaxLoopArrivals barrier arrivals per launch
+    const unsigned long long per_it = std::max(1ull, (unsigned long long)nc * (unsigned long long)c->vbd_loop_blocks);
+    const int max_it = (int)std::min<unsigned long long>(kMaxLoopArrivals / per_it, 1ull << 30);
+    if (max_it < 1) {
+        set_error("vbd loop: too many colours x blocks for one launch");
+        return ATS_ERR_INVALID;
+    }
+    for (int done = 0; done < iterations;) {
+        const int n = std::min(iterations - done, max_it);
+        done += n;
+        const int r = launch_vbd_loop_once(c, a, cs, nc, n, st);
+        if (r) return r;
+    }
+    return ATS_OK;
+}
+
+int launch_vbd_loop_once(ats_cloth* c, const SweepArgs& a, const int* cs, int nc, int iterations, cudaStream_t st) {
     ATS_CUDA(cudaMemsetAsync(c->loop_bar.p, 0, 2 * sizeof(unsigned), st));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(c->vbd_loop_blocks);
@@ -1179,8 +1221,6 @@ int launch_vbd_loop(ats_cloth* c, int iterations, cudaStream_t st) {
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    const int* cs = c->color_slices.p;
-    const int nc = c->L.n_vcolors;
     cudaError_t e;
     switch (c->L.tpv) {
         case 1: e = cudaLaunchKernelEx(&cfg, vbd_loop_kernel<1, 6, 6>, a, cs, nc, iterations, c->loop_bar.p, c->loop_err.p); break;
