@@ -1304,13 +1304,11 @@ int segment_sum(ats_cloth* c, const double* per_vertex, double* out, int take_sq
 // cancelling at the residuals those frames stop at, so FP32 terms (as the reference
 // energy's) lose nothing there, and this kernel needs half the registers of the FP64
 // one.
+// One slice; the data read once per probe (stencil rows, vertex records, frame-start
+// state) through evict-first loads.
 template <int TPV, int RE, int RB>
-__global__ void __launch_bounds__(128) stencil_grad32_kernel(EvalArgs a, float h, float h2inv) {
-    const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-    if (warp >= a.nslices) return;
-    const int lane = threadIdx.x & 31;
-    if (a.active && !a.active[__ldg(&a.slice_inst[warp])]) return;  // warp-uniform
-    const int4 sd = __ldg(&a.slices[warp]);
+__device__ __forceinline__ void grad32_slice(const EvalArgs& a, int slice, int lane, float h, float h2inv) {
+    const int4 sd = __ldg(&a.slices[slice]);
     const int rows = sd.w & 0xffff, erows = sd.w >> 16, brows = rows - erows;
     const int k = lane / TPV;
     const bool leader = k < sd.y && (lane % TPV) == 0;
@@ -1325,10 +1323,10 @@ __global__ void __launch_bounds__(128) stencil_grad32_kernel(EvalArgs a, float h
         we[r] = 0.f;
         le[r] = -1.f;
         if (r < erows) {
-            const int2 iw = __ldg(&a.st_iw[base + r * 32]);
+            const int2 iw = __ldcs(&a.st_iw[base + r * 32]);
             ue[r] = iw.x;
             we[r] = __int_as_float(iw.y);
-            le[r] = __ldg(&a.st_rest[base + r * 32]);
+            le[r] = __ldcs(&a.st_rest[base + r * 32]);
         }
     }
 #pragma unroll
@@ -1336,12 +1334,12 @@ __global__ void __launch_bounds__(128) stencil_grad32_kernel(EvalArgs a, float h
         ub[r] = v;
         wb[r] = 0.f;
         if (r < brows) {
-            const int2 iw = __ldg(&a.st_iw[bbase + r * 32]);
+            const int2 iw = __ldcs(&a.st_iw[bbase + r * 32]);
             ub[r] = iw.x;
             wb[r] = __int_as_float(iw.y);
         }
     }
-    const float4 mv = __ldg(&a.vm[v]);
+    const float4 mv = __ldcs(&a.vm[v]);
     const float4 ip = __ldg(&a.inst[__float_as_int(mv.w)]);
     const float4 xv = a.x[v];
     float4 xe[RE], xb[RB];
@@ -1374,7 +1372,7 @@ __global__ void __launch_bounds__(128) stencil_grad32_kernel(EvalArgs a, float h
         a.out0[v] = 0.0;
         return;
     }
-    const float4 p0 = a.x0[v], vv = a.vel[v];
+    const float4 p0 = __ldcs(&a.x0[v]), vv = __ldcs(&a.vel[v]);
     const float m = p0.w, mh = m * h2inv;
     fx += -mh * ((xv.x - p0.x) - vv.x * h) + m * ip.x;
     fy += -mh * ((xv.y - p0.y) - vv.y * h) + m * ip.y;
@@ -1382,12 +1380,52 @@ __global__ void __launch_bounds__(128) stencil_grad32_kernel(EvalArgs a, float h
     a.out0[v] = (double)fx * fx + (double)fy * fy + (double)fz * fz;
 }
 
+// The probe over a resident grid: warp w takes slices w, w + nwarps, ...; lane j of a
+// round looks up whether the round's j-th slice belongs to an instance being probed,
+// and the warp then runs those slices only. A probe of few instances costs a couple of
+// loads per warp instead of a CTA per slice.
+template <int TPV, int RE, int RB>
+__global__ void __launch_bounds__(128) stencil_grad32_kernel(EvalArgs a, float h, float h2inv) {
+    const int lane = threadIdx.x & 31;
+    const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
+    const int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    for (int round = w; round < a.nslices; round += 32 * nwarps) {
+        const int s = round + lane * nwarps;
+        const bool want = s < a.nslices && (!a.active || a.active[__ldg(&a.slice_inst[s])]);
+        unsigned m = __ballot_sync(0xffffffffu, want);
+        while (m) {
+            const int j = __ffs(m) - 1;
+            m &= m - 1;
+            grad32_slice<TPV, RE, RB>(a, round + j * nwarps, lane, h, h2inv);
+        }
+    }
+}
+
+// Resident CTAs of stencil_grad32_kernel, all SMs, per lanes per vertex (queried on
+// first use: the eager probe at the inertial guess comes before any capture).
+int grad32_ctas(int tpv) {
+    static int cache[4] = {};
+    const int ti = tpv == 1 ? 0 : tpv == 2 ? 1 : tpv == 4 ? 2 : 3;
+    if (!cache[ti]) {
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        switch (tpv) {
+            case 1: cache[ti] = resident_ctas(stencil_grad32_kernel<1, 6, 6>, 128, 0, sms); break;
+            case 2: cache[ti] = resident_ctas(stencil_grad32_kernel<2, 3, 3>, 128, 0, sms); break;
+            case 4: cache[ti] = resident_ctas(stencil_grad32_kernel<4, 2, 2>, 128, 0, sms); break;
+            default: cache[ti] = resident_ctas(stencil_grad32_kernel<8, 1, 1>, 128, 0, sms); break;
+        }
+    }
+    return cache[ti];
+}
+
 int enqueue_residual_norms(ats_cloth* c, cudaStream_t st, const int* active, bool fp32_terms) {
     EvalArgs a = eval_args(c);
     a.active = active;
     a.out0 = c->g2.p;
     if (fp32_terms) {
-        const int blocks = (a.nslices * 32 + 127) / 128;
+        const int blocks = std::min((a.nslices * 32 + 127) / 128, grad32_ctas(c->L.tpv));
         if (blocks > 0) {
             switch (c->L.tpv) {
                 case 1: stencil_grad32_kernel<1, 6, 6><<<blocks, 128, 0, st>>>(a, c->h, c->h2inv); count_launch(st); break;
