@@ -571,6 +571,19 @@ __global__ void __launch_bounds__(kRedThreads) sum_partials3_kernel(const double
 // kEvalGradF32 (stencil_grad32_kernel) is kEvalGrad with the per-vertex gradient in
 // the sweep's own FP32 arithmetic; only the sum over vertices is FP64.
 constexpr int kEvalGrad = 0, kEvalPot = 1, kEvalPotPair = 2;
+// Resident CTAs of `kernel` at `block` threads and `smem` bytes of dynamic shared
+// memory, all SMs together (the grid of the kernels that stride over their work).
+template <typename K>
+int resident_ctas(K kernel, int block, size_t smem, int sms) {
+    int res = 0;
+    if (smem > 0) {
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
+    }
+    const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&res, kernel, block, smem);
+    return std::max(1, sms) * (e == cudaSuccess && res > 0 ? res : 1);
+}
+
 struct EvalArgs {
     const float4* x;
     const float4* y;  // kEvalPotPair only
@@ -623,21 +636,18 @@ __device__ __forceinline__ void eval_row(float4 xv, float4 xu, float4 yv, float4
     }
 }
 
+// One slice of an FP64 stencil pass; the data read once per pass (stencil rows, vertex
+// records, frame-start state) through evict-first loads.
 template <int TPV, int RE, int RB, int MODE>
-__global__ void __launch_bounds__(128) stencil_eval_kernel(EvalArgs a) {
-    const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-    if (warp >= a.nslices) return;
-    const int lane = threadIdx.x & 31;
-    // a slice belongs to one instance, so this exit is warp-uniform
-    if (a.active && !a.active[__ldg(&a.slice_inst[warp])]) return;
-    const int4 sd = __ldg(&a.slices[warp]);
+__device__ __forceinline__ void eval_slice(const EvalArgs& a, int slice, int lane) {
+    const int4 sd = __ldg(&a.slices[slice]);
     const int rows = sd.w & 0xffff, erows = sd.w >> 16, brows = rows - erows;
     const int k = lane / TPV;
     const bool leader = k < sd.y && (lane % TPV) == 0;
     const int v = sd.x + min(k, sd.y - 1);
     const int base = sd.z + lane;
     const int bbase = base + erows * 32;
-    const float4 mv = __ldg(&a.vm[v]);
+    const float4 mv = __ldcs(&a.vm[v]);
     int ue[RE], ub[RB];
     float we[RE], le[RE], wb[RB];
 #pragma unroll
@@ -646,10 +656,10 @@ __global__ void __launch_bounds__(128) stencil_eval_kernel(EvalArgs a) {
         we[r] = 0.f;
         le[r] = -1.f;
         if (r < erows) {
-            const int2 iw = __ldg(&a.st_iw[base + r * 32]);
+            const int2 iw = __ldcs(&a.st_iw[base + r * 32]);
             ue[r] = iw.x;
             we[r] = __int_as_float(iw.y);
-            le[r] = __ldg(&a.st_rest[base + r * 32]);
+            le[r] = __ldcs(&a.st_rest[base + r * 32]);
         }
     }
 #pragma unroll
@@ -657,7 +667,7 @@ __global__ void __launch_bounds__(128) stencil_eval_kernel(EvalArgs a) {
         ub[r] = v;
         wb[r] = 0.f;
         if (r < brows) {
-            const int2 iw = __ldg(&a.st_iw[bbase + r * 32]);
+            const int2 iw = __ldcs(&a.st_iw[bbase + r * 32]);
             ub[r] = iw.x;
             wb[r] = __int_as_float(iw.y);
         }
@@ -700,20 +710,20 @@ __global__ void __launch_bounds__(128) stencil_eval_kernel(EvalArgs a) {
         a2 += __shfl_xor_sync(0xffffffffu, a2, o);
     }
     if (!leader) return;
-    const float4 p0 = a.x0[v];
+    const float4 p0 = __ldcs(&a.x0[v]);
     const double h = a.h, m = p0.w;
     if (MODE == kEvalGrad) {
         if (mv.y != 0.f) {
             a.out0[v] = 0.0;
             return;
         }
-        const float4 vv = a.vel[v];
+        const float4 vv = __ldcs(&a.vel[v]);
         a0 += m / (h * h) * ((double)xv.x - ((double)p0.x + h * vv.x + h * h * ip.x));
         a1 += m / (h * h) * ((double)xv.y - ((double)p0.y + h * vv.y + h * h * ip.y));
         a2 += m / (h * h) * ((double)xv.z - ((double)p0.z + h * vv.z + h * h * ip.z));
         a.out0[v] = a0 * a0 + a1 * a1 + a2 * a2;
     } else if (MODE == kEvalPot) {
-        const float4 vv = a.vel[v];
+        const float4 vv = __ldcs(&a.vel[v]);
         const bool pinned = mv.y != 0.f;
         const double ax = pinned ? 0.0 : ip.x, ay = pinned ? 0.0 : ip.y, az = pinned ? 0.0 : ip.z;
         const double dx = (double)xv.x - ((double)p0.x + h * vv.x + h * h * ax);
@@ -727,16 +737,49 @@ __global__ void __launch_bounds__(128) stencil_eval_kernel(EvalArgs a) {
     }
 }
 
+// An FP64 stencil pass over a resident grid, slices taken as in stencil_grad32_kernel:
+// warp w takes slices w, w + nwarps, ..., and runs those of active instances only.
+template <int TPV, int RE, int RB, int MODE>
+__global__ void __launch_bounds__(128) stencil_eval_kernel(EvalArgs a) {
+    const int lane = threadIdx.x & 31;
+    const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
+    const int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    for (int round = w; round < a.nslices; round += 32 * nwarps) {
+        const int s = round + lane * nwarps;
+        const bool want = s < a.nslices && (!a.active || a.active[__ldg(&a.slice_inst[s])]);
+        unsigned m = __ballot_sync(0xffffffffu, want);
+        while (m) {
+            const int j = __ffs(m) - 1;
+            m &= m - 1;
+            eval_slice<TPV, RE, RB, MODE>(a, round + j * nwarps, lane);
+        }
+    }
+}
+
+// Resident CTAs of stencil_eval_kernel<..., MODE>, all SMs (queried on first use).
+template <int TPV, int RE, int RB, int MODE>
+int eval_ctas() {
+    static int n = 0;
+    if (!n) {
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        n = resident_ctas(stencil_eval_kernel<TPV, RE, RB, MODE>, 128, 0, sms);
+    }
+    return n;
+}
+
 template <int MODE>
 cudaError_t stencil_eval_launch(int tpv, const EvalArgs& a, cudaStream_t st) {
     const int blocks = (a.nslices * 32 + 127) / 128;
     if (blocks == 0) return cudaSuccess;
     switch (tpv) {
-        case 1: stencil_eval_kernel<1, 6, 6, MODE><<<blocks, 128, 0, st>>>(a); count_launch(st); break;
-        case 2: stencil_eval_kernel<2, 3, 3, MODE><<<blocks, 128, 0, st>>>(a); count_launch(st); break;
-        case 4: stencil_eval_kernel<4, 2, 2, MODE><<<blocks, 128, 0, st>>>(a); count_launch(st); break;
-        default: stencil_eval_kernel<8, 1, 1, MODE><<<blocks, 128, 0, st>>>(a); count_launch(st); break;
+        case 1: stencil_eval_kernel<1, 6, 6, MODE><<<std::min(blocks, eval_ctas<1, 6, 6, MODE>()), 128, 0, st>>>(a); break;
+        case 2: stencil_eval_kernel<2, 3, 3, MODE><<<std::min(blocks, eval_ctas<2, 3, 3, MODE>()), 128, 0, st>>>(a); break;
+        case 4: stencil_eval_kernel<4, 2, 2, MODE><<<std::min(blocks, eval_ctas<4, 2, 2, MODE>()), 128, 0, st>>>(a); break;
+        default: stencil_eval_kernel<8, 1, 1, MODE><<<std::min(blocks, eval_ctas<8, 1, 1, MODE>()), 128, 0, st>>>(a); break;
     }
+    count_launch(st);
     return cudaGetLastError();
 }
 
@@ -934,17 +977,6 @@ size_t pipe_smem_bytes(int tpv, int block) {
         case 4: return warps * pipe_smem_per_warp<2, 2>();
         default: return warps * pipe_smem_per_warp<1, 1>();
     }
-}
-
-template <typename K>
-int resident_ctas(K kernel, int block, size_t smem, int sms) {
-    int res = 0;
-    if (smem > 0) {
-        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
-    }
-    const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&res, kernel, block, smem);
-    return std::max(1, sms) * (e == cudaSuccess && res > 0 ? res : 1);
 }
 
 // Resident CTAs of the list sweeps (form 0: vbd_sweep_list_kernel, 1:
