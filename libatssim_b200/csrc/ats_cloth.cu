@@ -431,7 +431,8 @@ __global__ void scatter_state_kernel(const float* __restrict__ xc, const float* 
     float4 p = make_float4(xc[o], xc[o + 1], xc[o + 2], m);
     x0[i] = p;
     x[i] = make_float4(p.x, p.y, p.z, 0.f);
-    vel[i] = has_v ? make_float4(vc[o], vc[o + 1], vc[o + 2], 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float keep = vel[i].w;  // the bending diagonal stays
+    vel[i] = has_v ? make_float4(vc[o], vc[o + 1], vc[o + 2], keep) : make_float4(0.f, 0.f, 0.f, keep);
 }
 
 __global__ void gather_state_kernel(const float4* __restrict__ src, const int* __restrict__ to_caller,
@@ -921,7 +922,17 @@ int upload_stencil(ats_cloth* c) {
     // a slice lies in one instance: the instance id of its first vertex
     std::vector<int> si(L.slices.size() / 4);
     for (size_t k = 0; k < si.size(); ++k) std::memcpy(&si[k], &L.vm[4 * (size_t)L.slices[4 * k] + 3], sizeof(int));
-    if ((r = upload(c->slice_inst, si, si.size())) || (r = upload(c->color_slices, L.color_slices, L.color_slices.size())))
+    // and its pinned vertices (bit k: vertex vbegin + k), for the sweeps that skip vm
+    std::vector<int2> sm(si.size());
+    for (size_t k = 0; k < si.size(); ++k) {
+        unsigned pins = 0;
+        const int vb = L.slices[4 * k], nvs = L.slices[4 * k + 1];
+        for (int j = 0; j < nvs && j < 32; ++j)
+            if (L.vm[4 * (size_t)(vb + j) + 1] != 0.f) pins |= 1u << j;
+        sm[k] = make_int2(si[k], (int)pins);
+    }
+    if ((r = upload(c->slice_inst, si, si.size())) || (r = upload(c->slice_meta, sm, sm.size())) ||
+        (r = upload(c->color_slices, L.color_slices, L.color_slices.size())))
         return r;
     // per-colour lists of the slices still iterating (residual-driven frames)
     std::vector<int> zeros(std::max<size_t>(si.size(), 1), 0);
@@ -1045,6 +1056,7 @@ int launch_sweep(ats_cloth* c, int color, cudaStream_t st, const int* active) {
     a.st_rest = c->st_rest.p;
     a.slices = c->slices.p;
     a.slice_inst = c->slice_inst.p;
+    a.slice_meta = c->slice_meta.p;
     a.inst = c->inst.p;
     // with an activity mask: only the slices the last compaction listed (the mask
     // itself is what the compaction read)
@@ -1215,6 +1227,7 @@ int launch_vbd_loop(ats_cloth* c, int iterations, cudaStream_t st) {
     a.st_rest = c->st_rest.p;
     a.slices = c->slices.p;
     a.slice_inst = c->slice_inst.p;
+    a.slice_meta = c->slice_meta.p;
     a.inst = c->inst.p;
     a.active = nullptr;
     a.list = nullptr;

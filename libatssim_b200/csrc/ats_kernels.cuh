@@ -3,7 +3,7 @@
 // Data layout in HBM (float4 = 16 B, one 128-bit load per vertex record):
 //   x     [V]  current iterate, w unused
 //   x0    [V]  frame / substep start position, w = mass
-//   vel   [V]  velocity, w unused
+//   vel   [V]  velocity, w = the vertex's bending Hessian diagonal (a copy of vm.x)
 //   vm    [V]  {k_b * sum Q_oo (bending Hessian diagonal), pin boost (0 / 1e9), inverse mass, instance id bits}
 //   inst  [I]  per instance {external acceleration xyz, k_stretch}
 // Vertices are ordered instance-major then colour-major, so the vertices of one
@@ -24,6 +24,7 @@
 namespace ats {
 
 constexpr float kEps = 1.19209290E-7f;  // src/SharedDefine/constant_value.h:9
+constexpr float kPinBoost = 1e9f;       // Hessian boost of a pinned vertex (vm.y), xpbd_constraints.h:4058
 
 // Position access of the sweep and XPBD bodies: plain loads / stores in kernels that
 // end at each colour (a launch starts with a clean L1), L2-only ones in the persistent
@@ -46,6 +47,7 @@ struct SweepArgs {
     const float* __restrict__ st_rest;
     const int4* __restrict__ slices;
     const int* __restrict__ slice_inst;  // instance of each slice
+    const int2* __restrict__ slice_meta; // {instance, pinned-vertex bits} of each slice
     const float4* __restrict__ inst;
     const int* __restrict__ active;      // vbd_sweep_kernel: per instance, null = all active
     const int* __restrict__ list;        // vbd_sweep_list_kernel: this colour's active slices
@@ -273,9 +275,12 @@ struct StreamLoads {
 
 // One slice of a sweep (descriptor sd): every vertex of the slice (its constant data,
 // then all neighbour positions at once, then the solve). M chooses how positions are
-// accessed, LD how the per-iteration constant data is loaded.
-template <int TPV, int RE, int RB, class M, class LD = ConstLoads>
-__device__ __forceinline__ void sweep_slice_sd(const SweepArgs& a, int4 sd, int lane) {
+// accessed, LD how the per-iteration constant data is loaded. With META the material
+// record vm is not read: the instance and the pinned vertices come from the slice's
+// metadata meta = {instance, pinned bits}, the bending diagonal from vel.w (the same
+// values, 16 bytes less per vertex).
+template <int TPV, int RE, int RB, class M, class LD = ConstLoads, bool META = false>
+__device__ __forceinline__ void sweep_slice_sd(const SweepArgs& a, int4 sd, int lane, int2 meta = make_int2(0, 0)) {
     const int rows = sd.w & 0xffff, erows = sd.w >> 16, brows = rows - erows;
     const int k = lane / TPV;
     const bool leader = k < sd.y && (lane % TPV) == 0;
@@ -306,8 +311,9 @@ __device__ __forceinline__ void sweep_slice_sd(const SweepArgs& a, int4 sd, int 
             wb[r] = __int_as_float(iw.y);
         }
     }
-    const float4 mv = LD::ld(&a.vm[v]);
-    const float4 ip = __ldg(&a.inst[__float_as_int(mv.w)]);
+    float4 mv = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (!META) mv = LD::ld(&a.vm[v]);
+    const float4 ip = __ldg(&a.inst[META ? meta.x : __float_as_int(mv.w)]);
     const float4 xv = M::ld(&a.x[v]);
     float4 xe[RE], xb[RB];
 #pragma unroll
@@ -319,6 +325,7 @@ __device__ __forceinline__ void sweep_slice_sd(const SweepArgs& a, int4 sd, int 
         p0 = LD::ld(&a.x0[v]);
         vv = LD::ld(&a.vel[v]);
     }
+    if (META) mv = make_float4(vv.w, ((unsigned)meta.y >> k) & 1u ? kPinBoost : 0.f, 0.f, 0.f);
     sweep_vertex<TPV, RE, RB, M>(a, v, leader, base, bbase, erows, brows, xv, xe, le, we, xb, wb, ip.w, ip, mv, p0,
                                  vv);
 }
@@ -471,9 +478,10 @@ __global__ void __launch_bounds__(256) vbd_sweep_list_kernel(SweepArgs a) {
 }
 
 // The list sweep with streaming loads for the per-iteration constant data and the
-// next slice's descriptor in flight while the current slice computes: a warp loads
-// the list entry two slices ahead and the descriptor one slice ahead, so the chain
-// in front of each slice's neighbour gathers is its stencil rows alone.
+// next slice's descriptor and metadata in flight while the current slice computes: a
+// warp loads the list entry two slices ahead and the descriptor one slice ahead, so
+// the chain in front of each slice's neighbour gathers is its stencil rows alone. The
+// material record is not read (sweep_slice_sd with META).
 template <int TPV, int RE, int RB>
 __global__ void __launch_bounds__(256) vbd_sweep_stream_kernel(SweepArgs a) {
     grid_dependency_wait();  // the list and the positions come from the kernels before
@@ -483,17 +491,24 @@ __global__ void __launch_bounds__(256) vbd_sweep_stream_kernel(SweepArgs a) {
     const int count = *a.list_count;
     int idx = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     if (idx >= count) return;
-    int4 sd = __ldg(&a.slices[a.list[idx]]);
+    const int first = a.list[idx];
+    int4 sd = __ldg(&a.slices[first]);
+    int2 meta = __ldg(&a.slice_meta[first]);
     int next = idx + nwarps < count ? a.list[idx + nwarps] : 0;
     for (;;) {
         const bool more = idx + nwarps < count;
         int4 sd_next = sd;
-        if (more) sd_next = __ldg(&a.slices[next]);
+        int2 meta_next = meta;
+        if (more) {
+            sd_next = __ldg(&a.slices[next]);
+            meta_next = __ldg(&a.slice_meta[next]);
+        }
         const int after = idx + 2 * nwarps < count ? a.list[idx + 2 * nwarps] : 0;
-        sweep_slice_sd<TPV, RE, RB, PlainMem, StreamLoads>(a, sd, lane);
+        sweep_slice_sd<TPV, RE, RB, PlainMem, StreamLoads, true>(a, sd, lane, meta);
         if (!more) break;
         idx += nwarps;
         sd = sd_next;
+        meta = meta_next;
         next = after;
     }
 }

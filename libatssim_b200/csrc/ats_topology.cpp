@@ -381,6 +381,7 @@ bool build_layout(const std::vector<Topology>& topos, const std::vector<ats_inst
             L.x0[4 * (size_t)lv + 2] = t.pos[3 * v + 2];
             L.x0[4 * (size_t)lv + 3] = mass;
             L.vm[4 * (size_t)lv + 0] = (float)(kb * hdiag);
+            L.vel[4 * (size_t)lv + 3] = L.vm[4 * (size_t)lv + 0];  // for the list sweep, which skips vm
             L.vm[4 * (size_t)lv + 1] = fixed ? 1e9f : 0.f;
             L.vm[4 * (size_t)lv + 2] = fixed ? 0.f : 1.0f / mass;
             int inst_id = i;

@@ -473,8 +473,10 @@ def test_persistent_vbd_frames_equal_per_colour_launches(ats, n):
 def test_list_sweep_forms_equal_plain(ats, tpv, form):
     """The residual-driven frames' sweep, plain against pipelined (each warp stages its
     next slice in shared memory while computing the current one) and streamed
-    (evict-first loads, next descriptor in flight): the same slices and the same
-    arithmetic, so bit-identical positions; with some instances stopping early."""
+    (evict-first loads, next descriptor in flight, material from the slice metadata and
+    vel.w): the same slices and the same arithmetic, so bit-identical positions; with
+    some instances stopping early, pinned corners, and a state set from the host halfway
+    (which must keep vel.w)."""
     insts, prm = configs.c2(num_instances=5, seed=3, side_range=(20, 90))
     a = ats.Cloth(insts, threads_per_vertex=tpv, block_size=128, **prm)
     b = ats.Cloth(insts, threads_per_vertex=tpv, block_size=128, **prm)
@@ -482,6 +484,10 @@ def test_list_sweep_forms_equal_plain(ats, tpv, form):
     b.set_list_sweep(form)
     assert a.info.list_form == 0 and b.info.list_form == form
     for f in range(4):
+        if f == 2:
+            xs, vs = a.state()
+            a.set_state(xs, vs)
+            b.set_state(xs, vs)
         tol = 0.0 if f % 2 == 0 else 0.35
         ia, ra = a.frame_to_residual(tol, check_every=5, max_iterations=15)
         ib, rb = b.frame_to_residual(tol, check_every=5, max_iterations=15)
