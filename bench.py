@@ -573,6 +573,10 @@ def run_learned(args):
                                                else "no capture of this kernel"),
                             "kernel": sweep_kernel,
                             "us_per_launch_upper_bound": per_launch * 1e3, "alg_bytes_per_launch": bytes_launch,
+                            "layout_bytes_per_launch": info.sweep_layout_bytes / info.num_vertex_colors,
+                            "layout_note": "bytes the streamed sweep must move in this layout (merged per-vertex "
+                                           "stencil, no per-vertex material record); achieved and frac use the "
+                                           "algorithmic bytes",
                             "timing": "50 listed iterations over all instances, CUDA events, predict/update/2 probes "
                                       "included", "peak_source": peak_src,
                             "sweeps_per_learned_frame": sweeps_per_learned_frame,

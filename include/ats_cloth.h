@@ -97,6 +97,10 @@ typedef struct ats_cloth_info {
     int vbd_form;           /* fixed-iteration VBD iterations: 0 a launch per colour, 1 persistent */
     int xpbd_form;          /* XPBD iterations: 0 a launch per colour, 1 persistent */
     int list_form;          /* list sweep of residual-driven frames: 0 plain, 1 pipelined, 2 streamed */
+    long long sweep_layout_bytes; /* bytes one VBD iteration of the streamed list sweep must move over
+                                     every instance in this layout: the stencil rows as stored (8 B a
+                                     slot, 4 more on edge rows), x read and written, x0 and vel per
+                                     vertex, 28 B a slice (descriptor, metadata, list entry) */
 } ats_cloth_info;
 
 /* ---------------------------------------------------------------- host-only mesh helpers */

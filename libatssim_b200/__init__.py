@@ -69,6 +69,7 @@ class ClothInfo(ctypes.Structure):
         ("vbd_form", ctypes.c_int),
         ("xpbd_form", ctypes.c_int),
         ("list_form", ctypes.c_int),
+        ("sweep_layout_bytes", ctypes.c_longlong),
     ]
 
 

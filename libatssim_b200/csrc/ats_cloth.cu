@@ -1868,6 +1868,12 @@ int ats_cloth_query(const ats_cloth* c, ats_cloth_info* info) {
     info->vbd_form = c->vbd_loop_blocks > 0 ? 1 : 0;
     info->xpbd_form = c->xpbd_loop_blocks > 0 ? 1 : 0;
     info->list_form = c->list_form;
+    long long sb = 64LL * c->L.nv;
+    for (size_t k = 0; k + 3 < c->L.slices.size(); k += 4) {
+        const int rows = c->L.slices[k + 3] & 0xffff, erows = c->L.slices[k + 3] >> 16;
+        sb += 32LL * (8 * rows + 4 * erows) + 28;
+    }
+    info->sweep_layout_bytes = sb;
     return ATS_OK;
 }
 
