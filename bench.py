@@ -315,8 +315,9 @@ def maxrank(v):
 # DRAM traffic over algorithmic bytes of the list sweeps, per launch: ncu
 # (dram__bytes_read.sum + dram__bytes_write.sum, 3 launches, --clock-control none) on the
 # 32-instance c4 case, 1 lane per vertex, 64 threads per block: 216.9 MB (plain) and
-# 209.0 MB (streamed) against 214.0 MB algorithmic.
-SWEEP_TRAFFIC_RATIO = {"vbd_sweep_list_kernel<1>": 1.013, "vbd_sweep_stream_kernel<1>": 0.977}
+# 195.3 MB (streamed, which skips the per-vertex material record) against 214.0 MB
+# algorithmic.
+SWEEP_TRAFFIC_RATIO = {"vbd_sweep_list_kernel<1>": 1.013, "vbd_sweep_stream_kernel<1>": 0.913}
 
 
 def sweep_roofline(cloth, stream, reps=3, iters=50):
