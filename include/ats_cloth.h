@@ -101,6 +101,8 @@ typedef struct ats_cloth_info {
                                      every instance in this layout: the stencil rows as stored (8 B a
                                      slot, 4 more on edge rows), x read and written, x0 and vel per
                                      vertex, 28 B a slice (descriptor, metadata, list entry) */
+    int tune_source;        /* shape and forms: 0 defaults or set explicitly, 1 timed by ats_autotune,
+                               2 taken from the autotuning cache */
 } ats_cloth_info;
 
 /* ---------------------------------------------------------------- host-only mesh helpers */
@@ -257,6 +259,19 @@ int ats_set_probe_policy(ats_cloth* cloth, int policy);
  * (ats_cloth_query reports the forms). The iterate x is restored afterwards; captured frame graphs are dropped (they
  * are re-captured on next use). Synchronises `stream`. */
 int ats_autotune(ats_cloth* cloth, int iterations, ats_stream stream, int* tpv, int* block_size);
+
+/* The autotuning cache: ats_autotune records its choices (lanes per vertex, block size,
+ * the three forms) per (GPU name and SM count, mesh class: vertex and instance counts in
+ * power-of-two buckets, vertex, stretch and bending colour counts), and a later call on a
+ * handle of the same GPU and class applies them without timing (ats_cloth_info's
+ * tune_source = 2). The cache is per process; _save writes it as text ("ats-autotune 1",
+ * then one "key tpv block vbd_form list_form xpbd_form" line per entry), _load merges
+ * such a file (ATS_ERR_INVALID if it cannot be read or a line is malformed; nothing is merged
+ * then), _clear empties it. No GPU is needed for these four. */
+int ats_autotune_cache_size(void);
+void ats_autotune_cache_clear(void);
+int ats_autotune_cache_save(const char* path);
+int ats_autotune_cache_load(const char* path);
 
 /* Two-device asynchronous iteration, as example2_async_iter.cpp:1160-1200 and
  * example3 run it: both devices iterate on their own copy of the positions from a

@@ -70,6 +70,7 @@ class ClothInfo(ctypes.Structure):
         ("xpbd_form", ctypes.c_int),
         ("list_form", ctypes.c_int),
         ("sweep_layout_bytes", ctypes.c_longlong),
+        ("tune_source", ctypes.c_int),
     ]
 
 
@@ -147,6 +148,9 @@ _SIGNATURES = {
     "ats_set_probe_policy": [_vp, ctypes.c_int],
     "ats_set_sweep_form": [_vp, ctypes.c_int, ctypes.c_int],
     "ats_set_list_sweep": [_vp, ctypes.c_int],
+    "ats_autotune_cache_size": [],
+    "ats_autotune_cache_save": [ctypes.c_char_p],
+    "ats_autotune_cache_load": [ctypes.c_char_p],
     "ats_energy_noalloc": [_vp, _vp, _vp, _vp, _vp, ctypes.c_int, _vp, _vp, ctypes.c_int, _vp, _vp, ctypes.c_int,
                            ctypes.c_float, ctypes.c_float, _fp, ctypes.c_float, _vp, _vp],
 }
@@ -167,6 +171,8 @@ def lib():
         L.ats_last_error.argtypes = []
         L.ats_mlp_param_count.restype = ctypes.c_int
         L.ats_mlp_param_count.argtypes = []
+        L.ats_autotune_cache_clear.restype = None
+        L.ats_autotune_cache_clear.argtypes = []
         _lib = L
     return _lib
 
@@ -206,6 +212,24 @@ def kernel_launches():
     n = ctypes.c_longlong(0)
     _check(lib().ats_kernel_launches(ctypes.byref(n)))
     return int(n.value)
+
+
+def autotune_cache_size():
+    """Entries of the process's autotuning cache (one per GPU and mesh class)."""
+    return int(lib().ats_autotune_cache_size())
+
+
+def autotune_cache_clear():
+    lib().ats_autotune_cache_clear()
+
+
+def autotune_cache_save(path):
+    _check(lib().ats_autotune_cache_save(os.fsencode(path)))
+
+
+def autotune_cache_load(path):
+    """Merges a file written by autotune_cache_save into the cache."""
+    _check(lib().ats_autotune_cache_load(os.fsencode(path)))
 
 
 # ---------------------------------------------------------------- mesh helpers

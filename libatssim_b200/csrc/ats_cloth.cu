@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstring>
 #include <atomic>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <thread>
@@ -1868,6 +1869,7 @@ int ats_cloth_query(const ats_cloth* c, ats_cloth_info* info) {
     info->vbd_form = c->vbd_loop_blocks > 0 ? 1 : 0;
     info->xpbd_form = c->xpbd_loop_blocks > 0 ? 1 : 0;
     info->list_form = c->list_form;
+    info->tune_source = c->tune_source;
     long long sb = 64LL * c->L.nv;
     for (size_t k = 0; k + 3 < c->L.slices.size(); k += 4) {
         const int rows = c->L.slices[k + 3] & 0xffff, erows = c->L.slices[k + 3] >> 16;
@@ -2089,12 +2091,171 @@ int ats_frame_graph(ats_cloth* c, int solver, ats_stream stream) {
     return ATS_OK;
 }
 
+}  // extern "C"
+
+namespace ats {
+// The autotuner's choices per (GPU, mesh class), shared by the handles of a process and
+// saved to / loaded from a text file by ats_autotune_cache_save / _load. The mesh class
+// is what the choices depend on: the vertex and instance counts (power-of-two buckets)
+// and the colour counts of both solvers.
+struct TuneChoice {
+    int tpv, block, vbd_form, list_form, xpbd_form;
+};
+std::mutex g_tune_mu;
+std::map<std::string, TuneChoice> g_tune_cache;
+
+int floor_log2(long long v) {
+    int k = 0;
+    while (v > 1) {
+        v >>= 1;
+        ++k;
+    }
+    return k;
+}
+
+std::string tune_key(const ats_cloth* c) {
+    cudaDeviceProp p;
+    std::string dev = "unknown";
+    int sms = 0;
+    if (cudaGetDeviceProperties(&p, c->device) == cudaSuccess) {
+        dev = p.name;
+        sms = p.multiProcessorCount;
+    }
+    for (char& ch : dev)
+        if (ch == ' ' || ch == '|' || ch == '\n') ch = '_';
+    char buf[256];
+    std::snprintf(buf, sizeof(buf), "%s|%d|v%d|i%d|c%d|s%d|b%d", dev.c_str(), sms, floor_log2(c->L.nv),
+                  floor_log2(c->L.ninst), c->L.n_vcolors, c->L.n_scolors, c->L.n_bcolors);
+    return buf;
+}
+
+// Applies cached choices to a handle: its layout for the lanes per vertex, the block
+// size and the forms (a persistent form only where the device can run it).
+int apply_tuning(ats_cloth* c, const TuneChoice& t) {
+    std::string err;
+    if (t.tpv != c->L.tpv) {
+        int r;
+        if (!build_slices(c->L, t.tpv, err)) {
+            set_error("ats_autotune: " + err);
+            return ATS_ERR_INVALID;
+        }
+        if ((r = upload_stencil(c))) return r;
+    }
+    c->block = t.block;
+    c->vbd_loop_blocks = t.vbd_form ? vbd_loop_blocks(c->L.tpv, c->block, c->device) : 0;
+    c->list_form = t.list_form;
+    list_sweep_ctas(c->L.tpv, c->block, c->list_form);
+    c->xpbd_loop_blocks = t.xpbd_form ? c->xpbd_loop_capable : 0;
+    c->prm.threads_per_vertex = c->L.tpv;
+    c->prm.block_size = c->block;
+    c->drop_graphs();
+    return ATS_OK;
+}
+}  // namespace ats
+
+extern "C" {
+
+int ats_autotune_cache_size(void) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    return (int)g_tune_cache.size();
+}
+
+void ats_autotune_cache_clear(void) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache.clear();
+}
+
+int ats_autotune_cache_save(const char* path) {
+    if (!path) {
+        set_error("ats_autotune_cache_save: null path");
+        return ATS_ERR_INVALID;
+    }
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    FILE* f = std::fopen(path, "w");
+    if (!f) {
+        set_error(std::string("ats_autotune_cache_save: cannot open ") + path);
+        return ATS_ERR_INVALID;
+    }
+    std::fprintf(f, "ats-autotune 1\n");
+    for (const auto& kv : g_tune_cache)
+        std::fprintf(f, "%s %d %d %d %d %d\n", kv.first.c_str(), kv.second.tpv, kv.second.block, kv.second.vbd_form,
+                     kv.second.list_form, kv.second.xpbd_form);
+    const bool ok = std::fclose(f) == 0;
+    if (!ok) {
+        set_error(std::string("ats_autotune_cache_save: write failed: ") + path);
+        return ATS_ERR_INVALID;
+    }
+    return ATS_OK;
+}
+
+int ats_autotune_cache_load(const char* path) {
+    if (!path) {
+        set_error("ats_autotune_cache_load: null path");
+        return ATS_ERR_INVALID;
+    }
+    FILE* f = std::fopen(path, "r");
+    if (!f) {
+        set_error(std::string("ats_autotune_cache_load: cannot open ") + path);
+        return ATS_ERR_INVALID;
+    }
+    char line[512];
+    std::map<std::string, TuneChoice> got;
+    bool header = false, bad = false;
+    while (std::fgets(line, sizeof(line), f)) {
+        if (!header) {
+            header = std::strncmp(line, "ats-autotune 1", 14) == 0;
+            if (!header) bad = true;
+            if (bad) break;
+            continue;
+        }
+        char key[400];
+        TuneChoice t;
+        if (std::sscanf(line, "%399s %d %d %d %d %d", key, &t.tpv, &t.block, &t.vbd_form, &t.list_form, &t.xpbd_form) != 6 ||
+            !(t.tpv == 1 || t.tpv == 2 || t.tpv == 4 || t.tpv == 8) || !(t.block == 64 || t.block == 128 || t.block == 256) ||
+            t.vbd_form < 0 || t.vbd_form > 1 || t.list_form < 0 || t.list_form > 2 || t.xpbd_form < 0 || t.xpbd_form > 1) {
+            bad = true;
+            break;
+        }
+        got[key] = t;
+    }
+    std::fclose(f);
+    if (bad || !header) {
+        set_error(std::string("ats_autotune_cache_load: malformed file ") + path);
+        return ATS_ERR_INVALID;
+    }
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    for (const auto& kv : got) g_tune_cache[kv.first] = kv.second;
+    return ATS_OK;
+}
+
 int ats_autotune(ats_cloth* c, int iterations, ats_stream stream, int* out_tpv, int* out_block) {
     if (!c || iterations <= 0) {
         set_error("ats_autotune: null handle or iterations <= 0");
         return ATS_ERR_INVALID;
     }
     cudaStream_t st = S(stream);
+    // a choice made before for this GPU and mesh class: applied without timing
+    const std::string key = tune_key(c);
+    {
+        TuneChoice t{};
+        bool hit = false;
+        {
+            std::lock_guard<std::mutex> lk(g_tune_mu);
+            auto it = g_tune_cache.find(key);
+            if (it != g_tune_cache.end()) {
+                t = it->second;
+                hit = true;
+            }
+        }
+        if (hit) {
+            const int r = apply_tuning(c, t);
+            if (r) return r;
+            c->tune_source = 2;
+            if (out_tpv) *out_tpv = c->L.tpv;
+            if (out_block) *out_block = c->block;
+            return ATS_OK;
+        }
+    }
     // keep the iterate: the trial sweeps move it
     DevBuf<float4> saved;
     ATS_CUDA(saved.alloc(c->L.nv));
@@ -2228,6 +2389,12 @@ int ats_autotune(ats_cloth* c, int iterations, ats_stream stream, int* out_tpv, 
     ATS_CUDA(cudaMemcpyAsync(c->x.p, saved.p, c->x.bytes(), cudaMemcpyDeviceToDevice, st));
     ATS_CUDA(cudaStreamSynchronize(st));
     if (r) return r;
+    c->tune_source = 1;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune_cache[key] = TuneChoice{c->L.tpv, c->block, c->vbd_loop_blocks > 0 ? 1 : 0, c->list_form,
+                                       c->xpbd_loop_blocks > 0 ? 1 : 0};
+    }
     if (out_tpv) *out_tpv = c->L.tpv;
     if (out_block) *out_block = c->block;
     return ATS_OK;

@@ -76,12 +76,13 @@ struct ats_cloth {
     DevBuf<float4> xb_q;
     DevBuf<float> xb_lambda;
     DevBuf<int> xs_color_d, xb_color_d;  // XPBD colour offsets, for the persistent kernel
-    DevBuf<unsigned> loop_bar;           // its grid barrier: arrivals, generation
+    DevBuf<unsigned> loop_bar;           // its grid barrier: arrivals since the launch, bit 31 error
     DevBuf<int> loop_err;                // set when a barrier wait ran out
     int xpbd_loop_capable = 0;           // co-resident blocks of the persistent XPBD kernel (0: unavailable)
     int xpbd_loop_blocks = 0;            // the blocks XPBD frames launch it with (0: per-colour launches)
     int vbd_loop_blocks = 0;             // the same for VBD iterations (0: one launch per colour; set by autotune)
     int list_form = 0;                   // list sweep of residual-driven frames: 0 plain, 1 pipelined, 2 streamed
+    int tune_source = 0;                 // shape and forms: 0 defaults or explicit, 1 timed, 2 tuning cache
     DevBuf<int2> en_edge;
     DevBuf<float> en_rest, en_k, en_q, en_kb;
     DevBuf<int4> en_bend;

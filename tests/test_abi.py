@@ -40,3 +40,34 @@ def test_invalid_arguments_report_errors(ats):
         ats.grid_mesh(1)
     assert e.value.status == ats.ATS_ERR_INVALID
     assert b"n >= 2" in ats.lib().ats_last_error()
+
+
+def test_autotune_cache_file_round_trip(ats, tmp_path):
+    """The autotuning cache's text file: load merges valid entries, save writes them
+    back, a malformed file is rejected whole (no GPU involved)."""
+    import pytest
+    ats.autotune_cache_clear()
+    assert ats.autotune_cache_size() == 0
+    src = tmp_path / "tune.txt"
+    src.write_text("ats-autotune 1\n"
+                   "NVIDIA_B200|148|v22|i6|c4|s7|b11 1 64 0 2 0\n"
+                   "NVIDIA_B200|148|v18|i0|c4|s6|b10 1 128 0 0 0\n")
+    ats.autotune_cache_load(str(src))
+    assert ats.autotune_cache_size() == 2
+    out = tmp_path / "out.txt"
+    ats.autotune_cache_save(str(out))
+    assert sorted(out.read_text().splitlines()) == sorted(src.read_text().splitlines())
+    for bad in ("ats-autotune 2\nk 1 64 0 0 0\n",               # unknown version
+                "ats-autotune 1\nk 3 64 0 0 0\n",               # lanes per vertex not 1, 2, 4, 8
+                "ats-autotune 1\nk 1 64 0 5 0\n",               # list form out of range
+                "ats-autotune 1\nk 1 64\n"):                    # short line
+        f = tmp_path / "bad.txt"
+        f.write_text(bad)
+        with pytest.raises(ats.AtsError) as e:
+            ats.autotune_cache_load(str(f))
+        assert e.value.status == ats.ATS_ERR_INVALID
+        assert ats.autotune_cache_size() == 2
+    with pytest.raises(ats.AtsError):
+        ats.autotune_cache_load(str(tmp_path / "missing.txt"))
+    ats.autotune_cache_clear()
+    assert ats.autotune_cache_size() == 0

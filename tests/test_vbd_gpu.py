@@ -495,3 +495,41 @@ def test_list_sweep_forms_equal_plain(ats, tpv, form):
     xa, va = a.state()
     xb, vb = b.state()
     assert np.array_equal(xa, xb) and np.array_equal(va, vb)
+
+
+def test_autotune_cache_hits_for_the_same_mesh_class(ats):
+    """A second handle of the same GPU and mesh class takes the first one's choices from
+    the autotuning cache without timing; the choices survive a save and load."""
+    import os
+    import tempfile
+    ats.autotune_cache_clear()
+    insts, prm = configs.c2(num_instances=3, seed=5, side_range=(30, 60))
+    a = ats.Cloth(insts, **prm)
+    shape_a = a.autotune(iterations=5)
+    assert a.info.tune_source == 1 and ats.autotune_cache_size() == 1
+    b = ats.Cloth(insts, **prm)
+    assert b.info.tune_source == 0
+    assert b.autotune(iterations=5) == shape_a
+    assert b.info.tune_source == 2
+    for f in ("vbd_form", "list_form", "xpbd_form"):
+        assert getattr(b.info, f) == getattr(a.info, f), f
+    # a different mesh class is timed
+    c = ats.Cloth([configs.grid_instance(200)], **prm)
+    c.autotune(iterations=5)
+    assert c.info.tune_source == 1 and ats.autotune_cache_size() == 2
+    # the cache through a file
+    path = os.path.join(tempfile.mkdtemp(), "tune.txt")
+    ats.autotune_cache_save(path)
+    ats.autotune_cache_clear()
+    ats.autotune_cache_load(path)
+    d = ats.Cloth(insts, **prm)
+    assert d.autotune(iterations=5) == shape_a and d.info.tune_source == 2
+    # the same shape and forms give the same frames
+    d.set_state(*a.state())
+    for _ in range(2):
+        a.frame()
+        d.frame()
+    assert np.array_equal(a.positions(), d.positions())
+    for h in (a, b, c, d):
+        h.close()
+    ats.autotune_cache_clear()
