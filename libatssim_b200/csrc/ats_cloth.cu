@@ -992,8 +992,8 @@ size_t pipe_smem_bytes(int tpv, int block) {
 }
 
 // Resident CTAs of the list sweeps (form 0: vbd_sweep_list_kernel, 1:
-// vbd_sweep_pipe_kernel, 2: vbd_sweep_stream_kernel), all SMs together, per (lanes per
-// vertex, block size); queried
+// vbd_sweep_pipe_kernel, 2: vbd_sweep_stream_kernel, 3: the same with evict-last
+// positions), all SMs together, per (lanes per vertex, block size); queried
 // (and the pipelined kernel's shared-memory attributes set) on first use, which is
 // outside stream capture (the eager iterations of ats_frame_to_residual's first frame,
 // or ats_autotune, come first).
@@ -1002,13 +1002,14 @@ int list_form_ctas(int form, int block, int sms) {
     switch (form) {
         case 1: return resident_ctas(vbd_sweep_pipe_kernel<TPV, RE, RB>, block, (block / 32) * pipe_smem_per_warp<RE, RB>(), sms);
         case 2: return resident_ctas(vbd_sweep_stream_kernel<TPV, RE, RB>, block, 0, sms);
+        case 3: return resident_ctas(vbd_sweep_stream_kernel<TPV, RE, RB, KeepMem>, block, 0, sms);
         default: return resident_ctas(vbd_sweep_list_kernel<TPV, RE, RB>, block, 0, sms);
     }
 }
 int list_sweep_ctas(int tpv, int block, int form) {
-    static int cache[3][4][3] = {};
+    static int cache[4][4][3] = {};
     const int ti = tpv == 1 ? 0 : tpv == 2 ? 1 : tpv == 4 ? 2 : 3, bi = block == 64 ? 0 : block == 128 ? 1 : 2;
-    int& slot = cache[form >= 0 && form < 3 ? form : 0][ti][bi];
+    int& slot = cache[form >= 0 && form < 4 ? form : 0][ti][bi];
     if (!slot) {
         int dev = 0, sms = 148;
         cudaGetDevice(&dev);
@@ -1024,7 +1025,7 @@ int list_sweep_ctas(int tpv, int block, int form) {
 }
 
 // listed: 0 one-wave sweep over the colour's slices, 1 list sweep, 2 pipelined list
-// sweep, 3 streamed list sweep
+// sweep, 3 streamed list sweep, 4 streamed with evict-last positions
 template <int TPV, int RE, int RB>
 cudaError_t sweep_launch(dim3 grid, dim3 block, cudaStream_t st, const SweepArgs& a, int listed) {
     cudaLaunchConfig_t cfg = {};
@@ -1037,7 +1038,8 @@ cudaError_t sweep_launch(dim3 grid, dim3 block, cudaStream_t st, const SweepArgs
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    const cudaError_t e = listed == 3   ? cudaLaunchKernelEx(&cfg, vbd_sweep_stream_kernel<TPV, RE, RB>, a)
+    const cudaError_t e = listed == 4   ? cudaLaunchKernelEx(&cfg, vbd_sweep_stream_kernel<TPV, RE, RB, KeepMem>, a)
+                          : listed == 3 ? cudaLaunchKernelEx(&cfg, vbd_sweep_stream_kernel<TPV, RE, RB>, a)
                           : listed == 2 ? cudaLaunchKernelEx(&cfg, vbd_sweep_pipe_kernel<TPV, RE, RB>, a)
                           : listed == 1 ? cudaLaunchKernelEx(&cfg, vbd_sweep_list_kernel<TPV, RE, RB>, a)
                                         : cudaLaunchKernelEx(&cfg, vbd_sweep_kernel<TPV, RE, RB>, a);
@@ -1695,8 +1697,9 @@ int ats_set_sweep_form(ats_cloth* c, int solver, int form) {
 }
 
 int ats_set_list_sweep(ats_cloth* c, int form) {
-    if (!c || form < 0 || form > 2) {
-        set_error("ats_set_list_sweep: need a handle and 0 (plain), 1 (pipelined) or 2 (streamed)");
+    if (!c || form < 0 || form > 3) {
+        set_error("ats_set_list_sweep: need a handle and 0 (plain), 1 (pipelined), 2 (streamed) or 3 (streamed, "
+                  "positions kept in L2)");
         return ATS_ERR_INVALID;
     }
     c->list_form = form;
@@ -2212,7 +2215,7 @@ int ats_autotune_cache_load(const char* path) {
         TuneChoice t;
         if (std::sscanf(line, "%399s %d %d %d %d %d", key, &t.tpv, &t.block, &t.vbd_form, &t.list_form, &t.xpbd_form) != 6 ||
             !(t.tpv == 1 || t.tpv == 2 || t.tpv == 4 || t.tpv == 8) || !(t.block == 64 || t.block == 128 || t.block == 256) ||
-            t.vbd_form < 0 || t.vbd_form > 1 || t.list_form < 0 || t.list_form > 2 || t.xpbd_form < 0 || t.xpbd_form > 1) {
+            t.vbd_form < 0 || t.vbd_form > 1 || t.list_form < 0 || t.list_form > 3 || t.xpbd_form < 0 || t.xpbd_form > 1) {
             bad = true;
             break;
         }
@@ -2327,14 +2330,14 @@ int ats_autotune(ats_cloth* c, int iterations, ats_stream stream, int* out_tpv, 
             if (r || ms >= best) c->vbd_loop_blocks = 0;
         }
     }
-    // the list sweep of the residual-driven frames, plain, pipelined or streamed, over
-    // every instance's slices (all instances active): the fastest of three timings each
+    // the list sweep of the residual-driven frames, its four forms, over every
+    // instance's slices (all instances active): the fastest of three timings each
     if (!r && c->L.ninst > 0) {
         std::vector<int> ones(c->L.ninst, 1);
         ATS_CUDA(cudaMemcpyAsync(c->active.p, ones.data(), ones.size() * sizeof(int), cudaMemcpyHostToDevice, st));
         if (!(r = enqueue_compaction(c, st))) {
-            float t_form[3] = {1e30f, 1e30f, 1e30f};
-            for (int form = 0; form < 3 && !r; ++form) {
+            float t_form[4] = {1e30f, 1e30f, 1e30f, 1e30f};
+            for (int form = 0; form < 4 && !r; ++form) {
                 c->list_form = form;
                 list_sweep_ctas(c->L.tpv, c->block, form);
                 if ((r = enqueue_iterations(c, ATS_SOLVER_VBD, 1, st, c->active.p))) break;
@@ -2353,7 +2356,7 @@ int ats_autotune(ats_cloth* c, int iterations, ats_stream stream, int* out_tpv, 
                 }
             }
             c->list_form = 0;
-            for (int form = 1; form < 3 && !r; ++form)
+            for (int form = 1; form < 4 && !r; ++form)
                 if (t_form[form] < t_form[c->list_form]) c->list_form = form;
         }
         ATS_CUDA(cudaStreamSynchronize(st));  // the host vector leaves scope

@@ -469,7 +469,7 @@ def test_persistent_vbd_frames_equal_per_colour_launches(ats, n):
 
 
 @pytest.mark.parametrize("tpv", [1, 2, 4, 8])
-@pytest.mark.parametrize("form", [1, 2])
+@pytest.mark.parametrize("form", [1, 2, 3])
 def test_list_sweep_forms_equal_plain(ats, tpv, form):
     """The residual-driven frames' sweep, plain against pipelined (each warp stages its
     next slice in shared memory while computing the current one) and streamed
