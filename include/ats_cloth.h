@@ -97,7 +97,7 @@ typedef struct ats_cloth_info {
     int vbd_form;           /* fixed-iteration VBD iterations: 0 a launch per colour, 1 persistent */
     int xpbd_form;          /* XPBD iterations: 0 a launch per colour, 1 persistent */
     int list_form;          /* list sweep of residual-driven frames: 0 plain, 1 pipelined, 2 streamed,
-                               3 streamed with positions kept in L2 */
+                               3 streamed with the positions persisting in L2 */
     long long sweep_layout_bytes; /* bytes one VBD iteration of the streamed list sweep must move over
                                      every instance in this layout: the stencil rows as stored (8 B a
                                      slot, 4 more on edge rows), x read and written, x0 and vel per
@@ -238,9 +238,12 @@ int ats_set_sweep_form(ats_cloth* cloth, int solver, int form);
  * current one; 2 streamed, where the data read once per iteration (stencil, vertex
  * records, frame-start state) goes through evict-first loads, leaving L2 to the
  * positions, and each warp's next slice descriptor loads while the current slice
- * computes; 3 as 2 with the positions' loads and stores marked evict-last in L2, so
- * that the neighbours the next colours gather stay there. Same positions. ats_autotune
- * times the four and keeps the fastest. */
+ * computes; 3 as 2 with the handle's positions kept in L2 as persisting lines (an
+ * access-policy window on each sweep launch), so that the neighbours the next colours
+ * gather are still there: while a handle uses form 3 it sizes the context's
+ * persisting-L2 set-aside (cudaLimitPersistingL2CacheSize) for its positions, and the
+ * last such handle puts the previous size back. ATS_ERR_STATE if the device has no
+ * persisting L2. Same positions. ats_autotune times the four and keeps the fastest. */
 int ats_set_list_sweep(ats_cloth* cloth, int form);
 
 /* Probe schedule of the residual-driven frames of this handle (ats_frame_to_residual(s),

@@ -512,7 +512,7 @@ class Cloth:
 
     def set_list_sweep(self, form):
         """Sweep of the residual-driven frames: 0 plain, 1 pipelined, 2 streamed, 3
-        streamed with positions kept in L2 (ats_set_list_sweep)."""
+        streamed with the positions persisting in L2 (ats_set_list_sweep)."""
         _check(lib().ats_set_list_sweep(self.h, int(form)))
         info = ClothInfo()
         _check(lib().ats_cloth_query(self.h, ctypes.byref(info)))

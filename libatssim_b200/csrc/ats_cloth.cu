@@ -992,8 +992,8 @@ size_t pipe_smem_bytes(int tpv, int block) {
 }
 
 // Resident CTAs of the list sweeps (form 0: vbd_sweep_list_kernel, 1:
-// vbd_sweep_pipe_kernel, 2: vbd_sweep_stream_kernel, 3: the same with evict-last
-// positions), all SMs together, per (lanes per vertex, block size); queried
+// vbd_sweep_pipe_kernel, 2 and 3: vbd_sweep_stream_kernel), all SMs together, per
+// (lanes per vertex, block size); queried
 // (and the pipelined kernel's shared-memory attributes set) on first use, which is
 // outside stream capture (the eager iterations of ats_frame_to_residual's first frame,
 // or ats_autotune, come first).
@@ -1001,8 +1001,8 @@ template <int TPV, int RE, int RB>
 int list_form_ctas(int form, int block, int sms) {
     switch (form) {
         case 1: return resident_ctas(vbd_sweep_pipe_kernel<TPV, RE, RB>, block, (block / 32) * pipe_smem_per_warp<RE, RB>(), sms);
-        case 2: return resident_ctas(vbd_sweep_stream_kernel<TPV, RE, RB>, block, 0, sms);
-        case 3: return resident_ctas(vbd_sweep_stream_kernel<TPV, RE, RB, KeepMem>, block, 0, sms);
+        case 2:
+        case 3: return resident_ctas(vbd_sweep_stream_kernel<TPV, RE, RB>, block, 0, sms);
         default: return resident_ctas(vbd_sweep_list_kernel<TPV, RE, RB>, block, 0, sms);
     }
 }
@@ -1025,26 +1025,98 @@ int list_sweep_ctas(int tpv, int block, int form) {
 }
 
 // listed: 0 one-wave sweep over the colour's slices, 1 list sweep, 2 pipelined list
-// sweep, 3 streamed list sweep, 4 streamed with evict-last positions
+// sweep, 3 streamed list sweep, 4 streamed with the positions as persisting L2 lines
+// (the access-policy window `win`)
 template <int TPV, int RE, int RB>
-cudaError_t sweep_launch(dim3 grid, dim3 block, cudaStream_t st, const SweepArgs& a, int listed) {
+cudaError_t sweep_launch(dim3 grid, dim3 block, cudaStream_t st, const SweepArgs& a, int listed,
+                         const cudaAccessPolicyWindow* win = nullptr) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = grid;
     cfg.blockDim = block;
     cfg.dynamicSmemBytes = listed == 2 ? (block.x / 32) * pipe_smem_per_warp<RE, RB>() : 0;
     cfg.stream = st;
-    cudaLaunchAttribute attr[1];
+    cudaLaunchAttribute attr[2];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    const cudaError_t e = listed == 4   ? cudaLaunchKernelEx(&cfg, vbd_sweep_stream_kernel<TPV, RE, RB, KeepMem>, a)
-                          : listed == 3 ? cudaLaunchKernelEx(&cfg, vbd_sweep_stream_kernel<TPV, RE, RB>, a)
+    if (listed == 4 && win && win->num_bytes > 0) {
+        attr[1].id = cudaLaunchAttributeAccessPolicyWindow;
+        attr[1].val.accessPolicyWindow = *win;
+        cfg.numAttrs = 2;
+    }
+    const cudaError_t e = listed >= 3   ? cudaLaunchKernelEx(&cfg, vbd_sweep_stream_kernel<TPV, RE, RB>, a)
                           : listed == 2 ? cudaLaunchKernelEx(&cfg, vbd_sweep_pipe_kernel<TPV, RE, RB>, a)
                           : listed == 1 ? cudaLaunchKernelEx(&cfg, vbd_sweep_list_kernel<TPV, RE, RB>, a)
                                         : cudaLaunchKernelEx(&cfg, vbd_sweep_kernel<TPV, RE, RB>, a);
     if (e == cudaSuccess) count_launch(st);
     return e;
+}
+
+// List form 3 keeps the positions in L2 between colours: a sweep streams about three
+// times the positions' bytes of stencil past them, and the next colours gather them
+// again as neighbours. The handles that use it share the context's persisting-L2
+// set-aside (cudaLimitPersistingL2CacheSize, a per-context limit): the first one sizes
+// it for its positions (up to the device maximum), the last one puts back the size it
+// found and resets the persisting lines. Each launch of its sweep carries an access-policy
+// window over the handle's positions whose hit ratio is the set-aside over the window.
+std::mutex g_l2_mu;
+int g_l2_users = 0;
+size_t g_l2_prev = 0;
+
+int l2_keep_acquire(ats_cloth* c) {
+    if (c->l2_keep) return ATS_OK;
+    int max_persist = 0, max_window = 0;
+    ATS_CUDA(cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, c->device));
+    ATS_CUDA(cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, c->device));
+    if (max_persist <= 0 || max_window <= 0) {
+        set_error("list sweep form 3: the device has no persisting L2");
+        return ATS_ERR_STATE;
+    }
+    const size_t window = std::min(c->x.bytes(), (size_t)max_window);
+    size_t setaside = 0;
+    {
+        std::lock_guard<std::mutex> lk(g_l2_mu);
+        size_t cur = 0;
+        ATS_CUDA(cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize));
+        if (g_l2_users == 0) g_l2_prev = cur;
+        const size_t want = std::min(window, (size_t)max_persist);
+        if (want > cur) ATS_CUDA(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want));
+        ATS_CUDA(cudaDeviceGetLimit(&setaside, cudaLimitPersistingL2CacheSize));
+        ++g_l2_users;
+    }
+    c->l2_window.base_ptr = c->x.p;
+    c->l2_window.num_bytes = window;
+    c->l2_window.hitRatio = window > 0 ? std::min(1.f, (float)((double)setaside / (double)window)) : 0.f;
+    c->l2_window.hitProp = cudaAccessPropertyPersisting;
+    c->l2_window.missProp = cudaAccessPropertyNormal;
+    c->l2_keep = true;
+    return ATS_OK;
+}
+
+void l2_keep_release(ats_cloth* c) {
+    if (!c->l2_keep) return;
+    c->l2_keep = false;
+    c->l2_window = cudaAccessPolicyWindow{};
+    std::lock_guard<std::mutex> lk(g_l2_mu);
+    if (--g_l2_users == 0) {
+        cudaDeviceSynchronize();
+        cudaCtxResetPersistingL2Cache();
+        cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, g_l2_prev);
+    }
+}
+
+// Sets the list form of a handle, taking or giving back its share of the set-aside.
+int set_list_form(ats_cloth* c, int form) {
+    if (form == 3) {
+        const int r = l2_keep_acquire(c);
+        if (r) return r;
+    } else {
+        l2_keep_release(c);
+    }
+    c->list_form = form;
+    list_sweep_ctas(c->L.tpv, c->block, form);
+    return ATS_OK;
 }
 
 int launch_sweep(ats_cloth* c, int color, cudaStream_t st, const int* active) {
@@ -1077,10 +1149,10 @@ int launch_sweep(ats_cloth* c, int color, cudaStream_t st, const int* active) {
     const dim3 grid(blocks), block(c->block);
     cudaError_t e;
     switch (c->L.tpv) {
-        case 1: e = sweep_launch<1, 6, 6>(grid, block, st, a, listed); break;
-        case 2: e = sweep_launch<2, 3, 3>(grid, block, st, a, listed); break;
-        case 4: e = sweep_launch<4, 2, 2>(grid, block, st, a, listed); break;
-        default: e = sweep_launch<8, 1, 1>(grid, block, st, a, listed); break;
+        case 1: e = sweep_launch<1, 6, 6>(grid, block, st, a, listed, &c->l2_window); break;
+        case 2: e = sweep_launch<2, 3, 3>(grid, block, st, a, listed, &c->l2_window); break;
+        case 4: e = sweep_launch<4, 2, 2>(grid, block, st, a, listed, &c->l2_window); break;
+        default: e = sweep_launch<8, 1, 1>(grid, block, st, a, listed, &c->l2_window); break;
     }
     if (e != cudaSuccess) {
         set_error(std::string("vbd sweep launch: ") + cudaGetErrorString(e));
@@ -1702,8 +1774,8 @@ int ats_set_list_sweep(ats_cloth* c, int form) {
                   "positions kept in L2)");
         return ATS_ERR_INVALID;
     }
-    c->list_form = form;
-    list_sweep_ctas(c->L.tpv, c->block, form);  // shared-memory attributes, outside any capture
+    const int r = set_list_form(c, form);  // shared-memory attributes, outside any capture
+    if (r) return r;
     c->drop_graphs();
     return ATS_OK;
 }
@@ -1849,6 +1921,7 @@ int ats_cloth_create(const ats_instance_desc* inst, int ninst, const ats_solver_
 int ats_cloth_destroy(ats_cloth* c) {
     if (!c) return ATS_OK;
     cudaDeviceSynchronize();
+    l2_keep_release(c);
     delete c;
     return ATS_OK;
 }
@@ -2146,8 +2219,7 @@ int apply_tuning(ats_cloth* c, const TuneChoice& t) {
     }
     c->block = t.block;
     c->vbd_loop_blocks = t.vbd_form ? vbd_loop_blocks(c->L.tpv, c->block, c->device) : 0;
-    c->list_form = t.list_form;
-    list_sweep_ctas(c->L.tpv, c->block, c->list_form);
+    if (set_list_form(c, t.list_form)) set_list_form(c, 2);  // no persisting L2 here: the streamed form
     c->xpbd_loop_blocks = t.xpbd_form ? c->xpbd_loop_capable : 0;
     c->prm.threads_per_vertex = c->L.tpv;
     c->prm.block_size = c->block;
@@ -2338,8 +2410,7 @@ int ats_autotune(ats_cloth* c, int iterations, ats_stream stream, int* out_tpv, 
         if (!(r = enqueue_compaction(c, st))) {
             float t_form[4] = {1e30f, 1e30f, 1e30f, 1e30f};
             for (int form = 0; form < 4 && !r; ++form) {
-                c->list_form = form;
-                list_sweep_ctas(c->L.tpv, c->block, form);
+                if (set_list_form(c, form)) continue;  // form 3 needs a persisting L2
                 if ((r = enqueue_iterations(c, ATS_SOLVER_VBD, 1, st, c->active.p))) break;
                 for (int rep = 0; rep < 3; ++rep) {
                     cudaEventRecord(e0, st);
@@ -2355,9 +2426,10 @@ int ats_autotune(ats_cloth* c, int iterations, ats_stream stream, int* out_tpv, 
                     t_form[form] = std::min(t_form[form], t);
                 }
             }
-            c->list_form = 0;
+            int best_form = 0;
             for (int form = 1; form < 4 && !r; ++form)
-                if (t_form[form] < t_form[c->list_form]) c->list_form = form;
+                if (t_form[form] < t_form[best_form]) best_form = form;
+            if (!r) r = set_list_form(c, best_form);
         }
         ATS_CUDA(cudaStreamSynchronize(st));  // the host vector leaves scope
     }

@@ -37,29 +37,6 @@ struct L2Mem {
     static __device__ __forceinline__ float4 ld(const float4* p) { return __ldcg(p); }
     static __device__ __forceinline__ void st(float4* p, float4 v) { __stcg(p, v); }
 };
-// Positions marked evict-last in L2 (an L2 cache-policy hint on each access): a sweep
-// streams its stencil past them with evict-first loads, and every later colour gathers
-// these positions again as neighbours.
-__device__ __forceinline__ uint64_t l2_evict_last_policy() {
-    uint64_t pol;
-    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
-    return pol;
-}
-struct KeepMem {
-    static __device__ __forceinline__ float4 ld(const float4* p) {
-        float4 v;
-        asm volatile("ld.global.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
-                     : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
-                     : "l"(p), "l"(l2_evict_last_policy()));
-        return v;
-    }
-    static __device__ __forceinline__ void st(float4* p, float4 v) {
-        asm volatile("st.global.L2::cache_hint.v4.f32 [%0], {%1, %2, %3, %4}, %5;" ::"l"(p), "f"(v.x), "f"(v.y),
-                     "f"(v.z), "f"(v.w), "l"(l2_evict_last_policy())
-                     : "memory");
-    }
-};
-
 struct SweepArgs {
     float4* __restrict__ x;
     const float4* __restrict__ x0;
@@ -504,7 +481,7 @@ __global__ void __launch_bounds__(256) vbd_sweep_list_kernel(SweepArgs a) {
 // warp loads the list entry two slices ahead and the descriptor one slice ahead, so
 // the chain in front of each slice's neighbour gathers is its stencil rows alone. The
 // material record is not read (sweep_slice_sd with META).
-template <int TPV, int RE, int RB, class M = PlainMem>
+template <int TPV, int RE, int RB>
 __global__ void __launch_bounds__(256) vbd_sweep_stream_kernel(SweepArgs a) {
     grid_dependency_wait();  // the list and the positions come from the kernels before
     allow_dependent_launch();
@@ -526,7 +503,7 @@ __global__ void __launch_bounds__(256) vbd_sweep_stream_kernel(SweepArgs a) {
             meta_next = __ldg(&a.slice_meta[next]);
         }
         const int after = idx + 2 * nwarps < count ? a.list[idx + 2 * nwarps] : 0;
-        sweep_slice_sd<TPV, RE, RB, M, StreamLoads, true>(a, sd, lane, meta);
+        sweep_slice_sd<TPV, RE, RB, PlainMem, StreamLoads, true>(a, sd, lane, meta);
         if (!more) break;
         idx += nwarps;
         sd = sd_next;
