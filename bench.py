@@ -101,7 +101,9 @@ def parse():
     p.add_argument("--no-extras", action="store_true")
     p.add_argument("--list-sweep", type=int, default=-1, choices=[-1, 0, 1, 2, 3],
                    help="sweep of the residual-driven frames: -1 the autotuner's choice, 0 plain, 1 pipelined, "
-                        "2 streamed, 3 streamed with the positions persisting in L2")
+                        "2 streamed, 3 prefetching")
+    p.add_argument("--l2-persisting", type=int, default=-1, choices=[-1, 0, 1],
+                   help="list sweeps keep the positions persisting in L2: -1 the autotuner's choice, 0 off, 1 on")
     p.add_argument("--tpv", type=int, default=0)
     p.add_argument("--block", type=int, default=0)
     return p.parse_args()
@@ -437,6 +439,8 @@ def run_learned(args):
     cloth.set_probe_policy(args.probe_policy)
     if args.list_sweep >= 0:
         cloth.set_list_sweep(args.list_sweep)
+    if args.l2_persisting >= 0:
+        cloth.set_l2_persisting(args.l2_persisting)
     info = cloth.info
     nv = info.num_verts
     # training data: plain frames of this rank's instances
@@ -479,8 +483,8 @@ def run_learned(args):
     # sweep roofline in this run (listed sweep over all instances)
     per_launch, rf_frame_ms, bytes_launch = sweep_roofline(cloth, stream)
     sweep_kernel = (("vbd_sweep_list_kernel", "vbd_sweep_pipe_kernel", "vbd_sweep_stream_kernel",
-                     "vbd_sweep_stream_kernel")[info.list_form] + f"<{info.threads_per_vertex}>"
-                    + (" (positions persisting in L2)" if info.list_form == 3 else ""))
+                     "vbd_sweep_prefetch_kernel")[info.list_form] + f"<{info.threads_per_vertex}>"
+                    + (" (positions persisting in L2)" if info.l2_persisting else ""))
     peak, peak_src = hbm_peak()
     achieved = bytes_launch / (per_launch * 1e-3) / 1e9
     sweeps_per_learned_frame = float(np.mean(res["learned_iters"].max(axis=1))) * info.num_vertex_colors

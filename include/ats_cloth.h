@@ -97,13 +97,14 @@ typedef struct ats_cloth_info {
     int vbd_form;           /* fixed-iteration VBD iterations: 0 a launch per colour, 1 persistent */
     int xpbd_form;          /* XPBD iterations: 0 a launch per colour, 1 persistent */
     int list_form;          /* list sweep of residual-driven frames: 0 plain, 1 pipelined, 2 streamed,
-                               3 streamed with the positions persisting in L2 */
+                               3 prefetching */
     long long sweep_layout_bytes; /* bytes one VBD iteration of the streamed list sweep must move over
                                      every instance in this layout: the stencil rows as stored (8 B a
                                      slot, 4 more on edge rows), x read and written, x0 and vel per
                                      vertex, 28 B a slice (descriptor, metadata, list entry) */
     int tune_source;        /* shape and forms: 0 defaults or set explicitly, 1 timed by ats_autotune,
                                2 taken from the autotuning cache */
+    int l2_persisting;      /* 1: list sweeps keep the positions in L2 as persisting lines */
 } ats_cloth_info;
 
 /* ---------------------------------------------------------------- host-only mesh helpers */
@@ -238,13 +239,19 @@ int ats_set_sweep_form(ats_cloth* cloth, int solver, int form);
  * current one; 2 streamed, where the data read once per iteration (stencil, vertex
  * records, frame-start state) goes through evict-first loads, leaving L2 to the
  * positions, and each warp's next slice descriptor loads while the current slice
- * computes; 3 as 2 with the handle's positions kept in L2 as persisting lines (an
- * access-policy window on each sweep launch), so that the neighbours the next colours
- * gather are still there: while a handle uses form 3 it sizes the context's
- * persisting-L2 set-aside (cudaLimitPersistingL2CacheSize) for its positions, and the
- * last such handle puts the previous size back. ATS_ERR_STATE if the device has no
- * persisting L2. Same positions. ats_autotune times the four and keeps the fastest. */
+ * computes; 3 prefetching, form 2 one stage deeper: while a slice computes, the
+ * neighbour indices of the next slice are loading, so a slice waits only for its
+ * neighbour gathers. Same positions. ats_autotune times the four and keeps the fastest. */
 int ats_set_list_sweep(ats_cloth* cloth, int form);
+
+/* on = 1: every list sweep of this handle keeps its positions in L2 as persisting lines
+ * (an access-policy window over them on each launch), so that the neighbours the next
+ * colours gather are still there after the colour's stencil has streamed past. While a
+ * handle has it on, the context's persisting-L2 set-aside (cudaLimitPersistingL2CacheSize,
+ * a per-context limit) is sized for its positions (up to the device maximum); the last
+ * such handle to turn it off or be destroyed puts the previous size back. ATS_ERR_STATE
+ * if the device has no persisting L2. Same positions. ats_autotune times it. */
+int ats_set_l2_persisting(ats_cloth* cloth, int on);
 
 /* Probe schedule of the residual-driven frames of this handle (ats_frame_to_residual(s),
  * ats_frame_warm_to_residual). 0 (default): every check_every iterations after an
@@ -270,8 +277,8 @@ int ats_autotune(ats_cloth* cloth, int iterations, ats_stream stream, int* tpv, 
  * the three forms) per (GPU name and SM count, mesh class: vertex and instance counts in
  * power-of-two buckets, vertex, stretch and bending colour counts), and a later call on a
  * handle of the same GPU and class applies them without timing (ats_cloth_info's
- * tune_source = 2). The cache is per process; _save writes it as text ("ats-autotune 1",
- * then one "key tpv block vbd_form list_form xpbd_form" line per entry), _load merges
+ * tune_source = 2). The cache is per process; _save writes it as text ("ats-autotune 2",
+ * then one "key tpv block vbd_form list_form xpbd_form l2_persisting" line per entry), _load merges
  * such a file (ATS_ERR_INVALID if it cannot be read or a line is malformed; nothing is merged
  * then), _clear empties it. No GPU is needed for these four. */
 int ats_autotune_cache_size(void);

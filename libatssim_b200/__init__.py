@@ -71,6 +71,7 @@ class ClothInfo(ctypes.Structure):
         ("list_form", ctypes.c_int),
         ("sweep_layout_bytes", ctypes.c_longlong),
         ("tune_source", ctypes.c_int),
+        ("l2_persisting", ctypes.c_int),
     ]
 
 
@@ -148,6 +149,7 @@ _SIGNATURES = {
     "ats_set_probe_policy": [_vp, ctypes.c_int],
     "ats_set_sweep_form": [_vp, ctypes.c_int, ctypes.c_int],
     "ats_set_list_sweep": [_vp, ctypes.c_int],
+    "ats_set_l2_persisting": [_vp, ctypes.c_int],
     "ats_autotune_cache_size": [],
     "ats_autotune_cache_save": [ctypes.c_char_p],
     "ats_autotune_cache_load": [ctypes.c_char_p],
@@ -512,8 +514,15 @@ class Cloth:
 
     def set_list_sweep(self, form):
         """Sweep of the residual-driven frames: 0 plain, 1 pipelined, 2 streamed, 3
-        streamed with the positions persisting in L2 (ats_set_list_sweep)."""
+        prefetching (ats_set_list_sweep)."""
         _check(lib().ats_set_list_sweep(self.h, int(form)))
+        info = ClothInfo()
+        _check(lib().ats_cloth_query(self.h, ctypes.byref(info)))
+        self.info = info
+
+    def set_l2_persisting(self, on):
+        """List sweeps keep the positions in L2 as persisting lines (ats_set_l2_persisting)."""
+        _check(lib().ats_set_l2_persisting(self.h, int(bool(on))))
         info = ClothInfo()
         _check(lib().ats_cloth_query(self.h, ctypes.byref(info)))
         self.info = info

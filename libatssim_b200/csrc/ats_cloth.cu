@@ -992,8 +992,8 @@ size_t pipe_smem_bytes(int tpv, int block) {
 }
 
 // Resident CTAs of the list sweeps (form 0: vbd_sweep_list_kernel, 1:
-// vbd_sweep_pipe_kernel, 2 and 3: vbd_sweep_stream_kernel), all SMs together, per
-// (lanes per vertex, block size); queried
+// vbd_sweep_pipe_kernel, 2: vbd_sweep_stream_kernel, 3: vbd_sweep_prefetch_kernel), all
+// SMs together, per (lanes per vertex, block size); queried
 // (and the pipelined kernel's shared-memory attributes set) on first use, which is
 // outside stream capture (the eager iterations of ats_frame_to_residual's first frame,
 // or ats_autotune, come first).
@@ -1001,8 +1001,8 @@ template <int TPV, int RE, int RB>
 int list_form_ctas(int form, int block, int sms) {
     switch (form) {
         case 1: return resident_ctas(vbd_sweep_pipe_kernel<TPV, RE, RB>, block, (block / 32) * pipe_smem_per_warp<RE, RB>(), sms);
-        case 2:
-        case 3: return resident_ctas(vbd_sweep_stream_kernel<TPV, RE, RB>, block, 0, sms);
+        case 2: return resident_ctas(vbd_sweep_stream_kernel<TPV, RE, RB>, block, 0, sms);
+        case 3: return resident_ctas(vbd_sweep_prefetch_kernel<TPV, RE, RB>, block, 0, sms);
         default: return resident_ctas(vbd_sweep_list_kernel<TPV, RE, RB>, block, 0, sms);
     }
 }
@@ -1025,8 +1025,8 @@ int list_sweep_ctas(int tpv, int block, int form) {
 }
 
 // listed: 0 one-wave sweep over the colour's slices, 1 list sweep, 2 pipelined list
-// sweep, 3 streamed list sweep, 4 streamed with the positions as persisting L2 lines
-// (the access-policy window `win`)
+// sweep, 3 streamed list sweep, 4 prefetching list sweep; a list sweep given a window
+// `win` carries it as its access-policy window (positions as persisting L2 lines)
 template <int TPV, int RE, int RB>
 cudaError_t sweep_launch(dim3 grid, dim3 block, cudaStream_t st, const SweepArgs& a, int listed,
                          const cudaAccessPolicyWindow* win = nullptr) {
@@ -1040,12 +1040,13 @@ cudaError_t sweep_launch(dim3 grid, dim3 block, cudaStream_t st, const SweepArgs
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (listed == 4 && win && win->num_bytes > 0) {
+    if (listed > 0 && win && win->num_bytes > 0) {
         attr[1].id = cudaLaunchAttributeAccessPolicyWindow;
         attr[1].val.accessPolicyWindow = *win;
         cfg.numAttrs = 2;
     }
-    const cudaError_t e = listed >= 3   ? cudaLaunchKernelEx(&cfg, vbd_sweep_stream_kernel<TPV, RE, RB>, a)
+    const cudaError_t e = listed == 4   ? cudaLaunchKernelEx(&cfg, vbd_sweep_prefetch_kernel<TPV, RE, RB>, a)
+                          : listed == 3 ? cudaLaunchKernelEx(&cfg, vbd_sweep_stream_kernel<TPV, RE, RB>, a)
                           : listed == 2 ? cudaLaunchKernelEx(&cfg, vbd_sweep_pipe_kernel<TPV, RE, RB>, a)
                           : listed == 1 ? cudaLaunchKernelEx(&cfg, vbd_sweep_list_kernel<TPV, RE, RB>, a)
                                         : cudaLaunchKernelEx(&cfg, vbd_sweep_kernel<TPV, RE, RB>, a);
@@ -1053,9 +1054,9 @@ cudaError_t sweep_launch(dim3 grid, dim3 block, cudaStream_t st, const SweepArgs
     return e;
 }
 
-// List form 3 keeps the positions in L2 between colours: a sweep streams about three
-// times the positions' bytes of stencil past them, and the next colours gather them
-// again as neighbours. The handles that use it share the context's persisting-L2
+// Persisting positions keep a handle's positions in L2 between colours: a list sweep
+// streams about three times the positions' bytes of stencil past them, and the next
+// colours gather them again as neighbours. The handles that use it share the context's persisting-L2
 // set-aside (cudaLimitPersistingL2CacheSize, a per-context limit): the first one sizes
 // it for its positions (up to the device maximum), the last one puts back the size it
 // found and resets the persisting lines. Each launch of its sweep carries an access-policy
@@ -1070,7 +1071,7 @@ int l2_keep_acquire(ats_cloth* c) {
     ATS_CUDA(cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, c->device));
     ATS_CUDA(cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, c->device));
     if (max_persist <= 0 || max_window <= 0) {
-        set_error("list sweep form 3: the device has no persisting L2");
+        set_error("persisting positions: the device has no persisting L2");
         return ATS_ERR_STATE;
     }
     const size_t window = std::min(c->x.bytes(), (size_t)max_window);
@@ -1106,16 +1107,17 @@ void l2_keep_release(ats_cloth* c) {
     }
 }
 
-// Sets the list form of a handle, taking or giving back its share of the set-aside.
+// Sets the list form of a handle (resident grid queried outside any capture).
 int set_list_form(ats_cloth* c, int form) {
-    if (form == 3) {
-        const int r = l2_keep_acquire(c);
-        if (r) return r;
-    } else {
-        l2_keep_release(c);
-    }
     c->list_form = form;
     list_sweep_ctas(c->L.tpv, c->block, form);
+    return ATS_OK;
+}
+
+// Takes or gives back the handle's share of the persisting-L2 set-aside.
+int set_l2_persisting(ats_cloth* c, bool on) {
+    if (on) return l2_keep_acquire(c);
+    l2_keep_release(c);
     return ATS_OK;
 }
 
@@ -1770,13 +1772,23 @@ int ats_set_sweep_form(ats_cloth* c, int solver, int form) {
 
 int ats_set_list_sweep(ats_cloth* c, int form) {
     if (!c || form < 0 || form > 3) {
-        set_error("ats_set_list_sweep: need a handle and 0 (plain), 1 (pipelined), 2 (streamed) or 3 (streamed, "
-                  "positions kept in L2)");
+        set_error("ats_set_list_sweep: need a handle and 0 (plain), 1 (pipelined), 2 (streamed) or 3 (prefetching)");
         return ATS_ERR_INVALID;
     }
     const int r = set_list_form(c, form);  // shared-memory attributes, outside any capture
     if (r) return r;
     c->drop_graphs();
+    return ATS_OK;
+}
+
+int ats_set_l2_persisting(ats_cloth* c, int on) {
+    if (!c || (on != 0 && on != 1)) {
+        set_error("ats_set_l2_persisting: need a handle and 0 or 1");
+        return ATS_ERR_INVALID;
+    }
+    const int r = set_l2_persisting(c, on != 0);
+    if (r) return r;
+    c->drop_graphs();  // captured sweeps hold the old launch attributes
     return ATS_OK;
 }
 
@@ -1946,6 +1958,7 @@ int ats_cloth_query(const ats_cloth* c, ats_cloth_info* info) {
     info->xpbd_form = c->xpbd_loop_blocks > 0 ? 1 : 0;
     info->list_form = c->list_form;
     info->tune_source = c->tune_source;
+    info->l2_persisting = c->l2_keep ? 1 : 0;
     long long sb = 64LL * c->L.nv;
     for (size_t k = 0; k + 3 < c->L.slices.size(); k += 4) {
         const int rows = c->L.slices[k + 3] & 0xffff, erows = c->L.slices[k + 3] >> 16;
@@ -2175,7 +2188,7 @@ namespace ats {
 // is what the choices depend on: the vertex and instance counts (power-of-two buckets)
 // and the colour counts of both solvers.
 struct TuneChoice {
-    int tpv, block, vbd_form, list_form, xpbd_form;
+    int tpv, block, vbd_form, list_form, xpbd_form, l2;
 };
 std::mutex g_tune_mu;
 std::map<std::string, TuneChoice> g_tune_cache;
@@ -2219,7 +2232,8 @@ int apply_tuning(ats_cloth* c, const TuneChoice& t) {
     }
     c->block = t.block;
     c->vbd_loop_blocks = t.vbd_form ? vbd_loop_blocks(c->L.tpv, c->block, c->device) : 0;
-    if (set_list_form(c, t.list_form)) set_list_form(c, 2);  // no persisting L2 here: the streamed form
+    set_list_form(c, t.list_form);
+    if (set_l2_persisting(c, t.l2 != 0)) set_l2_persisting(c, false);  // no persisting L2 on this device
     c->xpbd_loop_blocks = t.xpbd_form ? c->xpbd_loop_capable : 0;
     c->prm.threads_per_vertex = c->L.tpv;
     c->prm.block_size = c->block;
@@ -2251,10 +2265,10 @@ int ats_autotune_cache_save(const char* path) {
         set_error(std::string("ats_autotune_cache_save: cannot open ") + path);
         return ATS_ERR_INVALID;
     }
-    std::fprintf(f, "ats-autotune 1\n");
+    std::fprintf(f, "ats-autotune 2\n");
     for (const auto& kv : g_tune_cache)
-        std::fprintf(f, "%s %d %d %d %d %d\n", kv.first.c_str(), kv.second.tpv, kv.second.block, kv.second.vbd_form,
-                     kv.second.list_form, kv.second.xpbd_form);
+        std::fprintf(f, "%s %d %d %d %d %d %d\n", kv.first.c_str(), kv.second.tpv, kv.second.block, kv.second.vbd_form,
+                     kv.second.list_form, kv.second.xpbd_form, kv.second.l2);
     const bool ok = std::fclose(f) == 0;
     if (!ok) {
         set_error(std::string("ats_autotune_cache_save: write failed: ") + path);
@@ -2278,16 +2292,18 @@ int ats_autotune_cache_load(const char* path) {
     bool header = false, bad = false;
     while (std::fgets(line, sizeof(line), f)) {
         if (!header) {
-            header = std::strncmp(line, "ats-autotune 1", 14) == 0;
+            header = std::strncmp(line, "ats-autotune 2", 14) == 0;
             if (!header) bad = true;
             if (bad) break;
             continue;
         }
         char key[400];
         TuneChoice t;
-        if (std::sscanf(line, "%399s %d %d %d %d %d", key, &t.tpv, &t.block, &t.vbd_form, &t.list_form, &t.xpbd_form) != 6 ||
+        if (std::sscanf(line, "%399s %d %d %d %d %d %d", key, &t.tpv, &t.block, &t.vbd_form, &t.list_form, &t.xpbd_form,
+                        &t.l2) != 7 ||
             !(t.tpv == 1 || t.tpv == 2 || t.tpv == 4 || t.tpv == 8) || !(t.block == 64 || t.block == 128 || t.block == 256) ||
-            t.vbd_form < 0 || t.vbd_form > 1 || t.list_form < 0 || t.list_form > 3 || t.xpbd_form < 0 || t.xpbd_form > 1) {
+            t.vbd_form < 0 || t.vbd_form > 1 || t.list_form < 0 || t.list_form > 3 || t.xpbd_form < 0 || t.xpbd_form > 1 ||
+            t.l2 < 0 || t.l2 > 1) {
             bad = true;
             break;
         }
@@ -2408,9 +2424,17 @@ int ats_autotune(ats_cloth* c, int iterations, ats_stream stream, int* out_tpv, 
         std::vector<int> ones(c->L.ninst, 1);
         ATS_CUDA(cudaMemcpyAsync(c->active.p, ones.data(), ones.size() * sizeof(int), cudaMemcpyHostToDevice, st));
         if (!(r = enqueue_compaction(c, st))) {
-            float t_form[4] = {1e30f, 1e30f, 1e30f, 1e30f};
-            for (int form = 0; form < 4 && !r; ++form) {
-                if (set_list_form(c, form)) continue;  // form 3 needs a persisting L2
+            // forms 0-3, then the fastest with the positions persisting in L2 (form 4 here)
+            float t_form[5] = {1e30f, 1e30f, 1e30f, 1e30f, 1e30f};
+            int best_form = 0;
+            set_l2_persisting(c, false);
+            for (int form = 0; form < 5 && !r; ++form) {
+                if (form == 4) {
+                    for (int f = 1; f < 4; ++f)
+                        if (t_form[f] < t_form[best_form]) best_form = f;
+                    if (set_l2_persisting(c, true)) break;  // no persisting L2 on this device
+                }
+                set_list_form(c, form < 4 ? form : best_form);
                 if ((r = enqueue_iterations(c, ATS_SOLVER_VBD, 1, st, c->active.p))) break;
                 for (int rep = 0; rep < 3; ++rep) {
                     cudaEventRecord(e0, st);
@@ -2426,10 +2450,12 @@ int ats_autotune(ats_cloth* c, int iterations, ats_stream stream, int* out_tpv, 
                     t_form[form] = std::min(t_form[form], t);
                 }
             }
-            int best_form = 0;
-            for (int form = 1; form < 4 && !r; ++form)
-                if (t_form[form] < t_form[best_form]) best_form = form;
-            if (!r) r = set_list_form(c, best_form);
+            if (!r) {
+                for (int f = 1; f < 4; ++f)
+                    if (t_form[f] < t_form[best_form]) best_form = f;
+                set_list_form(c, best_form);
+                set_l2_persisting(c, t_form[4] < t_form[best_form]);
+            }
         }
         ATS_CUDA(cudaStreamSynchronize(st));  // the host vector leaves scope
     }
@@ -2468,7 +2494,7 @@ int ats_autotune(ats_cloth* c, int iterations, ats_stream stream, int* out_tpv, 
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
         g_tune_cache[key] = TuneChoice{c->L.tpv, c->block, c->vbd_loop_blocks > 0 ? 1 : 0, c->list_form,
-                                       c->xpbd_loop_blocks > 0 ? 1 : 0};
+                                       c->xpbd_loop_blocks > 0 ? 1 : 0, c->l2_keep ? 1 : 0};
     }
     if (out_tpv) *out_tpv = c->L.tpv;
     if (out_block) *out_block = c->block;
