@@ -99,9 +99,9 @@ def parse():
     p.add_argument("--trace-out", default="", help="write the full residual traces (JSON) here")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-extras", action="store_true")
-    p.add_argument("--list-sweep", type=int, default=-1, choices=[-1, 0, 1, 2, 3],
+    p.add_argument("--list-sweep", type=int, default=-1, choices=[-1, 0, 1, 2],
                    help="sweep of the residual-driven frames: -1 the autotuner's choice, 0 plain, 1 pipelined, "
-                        "2 streamed, 3 prefetching")
+                        "2 streamed")
     p.add_argument("--l2-persisting", type=int, default=-1, choices=[-1, 0, 1],
                    help="list sweeps keep the positions persisting in L2: -1 the autotuner's choice, 0 off, 1 on")
     p.add_argument("--tpv", type=int, default=0)
@@ -314,12 +314,15 @@ def maxrank(v):
     return float(sharding.allreduce_stats([float(v)], op="max")[0])
 
 
-# DRAM traffic over algorithmic bytes of the list sweeps, per launch: ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum, 3 launches, --clock-control none) on the
-# 32-instance c4 case, 1 lane per vertex, 64 threads per block: 216.9 MB (plain) and
-# 195.3 MB (streamed, which skips the per-vertex material record) against 214.0 MB
-# algorithmic.
-SWEEP_TRAFFIC_RATIO = {"vbd_sweep_list_kernel<1>": 1.013, "vbd_sweep_stream_kernel<1>": 0.913}
+# DRAM traffic over algorithmic bytes of the list sweeps, per launch, from ncu captures
+# of the full c4 batch (1 lane per vertex, 64 threads per block): dram__bytes_read.sum +
+# dram__bytes_write.sum, one pass, 3 launches, --cache-control none (warm caches, as in
+# the bench; ncu's default flushes them before every launch) --clock-control none.
+# Plain sweep: 32-instance case, cold caches, scaled (216.9 of 214.0 MB).
+SWEEP_TRAFFIC = {
+    "vbd_sweep_stream_kernel<1>": (0.889, "ncu, full c4 batch, warm caches: 357.9 MB a launch"),
+    "vbd_sweep_list_kernel<1>": (1.013, "ncu, 32-instance c4 case, cold caches, scaled by algorithmic bytes"),
+}
 
 
 def sweep_roofline(cloth, stream, reps=3, iters=50):
@@ -482,8 +485,8 @@ def run_learned(args):
 
     # sweep roofline in this run (listed sweep over all instances)
     per_launch, rf_frame_ms, bytes_launch = sweep_roofline(cloth, stream)
-    sweep_kernel = (("vbd_sweep_list_kernel", "vbd_sweep_pipe_kernel", "vbd_sweep_stream_kernel",
-                     "vbd_sweep_prefetch_kernel")[info.list_form] + f"<{info.threads_per_vertex}>"
+    sweep_kernel = (("vbd_sweep_list_kernel", "vbd_sweep_pipe_kernel", "vbd_sweep_stream_kernel")[info.list_form]
+                    + f"<{info.threads_per_vertex}>"
                     + (" (positions persisting in L2)" if info.l2_persisting else ""))
     peak, peak_src = hbm_peak()
     achieved = bytes_launch / (per_launch * 1e-3) / 1e9
@@ -570,13 +573,11 @@ def run_learned(args):
                                "host; wall clock"},
                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                             "frac": achieved / peak,
-                            "traffic": (SWEEP_TRAFFIC_RATIO[sweep_kernel] * bytes_launch
-                                        if sweep_kernel in SWEEP_TRAFFIC_RATIO else None),
-                            "traffic_source": ("not captured in this run: DRAM bytes read + written per launch from "
-                                               "an ncu capture of the 32-instance c4 case (3,528,428 vertices, "
-                                               "214.0 MB algorithmic per launch), scaled to this launch by its "
-                                               "algorithmic bytes" if sweep_kernel in SWEEP_TRAFFIC_RATIO
-                                               else "no capture of this kernel"),
+                            "traffic": (SWEEP_TRAFFIC[sweep_kernel][0] * bytes_launch
+                                        if sweep_kernel in SWEEP_TRAFFIC else None),
+                            "traffic_source": ("not captured in this run (DRAM bytes read + written per launch, as "
+                                               "a ratio to the algorithmic bytes): " + SWEEP_TRAFFIC[sweep_kernel][1]
+                                               if sweep_kernel in SWEEP_TRAFFIC else "no capture of this kernel"),
                             "kernel": sweep_kernel,
                             "us_per_launch_upper_bound": per_launch * 1e3, "alg_bytes_per_launch": bytes_launch,
                             "layout_bytes_per_launch": info.sweep_layout_bytes / info.num_vertex_colors,

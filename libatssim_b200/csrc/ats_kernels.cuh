@@ -512,110 +512,4 @@ __global__ void __launch_bounds__(256) vbd_sweep_stream_kernel(SweepArgs a) {
     }
 }
 
-// ---------------------------------------------------------------- prefetching list sweep
-// The streamed list sweep one stage deeper: while a warp computes slice i, the
-// neighbour indices of slice i + 1 are already loading (their stencil sectors come into
-// L1 and L2 then), the descriptor and metadata of slice i + 2, and the list entry of
-// slice i + 3. A slice then waits only for its neighbour gathers and the rest of its
-// stencil rows (weights, rest lengths: sectors already on chip), not for a DRAM round
-// trip before the gathers.
-template <int RE, int RB>
-struct SliceRows {
-    int ue[RE], ub[RB];
-};
-
-template <int TPV, int RE, int RB>
-__device__ __forceinline__ void load_rows(const SweepArgs& a, int4 sd, int lane, SliceRows<RE, RB>& s) {
-    const int erows = sd.w >> 16, brows = (sd.w & 0xffff) - erows;
-    const int v = sd.x + min(lane / TPV, sd.y - 1);
-    const int base = sd.z + lane, bbase = base + erows * 32;
-#pragma unroll
-    for (int r = 0; r < RE; ++r) s.ue[r] = r < erows ? __ldg(&a.st_iw[base + r * 32].x) : v;
-#pragma unroll
-    for (int r = 0; r < RB; ++r) s.ub[r] = r < brows ? __ldg(&a.st_iw[bbase + r * 32].x) : v;
-}
-
-// sweep_slice_sd (META, streamed constant data) with the neighbour indices given
-template <int TPV, int RE, int RB>
-__device__ __forceinline__ void sweep_rows(const SweepArgs& a, int4 sd, int2 meta, int lane, const SliceRows<RE, RB>& s) {
-    const int rows = sd.w & 0xffff, erows = sd.w >> 16, brows = rows - erows;
-    const int k = lane / TPV;
-    const bool leader = k < sd.y && (lane % TPV) == 0;
-    const int v = sd.x + min(k, sd.y - 1);
-    const int base = sd.z + lane;
-    const int bbase = base + erows * 32;
-    const float4 ip = __ldg(&a.inst[meta.x]);
-    const float4 xv = a.x[v];
-    float4 xe[RE], xb[RB];
-#pragma unroll
-    for (int r = 0; r < RE; ++r) xe[r] = a.x[s.ue[r]];
-#pragma unroll
-    for (int r = 0; r < RB; ++r) xb[r] = a.x[s.ub[r]];
-    float we[RE], le[RE], wb[RB];
-#pragma unroll
-    for (int r = 0; r < RE; ++r) {
-        we[r] = 0.f;
-        le[r] = -1.f;
-        if (r < erows) {
-            we[r] = __int_as_float(__ldcs(&a.st_iw[base + r * 32].y));
-            le[r] = __ldcs(&a.st_rest[base + r * 32]);
-        }
-    }
-#pragma unroll
-    for (int r = 0; r < RB; ++r) wb[r] = r < brows ? __int_as_float(__ldcs(&a.st_iw[bbase + r * 32].y)) : 0.f;
-    float4 p0 = make_float4(0.f, 0.f, 0.f, 0.f), vv = p0;
-    if (leader) {
-        p0 = __ldcs(&a.x0[v]);
-        vv = __ldcs(&a.vel[v]);
-    }
-    const float4 mv = make_float4(vv.w, ((unsigned)meta.y >> k) & 1u ? kPinBoost : 0.f, 0.f, 0.f);
-    sweep_vertex<TPV, RE, RB, PlainMem>(a, v, leader, base, bbase, erows, brows, xv, xe, le, we, xb, wb, ip.w, ip, mv,
-                                        p0, vv);
-}
-
-template <int TPV, int RE, int RB>
-__global__ void __launch_bounds__(256) vbd_sweep_prefetch_kernel(SweepArgs a) {
-    grid_dependency_wait();  // the list and the positions come from the kernels before
-    allow_dependent_launch();
-    const int lane = threadIdx.x & 31;
-    const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
-    const int count = *a.list_count;
-    int idx = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-    if (idx >= count) return;
-    const int s0 = a.list[idx];
-    int4 sd = __ldg(&a.slices[s0]);
-    int2 meta = __ldg(&a.slice_meta[s0]);
-    SliceRows<RE, RB> rows;
-    load_rows<TPV, RE, RB>(a, sd, lane, rows);
-    int4 sd1 = sd;
-    int2 meta1 = meta;
-    if (idx + nwarps < count) {
-        const int s1 = a.list[idx + nwarps];
-        sd1 = __ldg(&a.slices[s1]);
-        meta1 = __ldg(&a.slice_meta[s1]);
-    }
-    int s2 = idx + 2 * nwarps < count ? a.list[idx + 2 * nwarps] : 0;
-    for (;;) {
-        const bool more = idx + nwarps < count, more2 = idx + 2 * nwarps < count;
-        SliceRows<RE, RB> rows1 = rows;
-        if (more) load_rows<TPV, RE, RB>(a, sd1, lane, rows1);
-        int4 sd2 = sd1;
-        int2 meta2 = meta1;
-        if (more2) {
-            sd2 = __ldg(&a.slices[s2]);
-            meta2 = __ldg(&a.slice_meta[s2]);
-        }
-        const int s3 = idx + 3 * nwarps < count ? a.list[idx + 3 * nwarps] : 0;
-        sweep_rows<TPV, RE, RB>(a, sd, meta, lane, rows);
-        if (!more) break;
-        idx += nwarps;
-        sd = sd1;
-        meta = meta1;
-        rows = rows1;
-        sd1 = sd2;
-        meta1 = meta2;
-        s2 = s3;
-    }
-}
-
 }  // namespace ats
