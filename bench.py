@@ -320,6 +320,8 @@ def maxrank(v):
 # the bench; ncu's default flushes them before every launch) --clock-control none.
 # Plain sweep: 32-instance case, cold caches, scaled (216.9 of 214.0 MB).
 SWEEP_TRAFFIC = {
+    "vbd_sweep_stream_kernel<1> (positions persisting in L2)": (0.894, "ncu, full c4 batch, warm caches: "
+                                                                        "360.2 MB a launch"),
     "vbd_sweep_stream_kernel<1>": (0.889, "ncu, full c4 batch, warm caches: 357.9 MB a launch"),
     "vbd_sweep_list_kernel<1>": (1.013, "ncu, 32-instance c4 case, cold caches, scaled by algorithmic bytes"),
 }
