@@ -482,9 +482,7 @@ __global__ void __launch_bounds__(256) vbd_sweep_list_kernel(SweepArgs a) {
 // the chain in front of each slice's neighbour gathers is its stencil rows alone. The
 // material record is not read (sweep_slice_sd with META).
 template <int TPV, int RE, int RB>
-__global__ void __launch_bounds__(256) vbd_sweep_stream_kernel(SweepArgs a) {
-    grid_dependency_wait();  // the list and the positions come from the kernels before
-    allow_dependent_launch();
+__device__ __forceinline__ void stream_sweep(const SweepArgs& a) {
     const int lane = threadIdx.x & 31;
     const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
     const int count = *a.list_count;
@@ -510,6 +508,22 @@ __global__ void __launch_bounds__(256) vbd_sweep_stream_kernel(SweepArgs a) {
         meta = meta_next;
         next = after;
     }
+}
+
+template <int TPV, int RE, int RB>
+__global__ void __launch_bounds__(256) vbd_sweep_stream_kernel(SweepArgs a) {
+    grid_dependency_wait();  // the list and the positions come from the kernels before
+    allow_dependent_launch();
+    stream_sweep<TPV, RE, RB>(a);
+}
+
+// The same at 112 registers a thread: 9 CTAs of 64 threads per SM instead of 8, for a
+// few spilled registers.
+template <int TPV, int RE, int RB>
+__global__ void __maxnreg__(112) vbd_sweep_stream112_kernel(SweepArgs a) {
+    grid_dependency_wait();
+    allow_dependent_launch();
+    stream_sweep<TPV, RE, RB>(a);
 }
 
 }  // namespace ats

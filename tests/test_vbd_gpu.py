@@ -470,7 +470,7 @@ def test_persistent_vbd_frames_equal_per_colour_launches(ats, n):
 
 
 @pytest.mark.parametrize("tpv", [1, 2, 4, 8])
-@pytest.mark.parametrize("form", [1, 2])
+@pytest.mark.parametrize("form", [1, 2, 3])
 def test_list_sweep_forms_equal_plain(ats, tpv, form):
     """The residual-driven frames' sweep, plain against pipelined (each warp stages its
     next slice in shared memory while computing the current one), streamed (evict-first
@@ -537,3 +537,34 @@ def test_autotune_cache_hits_for_the_same_mesh_class(ats):
     for h in (a, b, c, d):
         h.close()
     ats.autotune_cache_clear()
+
+
+def test_list_sweep_and_l2_switch_arguments(ats):
+    """ats_set_list_sweep and ats_set_l2_persisting reject out-of-range arguments; the
+    context's persisting-L2 set-aside is sized while handles hold it and put back to
+    what it was when the last one lets go."""
+    import cuda.bindings.runtime as rt
+
+    def setaside():
+        err, v = rt.cudaDeviceGetLimit(rt.cudaLimit.cudaLimitPersistingL2CacheSize)
+        assert err == rt.cudaError_t.cudaSuccess
+        return v
+
+    insts, prm = configs.c2(num_instances=2, seed=1, side_range=(20, 30))
+    a = ats.Cloth(insts, **prm)
+    for bad in (-1, 4):
+        with pytest.raises(ats.AtsError) as e:
+            a.set_list_sweep(bad)
+        assert e.value.status == ats.ATS_ERR_INVALID
+    assert ats.lib().ats_set_l2_persisting(a.h, 2) == ats.ATS_ERR_INVALID
+    before = setaside()
+    a.set_l2_persisting(1)
+    b = ats.Cloth(insts, **prm)
+    b.set_l2_persisting(1)
+    assert a.info.l2_persisting == 1 and b.info.l2_persisting == 1
+    assert setaside() >= before
+    a.set_l2_persisting(0)
+    assert a.info.l2_persisting == 0
+    b.close()  # the last holder
+    assert setaside() == before
+    a.close()
