@@ -99,9 +99,9 @@ def parse():
     p.add_argument("--trace-out", default="", help="write the full residual traces (JSON) here")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-extras", action="store_true")
-    p.add_argument("--list-sweep", type=int, default=-1, choices=[-1, 0, 1, 2, 3],
+    p.add_argument("--list-sweep", type=int, default=-1, choices=[-1, 0, 1, 2],
                    help="sweep of the residual-driven frames: -1 the autotuner's choice, 0 plain, 1 pipelined, "
-                        "2 streamed, 3 streamed at 112 registers")
+                        "2 streamed")
     p.add_argument("--l2-persisting", type=int, default=-1, choices=[-1, 0, 1],
                    help="list sweeps keep the positions persisting in L2: -1 the autotuner's choice, 0 off, 1 on")
     p.add_argument("--tpv", type=int, default=0)
@@ -487,8 +487,7 @@ def run_learned(args):
 
     # sweep roofline in this run (listed sweep over all instances)
     per_launch, rf_frame_ms, bytes_launch = sweep_roofline(cloth, stream)
-    sweep_kernel = (("vbd_sweep_list_kernel", "vbd_sweep_pipe_kernel", "vbd_sweep_stream_kernel",
-                     "vbd_sweep_stream112_kernel")[info.list_form]
+    sweep_kernel = (("vbd_sweep_list_kernel", "vbd_sweep_pipe_kernel", "vbd_sweep_stream_kernel")[info.list_form]
                     + f"<{info.threads_per_vertex}>"
                     + (" (positions persisting in L2)" if info.l2_persisting else ""))
     peak, peak_src = hbm_peak()

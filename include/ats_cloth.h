@@ -96,8 +96,7 @@ typedef struct ats_cloth_info {
     long long device_bytes; /* device memory held by the handle */
     int vbd_form;           /* fixed-iteration VBD iterations: 0 a launch per colour, 1 persistent */
     int xpbd_form;          /* XPBD iterations: 0 a launch per colour, 1 persistent */
-    int list_form;          /* list sweep of residual-driven frames: 0 plain, 1 pipelined, 2 streamed,
-                               3 streamed at 112 registers a thread */
+    int list_form;          /* list sweep of residual-driven frames: 0 plain, 1 pipelined, 2 streamed */
     long long sweep_layout_bytes; /* bytes one VBD iteration of the streamed list sweep must move over
                                      every instance in this layout: the stencil rows as stored (8 B a
                                      slot, 4 more on edge rows), x read and written, x0 and vel per
@@ -239,9 +238,7 @@ int ats_set_sweep_form(ats_cloth* cloth, int solver, int form);
  * current one; 2 streamed, where the data read once per iteration (stencil, vertex
  * records, frame-start state) goes through evict-first loads, leaving L2 to the
  * positions, and each warp's next slice descriptor loads while the current slice
- * computes; 3 as 2 compiled for 112 registers a thread (9 CTAs of 64 threads per SM
- * instead of 8, a few registers spilled). Same positions. ats_autotune times the four
- * and keeps the fastest. */
+ * computes. Same positions. ats_autotune times the three and keeps the fastest. */
 int ats_set_list_sweep(ats_cloth* cloth, int form);
 
 /* on = 1: every list sweep of this handle keeps its positions in L2 as persisting lines

@@ -513,8 +513,8 @@ class Cloth:
         self.info = info
 
     def set_list_sweep(self, form):
-        """Sweep of the residual-driven frames: 0 plain, 1 pipelined, 2 streamed, 3
-        streamed at 112 registers (ats_set_list_sweep)."""
+        """Sweep of the residual-driven frames: 0 plain, 1 pipelined, 2 streamed
+        (ats_set_list_sweep)."""
         _check(lib().ats_set_list_sweep(self.h, int(form)))
         info = ClothInfo()
         _check(lib().ats_cloth_query(self.h, ctypes.byref(info)))

@@ -1011,14 +1011,13 @@ int list_form_ctas(int form, int block, int sms) {
     switch (form) {
         case 1: return resident_ctas(vbd_sweep_pipe_kernel<TPV, RE, RB>, block, (block / 32) * pipe_smem_per_warp<RE, RB>(), sms);
         case 2: return resident_ctas(vbd_sweep_stream_kernel<TPV, RE, RB>, block, 0, sms);
-        case 3: return resident_ctas(vbd_sweep_stream112_kernel<TPV, RE, RB>, block, 0, sms);
         default: return resident_ctas(vbd_sweep_list_kernel<TPV, RE, RB>, block, 0, sms);
     }
 }
 int list_sweep_ctas(int tpv, int block, int form) {
-    static int cache[4][4][3] = {};
+    static int cache[3][4][3] = {};
     const int ti = tpv == 1 ? 0 : tpv == 2 ? 1 : tpv == 4 ? 2 : 3, bi = block == 64 ? 0 : block == 128 ? 1 : 2;
-    int& slot = cache[form >= 0 && form < 4 ? form : 0][ti][bi];
+    int& slot = cache[form >= 0 && form < 3 ? form : 0][ti][bi];
     if (!slot) {
         int dev = 0, sms = 148;
         cudaGetDevice(&dev);
@@ -1054,8 +1053,7 @@ cudaError_t sweep_launch(dim3 grid, dim3 block, cudaStream_t st, const SweepArgs
         attr[1].val.accessPolicyWindow = *win;
         cfg.numAttrs = 2;
     }
-    const cudaError_t e = listed == 4   ? cudaLaunchKernelEx(&cfg, vbd_sweep_stream112_kernel<TPV, RE, RB>, a)
-                          : listed == 3 ? cudaLaunchKernelEx(&cfg, vbd_sweep_stream_kernel<TPV, RE, RB>, a)
+    const cudaError_t e = listed == 3   ? cudaLaunchKernelEx(&cfg, vbd_sweep_stream_kernel<TPV, RE, RB>, a)
                           : listed == 2 ? cudaLaunchKernelEx(&cfg, vbd_sweep_pipe_kernel<TPV, RE, RB>, a)
                           : listed == 1 ? cudaLaunchKernelEx(&cfg, vbd_sweep_list_kernel<TPV, RE, RB>, a)
                                         : cudaLaunchKernelEx(&cfg, vbd_sweep_kernel<TPV, RE, RB>, a);
@@ -1780,9 +1778,8 @@ int ats_set_sweep_form(ats_cloth* c, int solver, int form) {
 }
 
 int ats_set_list_sweep(ats_cloth* c, int form) {
-    if (!c || form < 0 || form > 3) {
-        set_error("ats_set_list_sweep: need a handle and 0 (plain), 1 (pipelined), 2 (streamed) or 3 (streamed at "
-                  "112 registers)");
+    if (!c || form < 0 || form > 2) {
+        set_error("ats_set_list_sweep: need a handle and 0 (plain), 1 (pipelined) or 2 (streamed)");
         return ATS_ERR_INVALID;
     }
     const int r = set_list_form(c, form);  // shared-memory attributes, outside any capture
@@ -2312,7 +2309,7 @@ int ats_autotune_cache_load(const char* path) {
         if (std::sscanf(line, "%399s %d %d %d %d %d %d", key, &t.tpv, &t.block, &t.vbd_form, &t.list_form, &t.xpbd_form,
                         &t.l2) != 7 ||
             !(t.tpv == 1 || t.tpv == 2 || t.tpv == 4 || t.tpv == 8) || !(t.block == 64 || t.block == 128 || t.block == 256) ||
-            t.vbd_form < 0 || t.vbd_form > 1 || t.list_form < 0 || t.list_form > 3 || t.xpbd_form < 0 || t.xpbd_form > 1 ||
+            t.vbd_form < 0 || t.vbd_form > 1 || t.list_form < 0 || t.list_form > 2 || t.xpbd_form < 0 || t.xpbd_form > 1 ||
             t.l2 < 0 || t.l2 > 1) {
             bad = true;
             break;
@@ -2434,17 +2431,17 @@ int ats_autotune(ats_cloth* c, int iterations, ats_stream stream, int* out_tpv, 
         std::vector<int> ones(c->L.ninst, 1);
         ATS_CUDA(cudaMemcpyAsync(c->active.p, ones.data(), ones.size() * sizeof(int), cudaMemcpyHostToDevice, st));
         if (!(r = enqueue_compaction(c, st))) {
-            // forms 0-3, then the fastest with the positions persisting in L2 (slot 4 here)
-            float t_form[5] = {1e30f, 1e30f, 1e30f, 1e30f, 1e30f};
+            // forms 0-2, then the fastest with the positions persisting in L2 (slot 3 here)
+            float t_form[4] = {1e30f, 1e30f, 1e30f, 1e30f};
             int best_form = 0;
             set_l2_persisting(c, false);
-            for (int form = 0; form < 5 && !r; ++form) {
-                if (form == 4) {
-                    for (int f = 1; f < 4; ++f)
+            for (int form = 0; form < 4 && !r; ++form) {
+                if (form == 3) {
+                    for (int f = 1; f < 3; ++f)
                         if (t_form[f] < t_form[best_form]) best_form = f;
                     if (set_l2_persisting(c, true)) break;  // no persisting L2 on this device
                 }
-                set_list_form(c, form < 4 ? form : best_form);
+                set_list_form(c, form < 3 ? form : best_form);
                 if ((r = enqueue_iterations(c, ATS_SOLVER_VBD, 1, st, c->active.p))) break;
                 for (int rep = 0; rep < 3; ++rep) {
                     cudaEventRecord(e0, st);
@@ -2461,10 +2458,10 @@ int ats_autotune(ats_cloth* c, int iterations, ats_stream stream, int* out_tpv, 
                 }
             }
             if (!r) {
-                for (int f = 1; f < 4; ++f)
+                for (int f = 1; f < 3; ++f)
                     if (t_form[f] < t_form[best_form]) best_form = f;
                 set_list_form(c, best_form);
-                set_l2_persisting(c, t_form[4] < t_form[best_form]);
+                set_l2_persisting(c, t_form[3] < t_form[best_form]);
             }
         }
         ATS_CUDA(cudaStreamSynchronize(st));  // the host vector leaves scope

@@ -81,8 +81,7 @@ struct ats_cloth {
     int xpbd_loop_capable = 0;           // co-resident blocks of the persistent XPBD kernel (0: unavailable)
     int xpbd_loop_blocks = 0;            // the blocks XPBD frames launch it with (0: per-colour launches)
     int vbd_loop_blocks = 0;             // the same for VBD iterations (0: one launch per colour; set by autotune)
-    int list_form = 0;                   // list sweep of residual-driven frames: 0 plain, 1 pipelined, 2 streamed,
-                                         // 3 streamed at 112 registers
+    int list_form = 0;                   // list sweep of residual-driven frames: 0 plain, 1 pipelined, 2 streamed
     int tune_source = 0;                 // shape and forms: 0 defaults or explicit, 1 timed, 2 tuning cache
     bool l2_keep = false;                // list sweeps keep the positions persisting in L2
     cudaAccessPolicyWindow l2_window{};  // their access-policy window (empty when off)

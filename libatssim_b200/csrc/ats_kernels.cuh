@@ -517,13 +517,4 @@ __global__ void __launch_bounds__(256) vbd_sweep_stream_kernel(SweepArgs a) {
     stream_sweep<TPV, RE, RB>(a);
 }
 
-// The same at 112 registers a thread: 9 CTAs of 64 threads per SM instead of 8, for a
-// few spilled registers.
-template <int TPV, int RE, int RB>
-__global__ void __maxnreg__(112) vbd_sweep_stream112_kernel(SweepArgs a) {
-    grid_dependency_wait();
-    allow_dependent_launch();
-    stream_sweep<TPV, RE, RB>(a);
-}
-
 }  // namespace ats

@@ -59,7 +59,7 @@ def test_autotune_cache_file_round_trip(ats, tmp_path):
     assert sorted(out.read_text().splitlines()) == sorted(src.read_text().splitlines())
     for bad in ("ats-autotune 1\nk 1 64 0 0 0\n",               # older version
                 "ats-autotune 2\nk 3 64 0 0 0 0\n",             # lanes per vertex not 1, 2, 4, 8
-                "ats-autotune 2\nk 1 64 0 4 0 0\n",             # list form out of range
+                "ats-autotune 2\nk 1 64 0 3 0 0\n",             # list form out of range
                 "ats-autotune 2\nk 1 64 0 0 0 2\n",             # persisting flag not 0 or 1
                 "ats-autotune 2\nk 1 64\n"):                    # short line
         f = tmp_path / "bad.txt"
