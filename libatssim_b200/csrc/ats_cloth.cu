@@ -1068,12 +1068,30 @@ cudaError_t sweep_launch(dim3 grid, dim3 block, cudaStream_t st, const SweepArgs
 // it for its positions (up to the device maximum), the last one puts back the size it
 // found and resets the persisting lines. Each launch of its sweep carries an access-policy
 // window over the handle's positions whose hit ratio is the set-aside over the window.
+// Per device: the handles holding a share and the set-aside size found before the first.
+struct L2Share {
+    int users = 0;
+    size_t prev = 0;
+};
 std::mutex g_l2_mu;
-int g_l2_users = 0;
-size_t g_l2_prev = 0;
+std::map<int, L2Share> g_l2;
+
+// Makes `dev` current for the scope (the limit calls act on the current device).
+struct CurrentDevice {
+    int prev = -1;
+    explicit CurrentDevice(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~CurrentDevice() {
+        int now = -1;
+        if (prev >= 0 && cudaGetDevice(&now) == cudaSuccess && now != prev) cudaSetDevice(prev);
+    }
+};
 
 int l2_keep_acquire(ats_cloth* c) {
     if (c->l2_keep) return ATS_OK;
+    CurrentDevice on(c->device);
     int max_persist = 0, max_window = 0;
     ATS_CUDA(cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, c->device));
     ATS_CUDA(cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, c->device));
@@ -1085,13 +1103,13 @@ int l2_keep_acquire(ats_cloth* c) {
     size_t setaside = 0;
     {
         std::lock_guard<std::mutex> lk(g_l2_mu);
+        L2Share& sh = g_l2[c->device];
         size_t cur = 0;
         ATS_CUDA(cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize));
-        if (g_l2_users == 0) g_l2_prev = cur;
         const size_t want = std::min(window, (size_t)max_persist);
         if (want > cur) ATS_CUDA(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want));
         ATS_CUDA(cudaDeviceGetLimit(&setaside, cudaLimitPersistingL2CacheSize));
-        ++g_l2_users;
+        if (sh.users++ == 0) sh.prev = cur;
     }
     c->l2_window.base_ptr = c->x.p;
     c->l2_window.num_bytes = window;
@@ -1106,11 +1124,13 @@ void l2_keep_release(ats_cloth* c) {
     if (!c->l2_keep) return;
     c->l2_keep = false;
     c->l2_window = cudaAccessPolicyWindow{};
+    CurrentDevice on(c->device);
     std::lock_guard<std::mutex> lk(g_l2_mu);
-    if (--g_l2_users == 0) {
+    L2Share& sh = g_l2[c->device];
+    if (--sh.users == 0) {
         cudaDeviceSynchronize();
         cudaCtxResetPersistingL2Cache();
-        cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, g_l2_prev);
+        cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, sh.prev);
     }
 }
 
