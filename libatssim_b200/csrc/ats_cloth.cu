@@ -941,9 +941,6 @@ int upload_stencil(ats_cloth* c) {
             if (L.vm[4 * (size_t)(vb + j) + 1] != 0.f) pins |= 1u << j;
         sm[k] = make_int2(si[k], (int)pins);
     }
-    if ((r = upload(c->row_base, L.row_base, L.row_base.size())) ||
-        (r = upload(c->st_idx16, L.st_idx16, L.st_idx16.size())) || (r = upload(c->st_w, L.st_w, L.st_w.size())))
-        return r;
     if ((r = upload(c->slice_inst, si, si.size())) || (r = upload(c->slice_meta, sm, sm.size())) ||
         (r = upload(c->color_slices, L.color_slices, L.color_slices.size())))
         return r;
@@ -1164,9 +1161,6 @@ int launch_sweep(ats_cloth* c, int color, cudaStream_t st, const int* active) {
     a.slices = c->slices.p;
     a.slice_inst = c->slice_inst.p;
     a.slice_meta = c->slice_meta.p;
-    a.row_base = c->row_base.p;
-    a.st_idx16 = c->st_idx16.p;
-    a.st_w = c->st_w.p;
     a.inst = c->inst.p;
     // with an activity mask: only the slices the last compaction listed (the mask
     // itself is what the compaction read)
@@ -1338,9 +1332,6 @@ int launch_vbd_loop(ats_cloth* c, int iterations, cudaStream_t st) {
     a.slices = c->slices.p;
     a.slice_inst = c->slice_inst.p;
     a.slice_meta = c->slice_meta.p;
-    a.row_base = c->row_base.p;
-    a.st_idx16 = c->st_idx16.p;
-    a.st_w = c->st_w.p;
     a.inst = c->inst.p;
     a.active = nullptr;
     a.list = nullptr;
@@ -1997,9 +1988,8 @@ int ats_cloth_query(const ats_cloth* c, ats_cloth_info* info) {
     info->l2_persisting = c->l2_keep ? 1 : 0;
     long long sb = 64LL * c->L.nv;
     for (size_t k = 0; k + 3 < c->L.slices.size(); k += 4) {
-        const int off = c->L.slices[k + 2], rows = c->L.slices[k + 3] & 0xffff, erows = c->L.slices[k + 3] >> 16;
-        sb += 32LL * 4 * erows + 28 + 4LL * std::min(rows, 32);
-        for (int r = 0; r < rows; ++r) sb += 32LL * (r < 32 && c->L.row_base[off / 32 + r] >= 0 ? 6 : 14);
+        const int rows = c->L.slices[k + 3] & 0xffff, erows = c->L.slices[k + 3] >> 16;
+        sb += 32LL * (8 * rows + 4 * erows) + 28;
     }
     info->sweep_layout_bytes = sb;
     return ATS_OK;

@@ -68,9 +68,6 @@ struct ats_cloth {
     DevBuf<int4> slices;
     DevBuf<int> slice_inst;     // instance of each slice
     DevBuf<int2> slice_meta;    // per slice {instance, bit k = vertex k of the slice pinned}
-    DevBuf<int> row_base;       // the streamed sweep's stencil: per row the base index (-1: use st_iw)
-    DevBuf<unsigned short> st_idx16;  // per entry the offset from its row's base
-    DevBuf<float> st_w;               // per entry the weight
     DevBuf<int> color_slices;   // n_vcolors + 1 slice offsets per colour
     DevBuf<int> act_list, act_count;  // per colour, the slices of instances still iterating
     DevBuf<int2> xs_edge;
@@ -137,8 +134,7 @@ struct ats_cloth {
     }
     size_t device_bytes() const {
         return x.bytes() + x0.bytes() + vel.bytes() + vm.bytes() + inst.bytes() + st_iw.bytes() + st_rest.bytes() +
-               slices.bytes() + slice_inst.bytes() + slice_meta.bytes() + row_base.bytes() + st_idx16.bytes() +
-               st_w.bytes() + color_slices.bytes() + act_list.bytes() + act_count.bytes() + xs_edge.bytes() + xs_rest.bytes() + xs_k.bytes() + xs_lambda.bytes() +
+               slices.bytes() + slice_inst.bytes() + slice_meta.bytes() + color_slices.bytes() + act_list.bytes() + act_count.bytes() + xs_edge.bytes() + xs_rest.bytes() + xs_k.bytes() + xs_lambda.bytes() +
                xb_idx.bytes() + xb_q.bytes() + xb_lambda.bytes() + en_edge.bytes() + en_rest.bytes() + en_k.bytes() +
                en_q.bytes() + en_kb.bytes() + en_bend.bytes() + inst_seg.bytes() + to_caller.bytes() + io_x.bytes() +
                io_v.bytes() + async_begin.bytes() + partial.bytes() +

@@ -47,9 +47,6 @@ struct SweepArgs {
     const int4* __restrict__ slices;
     const int* __restrict__ slice_inst;  // instance of each slice
     const int2* __restrict__ slice_meta; // {instance, pinned-vertex bits} of each slice
-    const int* __restrict__ row_base;    // the compact stencil (streamed sweep): per row its base index
-    const unsigned short* __restrict__ st_idx16;  // per entry the offset from the base
-    const float* __restrict__ st_w;      // per entry the weight
     const float4* __restrict__ inst;
     const int* __restrict__ active;      // vbd_sweep_kernel: per instance, null = all active
     const int* __restrict__ list;        // vbd_sweep_list_kernel: this colour's active slices
@@ -275,24 +272,12 @@ struct StreamLoads {
     static __device__ __forceinline__ T ld(const T* p) { return __ldcs(p); }
 };
 
-// Neighbour index and weight of entry `at` in global stencil row `row` of the compact
-// stencil: base + 16-bit offset, or the full entry where the row has no base (-1).
-// rb_lane holds the bases of the slice's first 32 rows, lane r row r's; `row` is the
-// same on every lane.
-__device__ __forceinline__ int2 compact_entry(const SweepArgs& a, int rb_lane, int row, size_t at) {
-    const int rb = row < 32 ? __shfl_sync(0xffffffffu, rb_lane, row) : -1;
-    const int off = (int)__ldcs(&a.st_idx16[at]);
-    const float w = __ldcs(&a.st_w[at]);
-    return make_int2(rb >= 0 ? rb + off : __ldcs(&a.st_iw[at]).x, __float_as_int(w));
-}
-
 // One slice of a sweep (descriptor sd): every vertex of the slice (its constant data,
 // then all neighbour positions at once, then the solve). M chooses how positions are
 // accessed, LD how the per-iteration constant data is loaded. With META the material
 // record vm is not read: the instance and the pinned vertices come from the slice's
 // metadata meta = {instance, pinned bits}, the bending diagonal from vel.w (the same
-// values, 16 bytes less per vertex), and the stencil rows come from the compact stencil
-// (6 bytes an entry instead of 8; the same indices and weights).
+// values, 16 bytes less per vertex).
 template <int TPV, int RE, int RB, class M, class LD = ConstLoads, bool META = false>
 __device__ __forceinline__ void sweep_slice_sd(const SweepArgs& a, int4 sd, int lane, int2 meta = make_int2(0, 0)) {
     const int rows = sd.w & 0xffff, erows = sd.w >> 16, brows = rows - erows;
@@ -301,7 +286,6 @@ __device__ __forceinline__ void sweep_slice_sd(const SweepArgs& a, int4 sd, int 
     const int v = sd.x + min(k, sd.y - 1);
     const int base = sd.z + lane;
     const int bbase = base + erows * 32;
-    const int rb_lane = META && lane < rows ? __ldg(&a.row_base[(sd.z >> 5) + lane]) : -1;
     int ue[RE], ub[RB];
     float we[RE], le[RE], wb[RB];
 #pragma unroll
@@ -310,7 +294,7 @@ __device__ __forceinline__ void sweep_slice_sd(const SweepArgs& a, int4 sd, int 
         we[r] = 0.f;
         le[r] = -1.f;
         if (r < erows) {
-            const int2 iw = META ? compact_entry(a, rb_lane, r, base + r * 32) : LD::ld(&a.st_iw[base + r * 32]);
+            const int2 iw = LD::ld(&a.st_iw[base + r * 32]);
             ue[r] = iw.x;
             we[r] = __int_as_float(iw.y);
             le[r] = LD::ld(&a.st_rest[base + r * 32]);
@@ -321,8 +305,7 @@ __device__ __forceinline__ void sweep_slice_sd(const SweepArgs& a, int4 sd, int 
         ub[r] = v;
         wb[r] = 0.f;
         if (r < brows) {
-            const int2 iw =
-                META ? compact_entry(a, rb_lane, erows + r, bbase + r * 32) : LD::ld(&a.st_iw[bbase + r * 32]);
+            const int2 iw = LD::ld(&a.st_iw[bbase + r * 32]);
             ub[r] = iw.x;
             wb[r] = __int_as_float(iw.y);
         }

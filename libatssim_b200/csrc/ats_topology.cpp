@@ -218,9 +218,6 @@ bool build_slices(Layout& L, int tpv, std::string& err) {
             }
     L.st_iw.assign(2 * total, 0);
     L.st_rest.assign(total, -1.f);
-    L.st_idx16.assign(total, 0);
-    L.st_w.assign(total, 0.f);
-    L.row_base.assign(total / 32, -1);
     L.slices.clear();
     L.slices.reserve(4 * nslices);
     L.color_slices.assign(1, 0);
@@ -256,21 +253,6 @@ bool build_slices(Layout& L, int tpv, std::string& err) {
                         L.st_iw[2 * at] = idx;
                         std::memcpy(&L.st_iw[2 * at + 1], &w, 4);
                         L.st_rest[at] = rest;
-                    }
-                }
-                // 16-bit offsets from the row's smallest index, where the row allows them
-                for (int row = 0; row < rows; ++row) {
-                    const size_t at0 = off + 32 * (size_t)row;
-                    int lo = L.st_iw[2 * at0], hi = lo;
-                    for (int th = 1; th < 32; ++th) {
-                        lo = std::min(lo, L.st_iw[2 * (at0 + th)]);
-                        hi = std::max(hi, L.st_iw[2 * (at0 + th)]);
-                    }
-                    const bool fits = (long long)hi - lo < 65536;
-                    L.row_base[at0 / 32] = fits ? lo : -1;
-                    for (int th = 0; th < 32; ++th) {
-                        L.st_idx16[at0 + th] = fits ? (uint16_t)(L.st_iw[2 * (at0 + th)] - lo) : (uint16_t)0;
-                        std::memcpy(&L.st_w[at0 + th], &L.st_iw[2 * (at0 + th) + 1], 4);
                     }
                 }
                 L.slices.push_back(s);

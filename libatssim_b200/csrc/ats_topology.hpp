@@ -69,13 +69,6 @@ struct Layout {
     std::vector<int> st_iw;         // 2 per entry: neighbour layout id (self for padding), bending weight bits
     std::vector<float> st_rest;     // per entry: rest length (edge rows only), -1 = padding
     std::vector<int> slices;        // 4 ints per slice: vbegin, nverts, entry offset, rows | edge rows << 16
-    // the same stencil for the streamed sweep, 6 bytes an entry instead of 8: per row of a
-    // slice (global row = entry offset / 32 + row) the smallest neighbour index of its 32
-    // entries, or -1 when the row spans 65,536 indices or more (then st_iw holds it);
-    // per entry the offset from that base and the weight
-    std::vector<int> row_base;
-    std::vector<uint16_t> st_idx16;
-    std::vector<float> st_w;
     std::vector<int> color_slices;  // n_vcolors + 1 offsets into slices
     // XPBD, colour-major over all instances
     std::vector<int> xs_edge;       // 2 per constraint (layout ids)

@@ -568,26 +568,3 @@ def test_list_sweep_and_l2_switch_arguments(ats):
     b.close()  # the last holder
     assert setaside() == before
     a.close()
-
-
-@pytest.mark.parametrize("tpv", [1, 2])
-def test_compact_stencil_with_wide_rows_equals_plain(ats, tpv):
-    """The streamed sweep reads the compact stencil (a base index per row, 16-bit offsets);
-    rows whose neighbours span 65,536 indices or more fall back to the full entries. A
-    300 x 300 cloth has such rows (about 2 % at one lane per vertex): positions stay
-    bit-identical to the plain list sweep's."""
-    insts = [configs.grid_instance(300), configs.grid_instance(40)]
-    prm = dict(implicit_dt=1.0 / 60.0, num_substep=1, iterations=10, damping=2.0)
-    a = ats.Cloth(insts, threads_per_vertex=tpv, block_size=64, **prm)
-    b = ats.Cloth(insts, threads_per_vertex=tpv, block_size=64, **prm)
-    a.set_list_sweep(0)
-    b.set_list_sweep(2)
-    for _ in range(3):
-        a.frame_to_residual(0.0, check_every=5, max_iterations=10)
-        b.frame_to_residual(0.0, check_every=5, max_iterations=10)
-    xa, va = a.state()
-    xb, vb = b.state()
-    assert np.linalg.norm(xa - insts[0].positions.min()) > 0
-    assert np.array_equal(xa, xb) and np.array_equal(va, vb)
-    a.close()
-    b.close()
