@@ -24,10 +24,7 @@ Headline workload (the default, a step = one simulated frame of the whole batch)
          FP64 residual traces of both forms, and timed frames to each tolerance.
   e2e    the learned frame through the public C ABI with host arrays: every frame
          uploads (x, v) from pinned host memory and reads them back (wall clock).
-         The value splits the batch into 4 handles of whole instances, each driven by
-         its own host thread and stream, so one group's copies overlap the others'
-         frames; the one-handle serial figure is reported beside it.
-  roofline  the list sweep the autotuner chose, the colour sweep of these frames: algorithmic
+  roofline  vbd_sweep_list_kernel, the colour sweep of these frames: algorithmic
          bytes per launch (40 V + 12 E + 56 B per iteration, shared by colour) over
          its per-launch time, measured in this run as 50 listed iterations timed with
          CUDA events (predict, update and two probes included, so a lower bound),
@@ -417,67 +414,6 @@ def plain_extras(stream, peak):
     return out
 
 
-def e2e_pipelined(insts, prm, info, model, args, x_h, v_h, groups=4, frames=5):
-    """The learned frame end to end through the C ABI, with the batch split into
-    `groups` handles of whole instances (balanced by vertex count), each iterated by its
-    own host thread on its own stream: a group's state goes up from pinned host memory,
-    its frame runs and its state comes back, while the other groups compute, so the
-    copies overlap the frames. Every instance still starts each frame from its host
-    state and returns it. Returns (frames/s of the whole batch, groups used)."""
-    import threading
-
-    import torch
-
-    import libatssim_b200 as ats
-    from libatssim_b200 import learned
-    vw = np.array([i.num_verts for i in insts])
-    cum = np.concatenate([[0], np.cumsum(vw)])
-    cuts = sorted(set([0, len(insts)] + [int(np.searchsorted(cum, cum[-1] * k / groups)) for k in range(1, groups)]))
-    spans = [(a, b) for a, b in zip(cuts[:-1], cuts[1:]) if b > a]
-    handles, streams, views = [], [], []
-    for a, b in spans:
-        c = ats.Cloth(insts[a:b], threads_per_vertex=info.threads_per_vertex, block_size=info.block_size, **prm)
-        c.set_probe_policy(args.probe_policy)
-        c.set_list_sweep(info.list_form)
-        if info.l2_persisting:
-            c.set_l2_persisting(1)
-        handles.append(c)
-        streams.append(torch.cuda.Stream())
-        views.append((x_h[cum[a]:cum[b]], v_h[cum[a]:cum[b]], [float(i.mass.sum()) for i in insts[a:b]]))
-    clock = {}
-    start = threading.Barrier(len(spans), action=lambda: clock.setdefault("t0", time.perf_counter()))
-    errors = []
-
-    def work(g):
-        c, st, (xg, vg, masses) = handles[g], streams[g], views[g]
-        try:
-            for f in range(frames + 1):
-                if f == 1:
-                    st.synchronize()
-                    start.wait()
-                c.set_accel(learned.wind_table(np.random.RandomState(30000 + 97 * g + f), masses), stream=st)
-                c.set_state(xg, vg, stream=st)
-                c.frame_warm_to_residual(model, args.tol, check_every=args.check_every, max_iterations=args.cap,
-                                         stream=st)
-                c.state_into(xg, vg, stream=st)
-            st.synchronize()
-        except Exception as e:  # reported after the join
-            errors.append(e)
-            start.abort()
-
-    threads = [threading.Thread(target=work, args=(g,)) for g in range(len(spans))]
-    for t in threads:
-        t.start()
-    for t in threads:
-        t.join()
-    t1 = time.perf_counter()
-    for c in handles:
-        c.close()
-    if errors:
-        raise errors[0]
-    return frames / (t1 - clock["t0"]), len(spans)
-
-
 def run_learned(args):
     """c4 (or c3): learned and plain forms to the same fixed tolerance."""
     import torch
@@ -578,9 +514,6 @@ def run_learned(args):
     torch.cuda.synchronize()
     e2e_s = maxrank((time.perf_counter() - t0) / e2e_frames)
     state_bytes = 2 * 3 * 4 * nv
-    # the same through several handles whose copies overlap each other's frames
-    pipe_fps, pipe_groups = e2e_pipelined(insts, prm, info, model, args, x_h, v_h)
-    pipe_fps = 1.0 / maxrank(1.0 / pipe_fps)
 
     sweep, trace, timed_tols = None, None, None
     if world == 1 and args.sweep_cap > 0:
@@ -636,16 +569,10 @@ def run_learned(args):
                                         f"of instance-frames within {args.cap} iterations; speed-up "
                                         f"{plain_ms / learned_ms:.2f}x against the 2x target")},
                "tolerance_sweep": sweep, "timed_to_tolerance": timed_tols,
-               "e2e": {"value": pipe_fps, "unit": UNIT, "h2d_bytes_per_step": state_bytes,
+               "e2e": {"value": 1.0 / e2e_s, "unit": UNIT, "h2d_bytes_per_step": state_bytes,
                        "d2h_bytes_per_step": state_bytes,
-                       "path": "pipelined (below); the serial figure beside it",
-                       "serial": {"value": 1.0 / e2e_s,
-                                  "path": "one handle: ats_set_state from pinned host, ats_frame_warm_to_residual, "
-                                          "ats_get_state to pinned host, frame after frame; wall clock"},
-                       "pipelined": {"value": pipe_fps, "groups": pipe_groups,
-                                     "path": f"{pipe_groups} handles of whole instances, one host thread and stream "
-                                             "each, the same three calls per frame; a group's copies overlap the "
-                                             "others' frames; wall clock from a common start"}},
+                       "path": "ats_set_state from pinned host, ats_frame_warm_to_residual, ats_get_state to pinned "
+                               "host; wall clock"},
                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                             "frac": achieved / peak,
                             "traffic": (SWEEP_TRAFFIC[sweep_kernel][0] * bytes_launch
