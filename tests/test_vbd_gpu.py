@@ -568,3 +568,45 @@ def test_list_sweep_and_l2_switch_arguments(ats):
     b.close()  # the last holder
     assert setaside() == before
     a.close()
+
+
+def test_edge_cases_tiny_pinned_and_empty(ats, oracle):
+    """Degenerate inputs the sweeps must carry: no instances (rejected), a single triangle
+    (3 vertices, no bending edge, a one-vertex slice per colour) batched with a normal
+    cloth, an instance with every vertex pinned (inactive from the start of a
+    residual-driven frame) and a frame with no iterations."""
+    prm = dict(implicit_dt=1.0 / 60.0, num_substep=1, iterations=8, damping=2.0)
+    with pytest.raises(ats.AtsError) as e:
+        ats.Cloth([], **prm)
+    assert e.value.status == ats.ATS_ERR_INVALID
+    tri_pos = np.array([[0.0, 0.0, 0.0], [0.1, 0.0, 0.0], [0.0, 0.0, 0.1]], dtype=np.float32)
+    tri = ats.Instance(tri_pos, np.array([[0, 1, 2]], dtype=np.int32), np.full(3, 0.01, np.float32),
+                       np.array([1, 0, 0], dtype=np.uint8), 1e3, 1e-2)
+    grid = configs.grid_instance(12)
+    pinned = configs.grid_instance(6)
+    pinned = ats.Instance(pinned.positions, pinned.faces, pinned.mass, np.ones(pinned.num_verts, np.uint8),
+                          pinned.k_stretch, pinned.k_bend)
+    cloth = ats.Cloth([tri, grid, pinned], **prm)
+    x_start = cloth.state()[0].copy()
+    for _ in range(3):
+        cloth.frame()
+    x, _ = cloth.state()
+    # the triangle and the grid against their own oracle scenes
+    n0, n1 = tri.num_verts, grid.num_verts
+    for inst, lo in ((tri, 0), (grid, n0)):
+        s = oracle.Scene(inst.positions, inst.faces, inst.mass, inst.fixed, iterations=8, k_stretch=inst.k_stretch,
+                         k_bend=inst.k_bend)
+        s.run(3)
+        xo, _ = s.state()
+        assert np.abs(x[lo:lo + inst.num_verts] - xo).max() <= 1e-5 * max(1.0, np.abs(xo).max())
+    # pinned vertices stay put up to their 1e9 Hessian boost: gravity over 1e9 moves them
+    # by about 1e-11 (the reference's compute_inertia does the same)
+    assert np.abs(x[n0 + n1:] - x_start[n0 + n1:]).max() < 1e-8
+    # residual-driven: the all-pinned instance runs no iteration; a zero cap runs none at all
+    for form in (0, 2):
+        cloth.set_list_sweep(form)
+        it, res = cloth.frame_to_residual(1e-4, check_every=4, max_iterations=12)
+        assert it[2] == 0 and it[1] == 12 and np.isfinite(res).all()
+        it, res = cloth.frame_to_residual(1e-4, check_every=4, max_iterations=0)
+        assert (it == 0).all()
+    cloth.close()
