@@ -70,5 +70,8 @@ def test_autotune_cache_file_round_trip(ats, tmp_path):
         assert ats.autotune_cache_size() == 2
     with pytest.raises(ats.AtsError):
         ats.autotune_cache_load(str(tmp_path / "missing.txt"))
+    with pytest.raises(ats.AtsError) as e:
+        ats.autotune_cache_save(str(tmp_path))  # a directory
+    assert e.value.status == ats.ATS_ERR_INVALID
     ats.autotune_cache_clear()
     assert ats.autotune_cache_size() == 0
