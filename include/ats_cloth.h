@@ -250,6 +250,15 @@ int ats_set_list_sweep(ats_cloth* cloth, int form);
  * if the device has no persisting L2. Same positions. ats_autotune times it. */
 int ats_set_l2_persisting(ats_cloth* cloth, int on);
 
+/* Self-test of the bounded device waits, on the current device: one kernel waits at a
+ * grid barrier (as the persistent kernels do) for arrivals that never come, one waits
+ * on an mbarrier (as the tensor-core inference does) on which nothing arrives; each must
+ * give up after `polls` polls and set its error word, and a kernel launched after them
+ * must still run. Reports ATS_ERR_TIMEOUT in each status when its wait expired as
+ * designed (ATS_OK if it did not), and returns ATS_ERR_STATE if the kernel after them
+ * did not run. No fault or hang is involved: every wait is bounded. */
+int ats_selftest_bounded_waits(unsigned polls, int* barrier_status, int* mbarrier_status);
+
 /* Probe schedule of the residual-driven frames of this handle (ats_frame_to_residual(s),
  * ats_frame_warm_to_residual). 0 (default): every check_every iterations after an
  * instance's first probe, and at max_iterations. 1 (extrapolated): the first two probes

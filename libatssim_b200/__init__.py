@@ -150,6 +150,7 @@ _SIGNATURES = {
     "ats_set_sweep_form": [_vp, ctypes.c_int, ctypes.c_int],
     "ats_set_list_sweep": [_vp, ctypes.c_int],
     "ats_set_l2_persisting": [_vp, ctypes.c_int],
+    "ats_selftest_bounded_waits": [ctypes.c_uint, _ip, _ip],
     "ats_autotune_cache_size": [],
     "ats_autotune_cache_save": [ctypes.c_char_p],
     "ats_autotune_cache_load": [ctypes.c_char_p],
@@ -214,6 +215,14 @@ def kernel_launches():
     n = ctypes.c_longlong(0)
     _check(lib().ats_kernel_launches(ctypes.byref(n)))
     return int(n.value)
+
+
+def selftest_bounded_waits(polls=4096):
+    """Runs a grid-barrier wait and an mbarrier wait that cannot complete; returns their
+    statuses (ATS_ERR_TIMEOUT each when the bound worked) (ats_selftest_bounded_waits)."""
+    b, m = ctypes.c_int(-1), ctypes.c_int(-1)
+    _check(lib().ats_selftest_bounded_waits(int(polls), ctypes.byref(b), ctypes.byref(m)))
+    return b.value, m.value
 
 
 def autotune_cache_size():

@@ -22,6 +22,7 @@
 
 #include "ats_internal.cuh"
 #include "ats_kernels.cuh"
+#include "ats_umma.cuh"
 
 namespace ats {
 
@@ -262,7 +263,8 @@ __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
-__device__ __forceinline__ bool grid_barrier(unsigned* bar, int* err, unsigned& target) {
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, int* err, unsigned& target,
+                                             unsigned max_polls = kBarrierSpins) {
     __shared__ int s_ok;
     target += gridDim.x;
     __syncthreads();
@@ -271,7 +273,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, int* err, unsigned& 
         unsigned v = atomicAdd(bar, 1u) + 1u;
         unsigned spins = 0;
         while ((v & ~kBarrierError) < target && !(v & kBarrierError)) {
-            if (++spins > kBarrierSpins) {
+            if (++spins > max_polls) {
                 v = atomicOr(bar, kBarrierError) | kBarrierError;
                 atomicExch(err, 1);
                 break;
@@ -893,6 +895,28 @@ __global__ void __launch_bounds__(256) residual_check_kernel(const double* norm,
         *n_active = count[0];
         *pidx = init ? 0 : p + 1;
     }
+}
+
+// Self-test of the bounded waits (ats_selftest_bounded_waits): each kernel waits for
+// something that never happens and must give up after `polls` polls with its error
+// word set. One block waits at a grid barrier for twice the blocks launched; one block
+// waits on an mbarrier on which nothing arrives.
+__global__ void selftest_barrier_kernel(unsigned* bar, int* err, unsigned polls) {
+    unsigned target = gridDim.x;  // grid_barrier adds gridDim.x: 2 x the arrivals there will be
+    grid_barrier(bar, err, target, polls);
+}
+
+__global__ void selftest_mbarrier_kernel(int* err, unsigned polls) {
+    __shared__ __align__(8) uint64_t mbar;
+    if (threadIdx.x == 0) umma::mbar_init(&mbar, 1);
+    __syncthreads();
+    const bool ok = umma::mbar_wait(&mbar, 0, polls);
+    if (!ok && threadIdx.x == 0) atomicExch(err, 1);
+    __syncthreads();
+}
+
+__global__ void selftest_touch_kernel(int* out) {
+    if (threadIdx.x == 0) *out = 12345;
 }
 
 }  // namespace
@@ -1816,6 +1840,35 @@ int ats_set_l2_persisting(ats_cloth* c, int on) {
     const int r = set_l2_persisting(c, on != 0);
     if (r) return r;
     c->drop_graphs();  // captured sweeps hold the old launch attributes
+    return ATS_OK;
+}
+
+int ats_selftest_bounded_waits(unsigned polls, int* barrier_status, int* mbarrier_status) {
+    if (!barrier_status || !mbarrier_status || polls == 0) {
+        set_error("ats_selftest_bounded_waits: need two status pointers and polls > 0");
+        return ATS_ERR_INVALID;
+    }
+    DevBuf<unsigned> bar;
+    DevBuf<int> words;
+    ATS_CUDA(bar.alloc(2));
+    ATS_CUDA(words.alloc(3));
+    ATS_CUDA(cudaMemset(bar.p, 0, 2 * sizeof(unsigned)));
+    ATS_CUDA(cudaMemset(words.p, 0, 3 * sizeof(int)));
+    selftest_barrier_kernel<<<1, 32>>>(bar.p, words.p, polls);
+    ATS_CUDA(cudaGetLastError());
+    selftest_mbarrier_kernel<<<1, 32>>>(words.p + 1, polls);
+    ATS_CUDA(cudaGetLastError());
+    selftest_touch_kernel<<<1, 32>>>(words.p + 2);  // the context still runs kernels
+    ATS_CUDA(cudaGetLastError());
+    ATS_CUDA(cudaDeviceSynchronize());
+    int h[3] = {0, 0, 0};
+    ATS_CUDA(cudaMemcpy(h, words.p, sizeof(h), cudaMemcpyDeviceToHost));
+    *barrier_status = h[0] ? ATS_ERR_TIMEOUT : ATS_OK;
+    *mbarrier_status = h[1] ? ATS_ERR_TIMEOUT : ATS_OK;
+    if (h[2] != 12345) {
+        set_error("ats_selftest_bounded_waits: a kernel after the expired waits did not run");
+        return ATS_ERR_STATE;
+    }
     return ATS_OK;
 }
 

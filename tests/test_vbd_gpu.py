@@ -610,3 +610,16 @@ def test_edge_cases_tiny_pinned_and_empty(ats, oracle):
         it, res = cloth.frame_to_residual(1e-4, check_every=4, max_iterations=0)
         assert (it == 0).all()
     cloth.close()
+
+
+def test_bounded_waits_expire_and_report(ats):
+    """The device waits are bounded: a grid-barrier wait for arrivals that never come and
+    an mbarrier wait on which nothing arrives both give up after their poll limit and
+    report it, and the context keeps running kernels (a frame afterwards)."""
+    b, m = ats.selftest_bounded_waits(4096)
+    assert b == ats.ATS_ERR_TIMEOUT and m == ats.ATS_ERR_TIMEOUT
+    insts, prm = configs.c2(num_instances=2, seed=2, side_range=(16, 24))
+    cloth = ats.Cloth(insts, **prm)
+    cloth.frame()
+    assert np.isfinite(cloth.state()[0]).all()
+    cloth.close()
