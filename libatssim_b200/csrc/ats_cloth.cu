@@ -1014,20 +1014,11 @@ template <int RE, int RB>
 constexpr size_t pipe_smem_per_warp() {
     return 2 * sizeof(SliceStage<RE, RB>);
 }
-size_t pipe_smem_bytes(int tpv, int block) {
-    const size_t warps = (size_t)block / 32;
-    switch (tpv) {
-        case 1: return warps * pipe_smem_per_warp<6, 6>();
-        case 2: return warps * pipe_smem_per_warp<3, 3>();
-        case 4: return warps * pipe_smem_per_warp<2, 2>();
-        default: return warps * pipe_smem_per_warp<1, 1>();
-    }
-}
 
 // Resident CTAs of the list sweeps (form 0: vbd_sweep_list_kernel, 1:
 // vbd_sweep_pipe_kernel, 2: vbd_sweep_stream_kernel), all SMs together, per (lanes per
-// vertex, block size); queried
-// (and the pipelined kernel's shared-memory attributes set) on first use, which is
+// vertex, block size); queried (and the pipelined kernel's shared-memory attributes
+// set) on first use, which is
 // outside stream capture (the eager iterations of ats_frame_to_residual's first frame,
 // or ats_autotune, come first).
 template <int TPV, int RE, int RB>
